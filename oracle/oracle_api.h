@@ -1,0 +1,38 @@
+// C-ABI of the CPU oracle (test infrastructure; see oracle_common.h). Images
+// are row-major; colour images are interleaved BGR uint8; the cost volume is
+// uint8 disparity-major ([D][H*W]); the segmentation pyramid uses the
+// reference's ISP layout (segment.cu:884-905).
+#pragma once
+#include <cstdint>
+
+extern "C" {
+// matching cost and colour (oracle_cost.cpp)
+void orc_grey_u8(const uint8_t *bgr, int n, uint8_t *out);
+void orc_census(const uint8_t *img, int W, int H, uint32_t *out);
+void orc_cost_volume(const uint32_t *cL, const uint32_t *cR, int W, int H, int D, uint8_t *vol,
+                     float *wta);
+void orc_cost_to_right(const uint8_t *volL, int W, int H, int D, uint8_t *volR, float *wta);
+void orc_lab_set_overrides(const uint32_t *keys, const float *vals, int n);
+void orc_lab(const uint8_t *bgr, int n, float *lab4);
+void orc_nn_grid(const float *lab4, int W, int H, int *nn, float *dist_min, int *bd);
+
+// segmentation (oracle_seg.cpp)
+int orc_crtrees(const int *nn, int N, int *clus);
+int orc_crtrees_literal(const int *nn, int N, int *clus);
+int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_sizes, int *clus,
+                float *mean, int *bd, int *bdl);
+
+// belief propagation (oracle_hbp.cpp)
+int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+            const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
+            float alpha, float tau_smooth, int min_level, int fp64, long max_steps, float *disp,
+            float *plane, float *state_belief, float *state_plane);
+
+// post-processing (oracle_post.cpp)
+void orc_lr_check(const float *dispL, const float *dispR, float *planeL, int W, int H,
+                  uint8_t *failL);
+void orc_plane_to_disp(const float *plane, int W, int H, float *disp);
+void orc_weighted_median(const uint8_t *bgr, const uint8_t *fail, float *plane, int W, int H,
+                         int stable);
+void orc_driver_median(float *D, int W, int H);
+}

@@ -1,0 +1,629 @@
+// CPU oracle, hierarchical belief propagation on the segmentation pyramid
+// (test infrastructure; see oracle_common.h). Restates HBP_ISP
+// (hbp_isp.hpp:122-442, hbp_isp.cu) for one view.
+//
+// Two modes share the code: R = float reproduces the engine bit for bit
+// (same operation order, same reductions); R = double is the FP64 oracle used
+// for the message-error report and as the CPU baseline.
+//
+// Reduction orders fixed by the engine (the reference uses float atomics and
+// Thrust reduce_by_key, whose order is unspecified):
+//   plane cost of node n, candidate k: the node's pixels in raster order are
+//   cut into chunks of 256; inside a chunk pixel j+32*s goes to slot j
+//   (slots accumulate sequentially from 0), the 32 slots are combined by the
+//   xor butterfly of orc::butterfly32; chunk sums are added in chunk order.
+//   belief[k][s] = cost[k][s] + msg_t of s's out-edges in edge order.
+//   dc colour term: (|dL| + |da|) + |db|; position term: dx*dx + dy*dy.
+#include <algorithm>
+#include <cfloat>
+#include <cstdio>
+
+#include "oracle_api.h"
+#include "oracle_common.h"
+
+using namespace orc;
+
+namespace
+{
+constexpr int P = 4, K = 12;
+constexpr int CHUNK = 256;
+
+template <typename R>
+struct P4
+{
+    R x, y, z, w;
+};
+
+template <typename R>
+struct Level
+{
+    int N = 0, E = 0, Nh = 1;
+    const int *clus = nullptr; // N -> parent
+    std::vector<float> mean;   // 6 x N (means for c < 5, count in c = 5)
+    const int *bd = nullptr;   // E pairs
+    const int *bdl = nullptr;  // E
+    std::vector<int> pix;      // HW pixel ids sorted by (node, pixel)
+    std::vector<int> pix_off;  // N + 1
+    std::vector<int> nb_off;   // N + 1 (CSR by source)
+    std::vector<int> rev;      // E
+    std::vector<R> dc;         // 2 x E
+    std::vector<int> child;    // N children sorted by (parent, child)
+    std::vector<int> child_off; // Nh + 1
+    std::vector<P4<R>> plane; // K x N
+    std::vector<R> cost, belief; // K x N
+    std::vector<int> pid;     // 3 x N
+};
+
+template <typename R>
+struct Engine
+{
+    int W, H, D, L;
+    R lambda, tau, tau_smooth;
+    const uint8_t *vol; // D x HW
+    const float *wta;
+    std::vector<Level<R>> lv;
+    std::vector<R> msg, msg_t;
+    std::vector<uint32_t> s_child, s_nb, s_ransac;
+    std::vector<int> order;
+    std::vector<P4<R>> plane_buf;
+    long steps = 0, max_steps = -1;
+    bool stopped = false;
+
+    R pixel_cost(int px, const P4<R> &pl) const
+    {
+        R x = (R)(px % W), y = (R)(px / W);
+        R d_f = pl.x * x + pl.y * y + pl.z;
+        int d = f2i_rd((float)d_f);
+        if (sizeof(R) == 8)
+        {
+            // FP64 mode: floor in double with the same NaN/saturation rules
+            double v = (double)d_f;
+            d = v != v ? 0 : (v >= 2147483648.0 ? 2147483647 : (v < -2147483648.0 ? (-2147483647 - 1) : (int)std::floor(v)));
+        }
+        R cost;
+        if (d < 0 || d >= D - 1)
+            cost = tau;
+        else
+        {
+            const size_t n = (size_t)W * H;
+            R v0 = (R)vol[(size_t)d * n + px], v1 = (R)vol[(size_t)(d + 1) * n + px];
+            cost = ((R)(d + 1) - d_f) * v0 + (d_f - (R)d) * v1;
+        }
+        return lambda * cost;
+    }
+
+    // compute_plane_cost (hbp_isp.cu:1159-1174) for slots s_c .. s_c+3.
+    void plane_cost(Level<R> &l, int s_c)
+    {
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int n = 0; n < l.N; ++n)
+        {
+            int b = l.pix_off[n], m = l.pix_off[n + 1] - b;
+            for (int p = 0; p < P; ++p)
+            {
+                const P4<R> pl = l.plane[(size_t)(s_c + p) * l.N + n];
+                R total = 0;
+                for (int c0 = 0; c0 < m; c0 += CHUNK)
+                {
+                    R slots[32];
+                    for (int j = 0; j < 32; ++j)
+                    {
+                        R acc = 0;
+                        for (int k = c0 + j; k < std::min(m, c0 + CHUNK); k += 32)
+                            acc += pixel_cost(l.pix[b + k], pl);
+                        slots[j] = acc;
+                    }
+                    R cs = butterfly32(slots);
+                    total = c0 == 0 ? cs : total + cs;
+                }
+                l.cost[(size_t)(s_c + p) * l.N + n] = total;
+            }
+        }
+    }
+
+    // ransac_candidate_plane + make_three_diff_id + fit_plane_from_points
+    // (hbp_isp.cu:504-548, :592-640).
+    void ransac(Level<R> &l)
+    {
+#pragma omp parallel for schedule(static)
+        for (int n = 0; n < l.N; ++n)
+        {
+            int cn = l.pix_off[n + 1] - l.pix_off[n], cp = l.pix_off[n];
+            uint32_t s = s_ransac[n];
+            for (int p = 2 * P; p < 3 * P; ++p)
+            {
+                s = lcg(s);
+                int p0 = (int)(s % (uint32_t)cn);
+                s = lcg(s);
+                int p1 = cn > 1 ? (int)(s % (uint32_t)(cn - 1)) : 0;
+                s = lcg(s);
+                int p2 = cn > 2 ? (int)(s % (uint32_t)(cn - 2)) : 0;
+                if (cn <= 3)
+                {
+                    p1 = (p0 + 1) % cn;
+                    p2 = (p1 + 1) % cn;
+                }
+                else
+                {
+                    if (p1 == p0)
+                        p1 = cn - 1;
+                    if (p2 == p0)
+                        p2 = (p1 == cn - 2) ? cn - 1 : cn - 2;
+                    else if (p2 == p1)
+                        p2 = (p0 == cn - 2) ? cn - 1 : cn - 2;
+                }
+                int ids[3] = {l.pix[cp + p0], l.pix[cp + p1], l.pix[cp + p2]};
+                R Ax = (R)(ids[0] % W), Ay = (R)(ids[0] / W), Az = (R)wta[ids[0]];
+                R Bx = (R)(ids[1] % W), By = (R)(ids[1] / W), Bz = (R)wta[ids[1]];
+                R Cx = (R)(ids[2] % W), Cy = (R)(ids[2] / W), Cz = (R)wta[ids[2]];
+                R ax = Bx - Ax, ay = By - Ay, az = Bz - Az;
+                R bx = Cx - Ax, by = Cy - Ay, bz = Cz - Az;
+                R nx = ay * bz - az * by;
+                R ny = az * bx - ax * bz;
+                R nz = ax * by - ay * bx;
+                nx /= nz;
+                ny /= nz;
+                nz /= nz;
+                P4<R> pl;
+                R eps = sizeof(R) == 4 ? (R)FLT_EPSILON : (R)DBL_EPSILON;
+                if (std::fabs(nz - (R)1) > eps)
+                    pl = {0, 0, (Az + Bz + Cz) / (R)3, 0};
+                else
+                    pl = {-nx, -ny, nx * Ax + ny * Ay + Az, 0};
+                l.plane[(size_t)p * l.N + n] = pl;
+                if (p == 3 * P - 1)
+                {
+                    l.pid[3 * (size_t)n] = ids[0];
+                    l.pid[3 * (size_t)n + 1] = ids[1];
+                    l.pid[3 * (size_t)n + 2] = ids[2];
+                }
+            }
+            s_ransac[n] = s;
+        }
+    }
+
+    // select_child_plane, neighbor_candidate_plane, set_candidate_plane_k
+    // (hbp_isp.cu:676-741, :1225-1243).
+    void spatial(int li)
+    {
+        Level<R> &l = lv[li], &h = lv[li + 1];
+        for (int id = 0; id < h.N; ++id)
+        {
+            int cn = l.child_off[id + 1] - l.child_off[id], cp = l.child_off[id];
+            uint32_t s = s_child[id];
+            for (int p = 0; p < P; ++p)
+            {
+                s = lcg(s);
+                int c = l.child[cp + (int)(s % (uint32_t)cn)];
+                h.plane[(size_t)(p + 2 * P) * h.N + id] = l.plane[c];
+            }
+            s_child[id] = s;
+        }
+        for (int id = 0; id < h.N; ++id)
+        {
+            int nbn = h.nb_off[id + 1] - h.nb_off[id], nbp = h.nb_off[id];
+            uint32_t s = s_nb[id];
+            for (int p = 0; p < P; ++p)
+            {
+                s = lcg(s);
+                int t = h.bd[2 * (size_t)(nbp + (int)(s % (uint32_t)nbn)) + 1];
+                plane_buf[(size_t)p * h.N + id] = h.plane[(size_t)(p + 2 * P) * h.N + t];
+            }
+            s_nb[id] = s;
+        }
+        for (int p = 0; p < P; ++p)
+            for (int id = 0; id < h.N; ++id)
+                h.plane[(size_t)(p + 2 * P) * h.N + id] = plane_buf[(size_t)p * h.N + id];
+        for (int n = 0; n < l.N; ++n)
+            for (int p = 2 * P; p < 3 * P; ++p)
+                l.plane[(size_t)p * l.N + n] = h.plane[(size_t)p * h.N + l.clus[n]];
+    }
+
+    // random_candidate_plane + normalize_plane (hbp_isp.cu:495-503, :641-674).
+    void random_adjust(Level<R> &l, R max_dz, R max_dn)
+    {
+        for (int n = 0; n < l.N; ++n)
+        {
+            uint32_t s = s_ransac[n];
+            R x = (R)l.mean[3 * (size_t)l.N + n], y = (R)l.mean[4 * (size_t)l.N + n];
+            for (int p = 2 * P; p < 3 * P; ++p)
+            {
+                P4<R> pl = l.plane[(size_t)p * l.N + n];
+                R z = pl.x * x + pl.y * y + pl.z;
+                auto unif = [&](R f) {
+                    s = lcg(s);
+                    return (R)s / (R)2147483648.0 * f;
+                };
+                R dz = unif(max_dz);
+                z += dz;
+                R dnx = unif(max_dn), dny = unif(max_dn), dnz = unif(max_dn);
+                R norm = std::sqrt(pl.x * pl.x + pl.y * pl.y + pl.z * pl.z);
+                pl.x /= norm;
+                pl.y /= norm;
+                pl.z /= norm;
+                pl.x += dnx;
+                pl.y += dny;
+                pl.z += dnz;
+                R a = -pl.x / pl.z, b = -pl.y / pl.z;
+                R c = z - a * x - b * y;
+                l.plane[(size_t)p * l.N + n] = {a, b, c, 0};
+            }
+            s_ransac[n] = s;
+        }
+    }
+
+    // belief_propagation (hbp_isp.cu:1206-1214, kernels :273-493).
+    void bp(Level<R> &l)
+    {
+        const int N = l.N, E = l.E;
+        // passing_msg_k
+        for (int e = 0; e < E; ++e)
+        {
+            int t = l.bd[2 * (size_t)e + 1];
+            for (int p = 0; p < 2 * P; ++p)
+                msg[(size_t)p * E + e] = l.belief[(size_t)p * N + t] - msg[(size_t)p * E + e];
+        }
+        // smooth_msg_k + normalize_msg_k
+#pragma omp parallel for schedule(static)
+        for (int e = 0; e < E; ++e)
+        {
+            int s = l.bd[2 * (size_t)e], t = l.bd[2 * (size_t)e + 1];
+            R X[6], Y[6];
+            for (int i = 0; i < 3; ++i)
+            {
+                int a = l.pid[3 * (size_t)s + i], b = l.pid[3 * (size_t)t + i];
+                X[i] = (R)(a % W);
+                Y[i] = (R)(a / W);
+                X[3 + i] = (R)(b % W);
+                Y[3 + i] = (R)(b / W);
+            }
+            R dist_color = std::fmax(l.dc[e], (R)0.01f);
+            R dist_pos = std::fmax(l.dc[(size_t)E + e], (R)1.0f);
+            R c0 = dist_color * (R)l.bdl[e];
+            R out[K];
+            for (int y = 0; y < K; ++y)
+            {
+                P4<R> ps = l.plane[(size_t)y * N + s];
+                R acc = 0, mn = (R)FLT_MAX;
+                for (int p = 0; p < 2 * P; ++p)
+                {
+                    if (p == P)
+                    {
+                        acc += mn;
+                        mn = (R)FLT_MAX;
+                    }
+                    P4<R> pt = l.plane[(size_t)p * N + t];
+                    R dx = ps.x - pt.x, dy = ps.y - pt.y, dz = ps.z - pt.z;
+                    R phi = 0;
+                    for (int i = 0; i < 6; ++i)
+                    {
+                        R term = std::fabs(dx * X[i] + dy * Y[i] + dz);
+                        phi = i == 0 ? term : phi + term;
+                    }
+                    phi = std::fmin(phi / (R)3 / dist_pos, tau_smooth);
+                    R m = msg[(size_t)p * E + e] + c0 * phi;
+                    if (m < mn)
+                        mn = m;
+                }
+                acc += mn;
+                out[y] = acc;
+            }
+            R mean = 0;
+            for (int k = 0; k < K; ++k)
+                mean += out[k];
+            mean /= (R)K;
+            for (int k = 0; k < K; ++k)
+                msg_t[(size_t)k * E + e] = out[k] - mean;
+        }
+        // aggregate_belief: belief = cost + out-edge messages in edge order
+        for (int n = 0; n < N; ++n)
+            for (int k = 0; k < K; ++k)
+            {
+                R b = l.cost[(size_t)k * N + n];
+                for (int e = l.nb_off[n]; e < l.nb_off[n + 1]; ++e)
+                    b += msg_t[(size_t)k * E + e];
+                l.belief[(size_t)k * N + n] = b;
+            }
+        // ping_pang_msg_k
+        for (int e = 0; e < E; ++e)
+            for (int k = 0; k < K; ++k)
+                msg[(size_t)k * E + l.rev[e]] = msg_t[(size_t)k * E + e];
+        // get_belief_order + select_belief + select_msg
+        for (int n = 0; n < N; ++n)
+        {
+            int ord[K] = {0};
+            for (int i = 0; i < K - 1; ++i)
+                for (int j = i + 1; j < K; ++j)
+                {
+                    if (l.belief[(size_t)j * N + n] < l.belief[(size_t)i * N + n])
+                        ord[i]++;
+                    else
+                        ord[j]++;
+                }
+            int nb = 0;
+            for (int k = 0; k < K; ++k)
+            {
+                order[(size_t)k * N + n] = ord[k];
+                if (ord[k] < P)
+                {
+                    l.plane[(size_t)nb * N + n] = l.plane[(size_t)k * N + n];
+                    l.cost[(size_t)nb * N + n] = l.cost[(size_t)k * N + n];
+                    l.belief[(size_t)nb * N + n] = l.belief[(size_t)k * N + n];
+                    nb++;
+                }
+            }
+        }
+        for (int e = 0; e < E; ++e)
+        {
+            int t = l.bd[2 * (size_t)e + 1];
+            int nb = 0;
+            for (int k = 0; k < K; ++k)
+                if (order[(size_t)k * N + t] < P)
+                {
+                    msg[(size_t)nb * E + e] = msg[(size_t)k * E + e];
+                    nb++;
+                }
+        }
+    }
+
+    void setup(const int *level_sizes, const int *clus, const float *mean, const int *bd,
+               const int *bdl)
+    {
+        lv.resize(L);
+        size_t oc = 0, ob = 0;
+        const int HW = W * H;
+        std::vector<int> im_clus(HW);
+        for (int i = 0; i < HW; ++i)
+            im_clus[i] = i;
+        for (int li = 0; li < L; ++li)
+        {
+            Level<R> &l = lv[li];
+            l.N = level_sizes[2 * li];
+            l.E = level_sizes[2 * li + 1];
+            l.Nh = li + 1 < L ? level_sizes[2 * (li + 1)] : 1;
+            l.clus = clus + oc;
+            l.mean.assign(mean + 6 * oc, mean + 6 * (oc + l.N));
+            l.bd = bd + 2 * ob;
+            l.bdl = bdl + ob;
+            oc += l.N;
+            ob += l.E;
+            // pixels grouped by node in raster order (setup_D4, hbp_isp.cu:871-891)
+            l.pix_off.assign(l.N + 1, 0);
+            for (int i = 0; i < HW; ++i)
+                l.pix_off[im_clus[i] + 1]++;
+            for (int n = 0; n < l.N; ++n)
+                l.pix_off[n + 1] += l.pix_off[n];
+            l.pix.resize(HW);
+            {
+                std::vector<int> fill(l.pix_off.begin(), l.pix_off.end() - 1);
+                for (int i = 0; i < HW; ++i)
+                    l.pix[fill[im_clus[i]]++] = i;
+            }
+            // CSR by source + reverse edge (reverse_bd_id, hbp_isp.cu:1003-1019)
+            l.nb_off.assign(l.N + 1, 0);
+            for (int e = 0; e < l.E; ++e)
+                l.nb_off[l.bd[2 * (size_t)e] + 1]++;
+            for (int n = 0; n < l.N; ++n)
+                l.nb_off[n + 1] += l.nb_off[n];
+            l.rev.assign(l.E, 0);
+            for (int e = 0; e < l.E; ++e)
+            {
+                int s = l.bd[2 * (size_t)e], t = l.bd[2 * (size_t)e + 1];
+                for (int r = l.nb_off[t]; r < l.nb_off[t + 1]; ++r)
+                    if (l.bd[2 * (size_t)r + 1] == s)
+                    {
+                        l.rev[e] = r;
+                        break;
+                    }
+            }
+            // sum_to_mean + compute_dist_color_pos (hbp_isp.cu:952-970, :78-126)
+            for (int c = 0; c < 5; ++c)
+                for (int n = 0; n < l.N; ++n)
+                    l.mean[(size_t)c * l.N + n] /= l.mean[5 * (size_t)l.N + n];
+            l.dc.assign(2 * (size_t)l.E, 0);
+            for (int e = 0; e < l.E; ++e)
+            {
+                int s = l.bd[2 * (size_t)e], t = l.bd[2 * (size_t)e + 1];
+                const float *m = l.mean.data();
+                float col = std::fabs(m[s] - m[t]) + std::fabs(m[l.N + s] - m[l.N + t]);
+                col = col + std::fabs(m[2 * (size_t)l.N + s] - m[2 * (size_t)l.N + t]);
+                float dx = m[3 * (size_t)l.N + s] - m[3 * (size_t)l.N + t];
+                float dy = m[4 * (size_t)l.N + s] - m[4 * (size_t)l.N + t];
+                float pos = dx * dx + dy * dy;
+                l.dc[e] = (R)(float)std::exp((double)(-col / 20.0f));
+                l.dc[(size_t)l.E + e] = (R)std::sqrt(pos);
+            }
+            // children grouped by parent (sort_clus, hbp_isp.cu:985-1001)
+            l.child_off.assign(l.Nh + 1, 0);
+            for (int n = 0; n < l.N; ++n)
+                l.child_off[l.clus[n] + 1]++;
+            for (int p = 0; p < l.Nh; ++p)
+                l.child_off[p + 1] += l.child_off[p];
+            l.child.resize(l.N);
+            {
+                std::vector<int> fill(l.child_off.begin(), l.child_off.end() - 1);
+                for (int n = 0; n < l.N; ++n)
+                    l.child[fill[l.clus[n]]++] = n;
+            }
+            l.plane.assign((size_t)K * l.N, P4<R>{0, 0, 0, 0});
+            l.cost.assign((size_t)K * l.N, 0);
+            l.belief.assign((size_t)K * l.N, 0);
+            l.pid.assign(3 * (size_t)l.N, 0);
+            if (li + 1 < L)
+                for (int i = 0; i < HW; ++i)
+                    im_clus[i] = l.clus[im_clus[i]];
+        }
+        msg.assign((size_t)K * lv[0].E, 0);
+        msg_t.assign((size_t)K * lv[0].E, 0);
+        s_child.assign(lv[0].N, 0);
+        s_nb.assign(lv[0].N, 0);
+        s_ransac.assign(lv[0].N, 0);
+        order.assign((size_t)K * lv[0].N, 0);
+        plane_buf.assign((size_t)P * lv[0].N, P4<R>{0, 0, 0, 0});
+    }
+
+    bool step_done()
+    {
+        steps++;
+        if (max_steps >= 0 && steps >= max_steps)
+            stopped = true;
+        return stopped;
+    }
+
+    // hbp_g (hbp_isp.cu:1283-1311) with init_bp (:930-950).
+    void hbp_level(int li)
+    {
+        Level<R> &l = lv[li], &h = lv[li + 1];
+        std::fill(msg.begin(), msg.begin() + (size_t)K * l.E, (R)0);
+        for (int n = 0; n < l.N; ++n)
+            for (int p = 0; p < P; ++p)
+            {
+                P4<R> pr = h.plane[(size_t)p * h.N + l.clus[n]];
+                l.plane[(size_t)p * l.N + n] = pr;
+                l.plane[(size_t)(p + P) * l.N + n] = pr;
+                l.plane[(size_t)(p + 2 * P) * l.N + n] = pr;
+            }
+        plane_cost(l, 0);
+        plane_cost(l, P);
+        l.belief = l.cost;
+        for (int n = 0; n < l.N; ++n)
+        {
+            s_nb[n] = (uint32_t)l.nb_off[n];
+            s_ransac[n] = (uint32_t)l.pix_off[n];
+        }
+        for (int p = 0; p < h.N; ++p)
+            s_child[p] = (uint32_t)l.child_off[p];
+
+        const int iter_bp = 10 + 10 * li;
+        float max_dz = (float)D / 2.0f * (float)li / (float)L;
+        float max_dn = 1.0f * (float)li / (float)L;
+        for (int i = 0; i < iter_bp && !stopped; ++i)
+        {
+            int iter_random = (i <= iter_bp / 4 * 3) ? 4 : 5;
+            for (int it = 0;; ++it)
+            {
+                if (it <= 3)
+                    ransac(l);
+                else if (it <= 4)
+                    spatial(li);
+                else if (it <= iter_random && max_dz >= 0.01f)
+                {
+                    random_adjust(l, (R)max_dz, (R)max_dn);
+                    max_dz /= 2.0f;
+                    max_dn /= 2.0f;
+                }
+                else
+                    break;
+                plane_cost(l, 2 * P);
+                bp(l);
+                if (step_done())
+                    return;
+            }
+        }
+    }
+};
+
+template <typename R>
+int run(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+        const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
+        float tau_smooth, int min_level, long max_steps, float *disp, float *plane_out,
+        float *state_belief, float *state_plane)
+{
+    if (L < 1 || min_level < 0 || min_level > L - 1)
+        return -1;
+    Engine<R> eng;
+    eng.W = W;
+    eng.H = H;
+    eng.D = D;
+    eng.L = L;
+    eng.lambda = (R)alpha;
+    eng.tau = (R)25.0f;
+    eng.tau_smooth = (R)tau_smooth;
+    eng.vol = vol;
+    eng.wta = wta;
+    eng.max_steps = max_steps;
+    eng.setup(level_sizes, clus, mean, bd, bdl);
+    // top level: messages and beliefs zero, planes zero (never written by the
+    // reference, hbp_isp.cu:1333-1337)
+    int lm = min_level;
+    for (int li = L - 2; li >= min_level; --li)
+    {
+        eng.hbp_level(li);
+        if (eng.stopped)
+        {
+            lm = li;
+            break;
+        }
+    }
+    Level<R> &l = eng.lv[lm];
+    if (state_belief)
+        for (size_t i = 0; i < (size_t)K * l.N; ++i)
+            state_belief[i] = (float)l.belief[i];
+    if (state_plane)
+        for (size_t i = 0; i < (size_t)K * l.N; ++i)
+        {
+            state_plane[4 * i] = (float)l.plane[i].x;
+            state_plane[4 * i + 1] = (float)l.plane[i].y;
+            state_plane[4 * i + 2] = (float)l.plane[i].z;
+            state_plane[4 * i + 3] = (float)l.plane[i].w;
+        }
+    // map_msg (hbp_isp.cu:1081-1105): first slot among 0..3 holding the
+    // minimum belief; per pixel d = clamp(a*x + b*y + c, 0, D-1).
+    std::vector<P4<R>> best(l.N);
+    for (int n = 0; n < l.N; ++n)
+    {
+        R mn = l.belief[n];
+        for (int p = 1; p < P; ++p)
+            mn = std::min(mn, l.belief[(size_t)p * l.N + n]);
+        int mp = 0;
+        for (int p = 0; p < P; ++p)
+            if (l.belief[(size_t)p * l.N + n] == mn)
+            {
+                mp = p;
+                break;
+            }
+        best[n] = l.plane[(size_t)mp * l.N + n];
+    }
+    for (int k = 0; k < l.N; ++k)
+        for (int j = l.pix_off[k]; j < l.pix_off[k + 1]; ++j)
+        {
+            int px = l.pix[j];
+            const P4<R> &pl = best[k];
+            R x = (R)(px % W), y = (R)(px / W);
+            R d = pl.x * x + pl.y * y + pl.z;
+            d = std::fmin(std::fmax(d, (R)0), (R)(D - 1));
+            disp[px] = (float)d;
+            if (plane_out)
+            {
+                plane_out[3 * (size_t)px] = (float)pl.x;
+                plane_out[3 * (size_t)px + 1] = (float)pl.y;
+                plane_out[3 * (size_t)px + 2] = (float)pl.z;
+            }
+        }
+    return (int)eng.steps;
+}
+} // namespace
+
+extern "C" {
+
+// HBP_ISP(ISPData, StereoData, alpha, tau_smooth).run_ms(min_level)
+// (hbp_isp.hpp:288-386, hbp_isp.cu:1313-1346) on a segmentation pyramid in
+// the ISP layout of orc_segment, the u8 disparity-major cost volume and the
+// WTA disparity. fp64 != 0 selects the FP64 oracle. max_steps >= 0 stops after
+// that many candidate/BP steps and reports the current level's beliefs and
+// planes (K x N, plane as 4 floats) in state_*; otherwise those are filled
+// for min_level. Returns the number of BP steps run, or < 0 on bad input.
+int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+            const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
+            float alpha, float tau_smooth, int min_level, int fp64, long max_steps, float *disp,
+            float *plane, float *state_belief, float *state_plane)
+{
+    if (fp64)
+        return run<double>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha,
+                           tau_smooth, min_level, max_steps, disp, plane, state_belief,
+                           state_plane);
+    return run<float>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth,
+                      min_level, max_steps, disp, plane, state_belief, state_plane);
+}
+
+} // extern "C"

@@ -1,0 +1,199 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE: a CPU restatement of the reference HBP-ISP stereo path
+used to check the B200 engine. Only tests/, ``__graft_entry__.smoke()`` and
+bench.py's CPU-baseline / reference legs import this module; the engine never
+does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+P = C.c_void_p
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(P)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        _lib.orc_crtrees.restype = C.c_int
+        _lib.orc_crtrees_literal.restype = C.c_int
+        _lib.orc_segment.restype = C.c_int
+        _lib.orc_hbp.restype = C.c_int
+        _lib.orc_hbp.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
+                                 C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
+    return _lib
+
+
+def grey_u8(bgr: np.ndarray) -> np.ndarray:
+    bgr = np.ascontiguousarray(bgr, np.uint8)
+    out = np.zeros(bgr.shape[:2], np.uint8)
+    lib().orc_grey_u8(_p(bgr), int(bgr.shape[0] * bgr.shape[1]), _p(out))
+    return out
+
+
+def census(grey: np.ndarray) -> np.ndarray:
+    grey = np.ascontiguousarray(grey, np.uint8)
+    H, W = grey.shape
+    out = np.zeros((H, W), np.uint32)
+    lib().orc_census(_p(grey), W, H, _p(out))
+    return out
+
+
+def cost_volume(cL, cR, D):
+    H, W = cL.shape
+    vol = np.zeros((D, H * W), np.uint8)
+    wta = np.zeros((H, W), np.float32)
+    lib().orc_cost_volume(_p(np.ascontiguousarray(cL)), _p(np.ascontiguousarray(cR)), W, H, D, _p(vol), _p(wta))
+    return vol, wta
+
+
+def cost_to_right(volL, W, H, D):
+    volR = np.zeros_like(volL)
+    wta = np.zeros((H, W), np.float32)
+    lib().orc_cost_to_right(_p(np.ascontiguousarray(volL)), W, H, D, _p(volR), _p(wta))
+    return volR, wta
+
+
+def set_lab_overrides(keys: np.ndarray, vals: np.ndarray):
+    keys = np.ascontiguousarray(keys, np.uint32)
+    vals = np.ascontiguousarray(vals, np.float32)
+    order = np.argsort(keys)
+    keys, vals = keys[order], vals[order]
+    global _lab_keep
+    _lab_keep = (keys, vals)
+    lib().orc_lab_set_overrides(_p(keys), _p(vals), int(len(keys)))
+
+
+def lab(bgr: np.ndarray) -> np.ndarray:
+    bgr = np.ascontiguousarray(bgr, np.uint8)
+    H, W = bgr.shape[:2]
+    out = np.zeros((H, W, 4), np.float32)
+    lib().orc_lab(_p(bgr), H * W, _p(out))
+    return out
+
+
+def nn_grid(lab4: np.ndarray):
+    lab4 = np.ascontiguousarray(lab4, np.float32)
+    H, W = lab4.shape[:2]
+    nn = np.zeros(H * W, np.int32)
+    dmin = np.zeros(H * W, np.float32)
+    bd = np.zeros((H * W * 4, 2), np.int32)
+    lib().orc_nn_grid(_p(lab4), W, H, _p(nn), _p(dmin), _p(bd))
+    return nn, dmin, bd
+
+
+def crtrees(nn: np.ndarray, literal: bool = False):
+    nn = np.ascontiguousarray(nn, np.int32)
+    out = np.zeros_like(nn)
+    f = lib().orc_crtrees_literal if literal else lib().orc_crtrees
+    n = f(_p(nn), len(nn), _p(out))
+    return out, n
+
+
+def segment(lab4: np.ndarray) -> dict:
+    lab4 = np.ascontiguousarray(lab4, np.float32)
+    H, W = lab4.shape[:2]
+    n = H * W
+    sizes = np.zeros(2 * 64, np.int32)
+    clus = np.zeros(2 * n, np.int32)
+    mean = np.zeros(12 * n, np.float32)
+    bd = np.zeros(16 * n, np.int32)
+    bdl = np.zeros(8 * n, np.int32)
+    L = lib().orc_segment(_p(lab4), W, H, 64, _p(sizes), _p(clus), _p(mean), _p(bd), _p(bdl))
+    sizes = sizes[: 2 * L].reshape(L, 2)
+    tc, tb = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
+    return dict(level_sizes=sizes, clus=clus[:tc], mean=mean[: 6 * tc], bd=bd[: 2 * tb].reshape(tb, 2), bdl=bdl[:tb])
+
+
+def hbp(seg: dict, vol, wta, W, H, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False,
+        max_steps=-1):
+    """Returns (disparity HxW, plane HxWx3, steps, belief KxN, plane KxNx4)."""
+    sizes = np.ascontiguousarray(seg["level_sizes"], np.int32)
+    L = sizes.shape[0]
+    disp = np.zeros((H, W), np.float32)
+    plane = np.zeros((H, W, 3), np.float32)
+    nmax = int(sizes[:, 0].max())
+    sb = np.zeros(12 * nmax, np.float32)
+    sp = np.zeros(12 * nmax * 4, np.float32)
+    mean = np.ascontiguousarray(seg["mean"], np.float32).copy()
+    steps = lib().orc_hbp(_p(sizes), L, _p(np.ascontiguousarray(seg["clus"], np.int32)), _p(mean),
+                          _p(np.ascontiguousarray(seg["bd"], np.int32)),
+                          _p(np.ascontiguousarray(seg["bdl"], np.int32)),
+                          _p(np.ascontiguousarray(vol, np.uint8)), _p(np.ascontiguousarray(wta, np.float32)),
+                          W, H, D, alpha, tau_smooth, min_level, int(fp64), int(max_steps), _p(disp),
+                          _p(plane), _p(sb), _p(sp))
+    if steps < 0:
+        raise ValueError("oracle hbp rejected its input")
+    return disp, plane, steps, sb, sp
+
+
+def lr_check(dispL, dispR, planeL):
+    H, W = dispL.shape
+    pl = np.ascontiguousarray(planeL, np.float32).copy()
+    fail = np.zeros((H, W), np.uint8)
+    lib().orc_lr_check(_p(np.ascontiguousarray(dispL, np.float32)), _p(np.ascontiguousarray(dispR, np.float32)),
+                       _p(pl), W, H, _p(fail))
+    return pl, fail
+
+
+def plane_to_disp(plane):
+    H, W = plane.shape[:2]
+    d = np.zeros((H, W), np.float32)
+    lib().orc_plane_to_disp(_p(np.ascontiguousarray(plane, np.float32)), W, H, _p(d))
+    return d
+
+
+def weighted_median(bgr, fail, plane, stable=True):
+    H, W = fail.shape
+    pl = np.ascontiguousarray(plane, np.float32).copy()
+    lib().orc_weighted_median(_p(np.ascontiguousarray(bgr, np.uint8)), _p(np.ascontiguousarray(fail, np.uint8)),
+                              _p(pl), W, H, int(stable))
+    return pl
+
+
+def driver_median(disp):
+    d = np.ascontiguousarray(disp, np.float32).copy()
+    H, W = d.shape
+    lib().orc_driver_median(_p(d), W, H)
+    return d
+
+
+def cost_stage(L, R, D):
+    """grey -> census -> volume/WTA for a BGR pair (the StereoCost Census path)."""
+    gL, gR = grey_u8(L), grey_u8(R)
+    cL, cR = census(gL), census(gR)
+    vol, wta = cost_volume(cL, cR, D)
+    return dict(greyL=gL, greyR=gR, censusL=cL, censusR=cR, vol=vol, wta=wta)
+
+
+def pipeline(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False, right_view=False):
+    """The single-pair path of main_stereo_hbp_isp.cu:33-72 (without the driver
+    median); right_view selects the right-view path of main_bench_middv3.cu:189-203."""
+    H, W = L.shape[:2]
+    cs = cost_stage(L, R, D)
+    vol, wta = cs["vol"], cs["wta"]
+    if right_view:
+        vol, wta = cost_to_right(vol, W, H, D)
+    seg = segment(lab(R if right_view else L))
+    disp, plane, steps, _, _ = hbp(seg, vol, wta, W, H, D, alpha, tau_smooth, min_level, fp64)
+    return dict(disp=disp, plane=plane, steps=steps, seg=seg, wta=wta, vol=vol)

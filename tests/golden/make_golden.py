@@ -1,0 +1,248 @@
+"""Generate the golden fixtures in tests/golden/ by running the reference's own
+CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
+synthetic scenes. It needs a GPU; run it on a B200 box:
+
+    python tests/golden/make_golden.py --out <dir>
+
+and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
+outputs for every stage of the stereo path at small sizes (full arrays) and at
+the 450x375, D=64 single-pair configuration (hashes, WTA, level-1 labels,
+disparity). The reference library is only read here and by the GPU parity
+tests; the product never loads it.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "hbp-isp_b200"))
+from scenes import make_scene  # noqa: E402
+
+P = C.c_void_p
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(P)
+
+
+class RefLib:
+    """ctypes binding of oracle/ref/ref_harness.cu."""
+
+    def __init__(self, path: str | None = None):
+        path = path or os.path.join(ROOT, "oracle", "_ref", "libhbpref.so")
+        self.lib = C.CDLL(path)
+        for name in ("ref_grey", "ref_lab", "ref_1nn_grid", "ref_crtrees", "ref_cost",
+                     "ref_segment", "ref_hbp_pair", "ref_post"):
+            getattr(self.lib, name).restype = C.c_int
+        self.lib.ref_hbp_pair.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                          C.c_int, C.c_int, P, P]
+
+    def grey(self, bgr):
+        H, W, _ = bgr.shape
+        f = np.zeros((H, W), np.float32)
+        u = np.zeros((H, W), np.uint8)
+        rc = self.lib.ref_grey(ptr(bgr), W, H, ptr(f), ptr(u))
+        assert rc == 0, rc
+        return f, u
+
+    def lab(self, bgr):
+        H, W, _ = bgr.shape
+        out = np.zeros((H, W, 4), np.float32)
+        rc = self.lib.ref_lab(ptr(bgr), W, H, ptr(out))
+        assert rc == 0, rc
+        return out
+
+    def nn_grid(self, lab4):
+        H, W, _ = lab4.shape
+        nn = np.zeros(H * W, np.int32)
+        dmin = np.zeros(H * W, np.float32)
+        d4 = np.full(H * W * 4, np.nan, np.float32)
+        rc = self.lib.ref_1nn_grid(ptr(np.ascontiguousarray(lab4)), W, H, ptr(nn), ptr(dmin), ptr(d4))
+        assert rc == 0, rc
+        return nn, dmin, d4.reshape(H * W, 4)
+
+    def crtrees(self, nn):
+        nn = np.ascontiguousarray(nn, np.int32)
+        clus = np.zeros_like(nn)
+        n = self.lib.ref_crtrees(ptr(nn), len(nn), ptr(clus))
+        assert n >= 0, n
+        return clus, n
+
+    def cost(self, L, R, D, to_right=False):
+        H, W, _ = L.shape
+        Da = (D + 31) // 32 * 32
+        out = dict(
+            greyL=np.zeros((H, W), np.uint8), greyR=np.zeros((H, W), np.uint8),
+            censusL=np.zeros((H, W), np.uint32), censusR=np.zeros((H, W), np.uint32),
+            vol_u8=np.zeros((H * W, Da), np.uint8), vol_f32=np.zeros((D, H * W), np.float32),
+            wta=np.zeros((H, W), np.float32))
+        rc = self.lib.ref_cost(ptr(L), ptr(R), W, H, D, int(to_right), ptr(out["greyL"]),
+                               ptr(out["greyR"]), ptr(out["censusL"]), ptr(out["censusR"]),
+                               ptr(out["vol_u8"]), ptr(out["vol_f32"]), ptr(out["wta"]))
+        assert rc == 0, rc
+        return out
+
+    def segment(self, bgr):
+        H, W, _ = bgr.shape
+        n = H * W
+        sizes = np.zeros(2 * 64, np.int32)
+        clus = np.zeros(2 * n, np.int32)
+        mean = np.zeros(12 * n, np.float32)
+        bd = np.zeros(16 * n, np.int32)
+        bdl = np.zeros(8 * n, np.int32)
+        L = self.lib.ref_segment(ptr(bgr), W, H, 64, ptr(sizes), ptr(clus), ptr(mean), ptr(bd), ptr(bdl))
+        assert L > 0, L
+        sizes = sizes[: 2 * L].reshape(L, 2)
+        tc, tb = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
+        return dict(level_sizes=sizes, clus=clus[:tc], mean=mean[: 6 * tc], bd=bd[: 2 * tb].reshape(tb, 2),
+                    bdl=bdl[:tb])
+
+    def hbp_pair(self, L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, right_view=False):
+        H, W, _ = L.shape
+        disp = np.zeros((H, W), np.float32)
+        plane = np.zeros((H, W, 3), np.float32)
+        levels = self.lib.ref_hbp_pair(ptr(L), ptr(R), W, H, D, alpha, tau_smooth, min_level,
+                                       int(right_view), ptr(disp), ptr(plane))
+        assert levels > 0, levels
+        return disp, plane, levels
+
+    def post(self, L, R, dispL, planeL, dispR, planeR, median=True):
+        H, W, _ = L.shape
+        dL, pL = dispL.copy(), planeL.copy()
+        rc = self.lib.ref_post(ptr(L), ptr(R), W, H, ptr(dL), ptr(pL), ptr(np.ascontiguousarray(dispR)),
+                               ptr(np.ascontiguousarray(planeR)), int(median))
+        assert rc == 0, rc
+        return dL, pL
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def random_graphs(seed: int = 4242):
+    """Functional graphs (every node has exactly one successor) of several shapes."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    graphs = []
+    for N in (1, 2, 3, 5, 8, 17, 64, 257, 1000, 4096):
+        graphs.append(rng.integers(0, N, N).astype(np.int32))  # uniform successor
+    for N in (10, 100, 1000):
+        g = np.arange(1, N + 1, dtype=np.int32)  # one long chain ending in a self-loop
+        g[-1] = N - 1
+        graphs.append(g)
+        graphs.append(np.zeros(N, np.int32))  # star into node 0
+        perm = rng.permutation(N).astype(np.int32)  # a permutation: cycles only
+        graphs.append(perm)
+    for N in (500, 3000):
+        # 1-NN graph of random points on a line with mutual-pair cycles and trees
+        x = np.sort(rng.uniform(0, 1, N))
+        left = np.r_[np.inf, np.diff(x)]
+        right = np.r_[np.diff(x), np.inf]
+        idx = np.arange(N)
+        graphs.append(np.where(left < right, idx - 1, idx + 1).astype(np.int32))
+    for N in (300, 2000):
+        # random trees hanging on a few cycles of length 1..6
+        g = np.empty(N, np.int32)
+        k = 0
+        while k < N:
+            L = int(rng.integers(1, 7))
+            L = min(L, N - k)
+            g[k:k + L] = np.r_[np.arange(k + 1, k + L), k]
+            k += L
+            if k < N:
+                m = min(int(rng.integers(5, 40)), N - k)
+                g[k:k + m] = rng.integers(0, k, m)
+                k += m
+        graphs.append(g)
+    return graphs
+
+
+def random_lab(seed: int = 99) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lab_rand = np.zeros((128, 192, 4), np.float32)
+    lab_rand[..., 0] = rng.uniform(0, 100, (128, 192))
+    lab_rand[..., 1:3] = rng.uniform(-90, 90, (128, 192, 2))
+    lab_rand[..., 3] = 1
+    lab_rand[40:60, 40:60, :3] = np.round(lab_rand[40:60, 40:60, :3])  # exact ties
+    return lab_rand
+
+
+def scene_record(ref: RefLib, W, H, D, seed, full: bool):
+    s = make_scene(W, H, D, seed)
+    L, R = s.left, s.right
+    rec = dict(W=W, H=H, D=D, seed=seed, left=L, right=R)
+    cost = ref.cost(L, R, D)
+    costR = ref.cost(L, R, D, to_right=True)
+    lab = ref.lab(L)
+    nn, dmin, d4 = ref.nn_grid(lab)
+    seg = ref.segment(L)
+    n1 = int(seg["level_sizes"][0, 0])
+    clus1 = seg["clus"][:n1]
+    disp, plane, levels = ref.hbp_pair(L, R, D)
+    dispR, planeR, levelsR = ref.hbp_pair(L, R, D, right_view=True)
+    post_d, post_p = ref.post(L, R, disp, plane, dispR, planeR, median=True)
+    lr_d, lr_p = ref.post(L, R, disp, plane, dispR, planeR, median=False)
+    rec.update(
+        sha_greyL=sha(cost["greyL"]), sha_greyR=sha(cost["greyR"]),
+        sha_censusL=sha(cost["censusL"]), sha_censusR=sha(cost["censusR"]),
+        sha_vol_u8=sha(cost["vol_u8"]), sha_vol_f32=sha(cost["vol_f32"]),
+        sha_lab=sha(lab), sha_nn=sha(nn),
+        wta=cost["wta"].astype(np.uint16), wta_right=costR["wta"].astype(np.uint16),
+        sha_vol_right=sha(costR["vol_f32"]),
+        level_sizes=seg["level_sizes"], clus1=clus1, sha_clus1=sha(clus1),
+        disp=disp, disp_right=dispR, levels=levels, levels_right=levelsR,
+        post_disp=post_d, lr_disp=lr_d,
+    )
+    if full:
+        rec.update(
+            greyL=cost["greyL"], greyR=cost["greyR"], censusL=cost["censusL"], censusR=cost["censusR"],
+            lab=lab, nn=nn, dist_min=dmin,
+            dist4=d4, seg_clus=seg["clus"], seg_mean=seg["mean"], seg_bd=seg["bd"], seg_bdl=seg["bdl"],
+            plane=plane, plane_right=planeR, post_plane=post_p, lr_plane=lr_p,
+        )
+    return rec
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--lib", default=None)
+    args = ap.parse_args()
+    os.makedirs(args.out, exist_ok=True)
+    ref = RefLib(args.lib)
+
+    for (W, H, D, seed, full, name) in [
+        (96, 64, 32, 7, True, "tiny_96x64_d32_s7"),
+        (160, 120, 48, 11, True, "small_160x120_d48_s11"),
+        (450, 375, 64, 1000, False, "c1_450x375_d64_s1000"),
+    ]:
+        rec = scene_record(ref, W, H, D, seed, full)
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
+        print(name, "levels", rec["levels"], rec["levels_right"], "sizes", rec["level_sizes"][:, 0].tolist())
+
+    graphs = random_graphs()
+    outs, nums = [], []
+    for g in graphs:
+        c, n = ref.crtrees(g)
+        outs.append(c)
+        nums.append(n)
+    np.savez_compressed(os.path.join(args.out, "crtrees_graphs.npz"),
+                        **{f"g{i}": g for i, g in enumerate(graphs)},
+                        **{f"c{i}": c for i, c in enumerate(outs)}, nums=np.array(nums, np.int32))
+    print("crtrees graphs", len(graphs), "clusters", nums)
+
+    # Random LAB images exercise the pixel 1-NN distance arithmetic over a wide
+    # range of values (used to pin the floating-point evaluation order).
+    nn, dmin, d4 = ref.nn_grid(random_lab())
+    # the random LAB image is regenerated from its seed by the tests
+    np.savez_compressed(os.path.join(args.out, "nn_grid_random.npz"), nn=nn, dist_min=dmin, dist4=d4)
+    print("done")
+
+
+if __name__ == "__main__":
+    main()
