@@ -1,0 +1,494 @@
+// C ABI of the engine (include/hbp_b200.h): context, device arena, the
+// single-pair pipeline and the stage entry points.
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "engine.h"
+
+namespace hbp
+{
+void Arena::init(size_t bytes)
+{
+    release();
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        throw StatusError{HBP_ERR_OUT_OF_MEMORY, "device slab allocation failed"};
+    }
+    base = static_cast<char *>(p);
+    cap = bytes;
+    off = 0;
+    owned = true;
+}
+
+void Arena::attach(void *p, size_t bytes)
+{
+    release();
+    base = static_cast<char *>(p);
+    cap = bytes;
+    off = 0;
+    owned = false;
+}
+
+void Arena::release()
+{
+    if (owned && base)
+        cudaFree(base);
+    base = nullptr;
+    cap = off = 0;
+    owned = false;
+}
+
+void *Arena::raw(size_t bytes, size_t align)
+{
+    size_t o = (off + align - 1) / align * align;
+    if (o + bytes > cap)
+        throw StatusError{HBP_ERR_OUT_OF_MEMORY, "device slab exhausted"};
+    off = o + bytes;
+    return base + o;
+}
+} // namespace hbp
+
+using namespace hbp;
+
+struct hbp_ctx
+{
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Arena arena; // pipeline buffers and pyramid
+    Arena tmp;   // scratch of sorts / scans / segmentation
+    Pyramid pyr;
+    bool have_pyr = false;
+    int *err_dev = nullptr;
+    float *wtab = nullptr; // weighted-median weight table (766 floats)
+    long cap_pixels = 0;
+    int cap_disp = 0;
+};
+
+namespace
+{
+thread_local std::string g_err;
+
+hbp_status fail(hbp_status s, const std::string &msg)
+{
+    g_err = msg;
+    return s;
+}
+
+template <typename F>
+hbp_status guarded(F &&f)
+{
+    try
+    {
+        f();
+        return HBP_OK;
+    }
+    catch (const CudaFailure &e)
+    {
+        return fail(HBP_ERR_CUDA, std::string("CUDA error ") + cudaGetErrorString(e.err) + " at " +
+                                      e.file + ":" + std::to_string(e.line));
+    }
+    catch (const StatusError &e)
+    {
+        return fail(e.st, e.what);
+    }
+    catch (const std::bad_alloc &)
+    {
+        return fail(HBP_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    catch (const std::exception &e)
+    {
+        return fail(HBP_ERR_INTERNAL, e.what());
+    }
+}
+
+size_t slab_bytes(long pixels, int D)
+{
+    return (size_t)pixels * (size_t)(2 * (D + 16) + 1200) + ((size_t)96 << 20);
+}
+size_t tmp_bytes(long pixels) { return (size_t)pixels * 480 + ((size_t)64 << 20); }
+
+void ensure_capacity(hbp_ctx *c, long pixels, int D)
+{
+    if (pixels <= c->cap_pixels && D <= c->cap_disp)
+        return;
+    long np = std::max(pixels, c->cap_pixels);
+    int nd = std::max(D, c->cap_disp);
+    HBP_CUDA(cudaSetDevice(c->device));
+    HBP_CUDA(cudaStreamSynchronize(c->st));
+    c->have_pyr = false;
+    c->arena.init(slab_bytes(np, nd));
+    c->tmp.init(tmp_bytes(np));
+    c->cap_pixels = np;
+    c->cap_disp = nd;
+}
+
+void check_device_error(hbp_ctx *c)
+{
+    int h = 0;
+    HBP_CUDA(cudaMemcpyAsync(&h, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    HBP_CUDA(cudaStreamSynchronize(c->st));
+    if (h == DERR_BARRIER_TIMEOUT)
+        throw StatusError{HBP_ERR_TIMEOUT, "a grid barrier timed out"};
+    if (h == DERR_NO_CONVERGENCE)
+        throw StatusError{HBP_ERR_NO_CONVERGENCE, "CRTrees did not converge within its bound"};
+    if (h != 0)
+        throw StatusError{HBP_ERR_INTERNAL, "device error word set"};
+}
+
+cudaStream_t pick(hbp_ctx *c, void *s) { return s ? (cudaStream_t)s : c->st; }
+
+void check_dims(int W, int H, int D)
+{
+    if (W < 16 || H < 16 || W > 65535 || H > 65535 || D < 2 || D > 1024 || D >= W)
+        throw StatusError{HBP_ERR_INVALID_ARG, "need 16 <= W,H <= 65535 and 2 <= D <= min(1024, W-1)"};
+}
+
+HbpParams to_params(const hbp_params *p)
+{
+    HbpParams q;
+    if (p)
+    {
+        q.alpha = p->alpha;
+        q.tau_smooth = p->tau_smooth;
+        q.min_level = p->min_level;
+        q.msg_fp16 = p->msg_fp16;
+    }
+    return q;
+}
+} // namespace
+
+extern "C" {
+
+void hbp_default_params(hbp_params *p)
+{
+    if (!p)
+        return;
+    p->alpha = 1000.1f;
+    p->tau_smooth = 0.6f;
+    p->min_level = 2;
+    p->msg_fp16 = 0;
+    p->post = 1;
+}
+
+const char *hbp_status_string(hbp_status s)
+{
+    switch (s)
+    {
+    case HBP_OK: return "ok";
+    case HBP_ERR_INVALID_ARG: return "invalid argument";
+    case HBP_ERR_OUT_OF_MEMORY: return "out of memory";
+    case HBP_ERR_ADMISSION_REJECTED: return "admission rejected";
+    case HBP_ERR_NO_CONVERGENCE: return "no convergence";
+    case HBP_ERR_CUDA: return "CUDA error";
+    case HBP_ERR_TIMEOUT: return "timeout";
+    case HBP_ERR_NOT_READY: return "not ready";
+    case HBP_ERR_INTERNAL: return "internal error";
+    }
+    return "unknown status";
+}
+
+const char *hbp_last_error(void) { return g_err.c_str(); }
+
+hbp_status hbp_ctx_create(int device, long max_pixels, int max_disp, hbp_ctx **out)
+{
+    if (!out || max_pixels < 0 || max_disp < 0)
+        return fail(HBP_ERR_INVALID_ARG, "bad context arguments");
+    *out = nullptr;
+    hbp_ctx *c = new (std::nothrow) hbp_ctx;
+    if (!c)
+        return fail(HBP_ERR_OUT_OF_MEMORY, "host allocation failed");
+    hbp_status s = guarded([&] {
+        c->device = device;
+        HBP_CUDA(cudaSetDevice(device));
+        HBP_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        HBP_CUDA(cudaMalloc(&c->err_dev, sizeof(int) * 4));
+        HBP_CUDA(cudaMemset(c->err_dev, 0, sizeof(int) * 4));
+        float tab[766];
+        median_weight_table(tab);
+        HBP_CUDA(cudaMalloc(&c->wtab, sizeof(tab)));
+        HBP_CUDA(cudaMemcpy(c->wtab, tab, sizeof(tab), cudaMemcpyHostToDevice));
+        if (max_pixels > 0)
+            ensure_capacity(c, max_pixels, max_disp > 0 ? max_disp : 256);
+    });
+    if (s != HBP_OK)
+    {
+        hbp_ctx_destroy(c);
+        return s;
+    }
+    *out = c;
+    return HBP_OK;
+}
+
+void hbp_ctx_destroy(hbp_ctx *c)
+{
+    if (!c)
+        return;
+    cudaSetDevice(c->device);
+    if (c->st)
+        cudaStreamSynchronize(c->st);
+    c->arena.release();
+    c->tmp.release();
+    if (c->err_dev)
+        cudaFree(c->err_dev);
+    if (c->wtab)
+        cudaFree(c->wtab);
+    if (c->st)
+        cudaStreamDestroy(c->st);
+    delete c;
+}
+
+void *hbp_ctx_stream(hbp_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+int hbp_volume_pitch(int W) { return volume_pitch(W); }
+
+hbp_status hbp_cost_census_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
+                             uint32_t *censusL, uint32_t *censusR, uint8_t *vol, float *wta,
+                             uint8_t *volR, float *wtaR, void *stream)
+{
+    if (!c || !bgrL || !bgrR || !censusL || !censusR || !vol || !wta || (!volR) != (!wtaR))
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, D);
+        HBP_CUDA(cudaSetDevice(c->device));
+        launch_cost(bgrL, bgrR, W, H, D, censusL, censusR, vol, wta, volR, wtaR, pick(c, stream));
+    });
+}
+
+hbp_status hbp_lab_d(hbp_ctx *c, const uint8_t *bgr, long n, float *lab4, void *stream)
+{
+    if (!c || !bgr || !lab4 || n <= 0 || n > (1l << 31) - 1)
+        return fail(HBP_ERR_INVALID_ARG, "bad arguments");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        launch_lab(bgr, (int)n, (float4 *)lab4, pick(c, stream));
+    });
+}
+
+hbp_status hbp_crtrees_d(hbp_ctx *c, const int *nn, int N, int *clus, int *num_clusters, void *stream)
+{
+    if (!c || !nn || !clus || !num_clusters || N <= 0)
+        return fail(HBP_ERR_INVALID_ARG, "bad arguments");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, std::max<long>(N, c->cap_pixels), std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        // every successor must name a node: check on the host before launching
+        std::vector<int> h(N);
+        HBP_CUDA(cudaMemcpyAsync(h.data(), nn, sizeof(int) * N, cudaMemcpyDeviceToHost, st));
+        HBP_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < N; ++i)
+            if (h[i] < 0 || h[i] >= N)
+                throw StatusError{HBP_ERR_INVALID_ARG, "successor out of range"};
+        c->tmp.reset();
+        HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
+        int *num_dev = c->tmp.alloc<int>(1);
+        crtrees_labels(nn, N, clus, num_dev, c->err_dev, c->tmp, st);
+        HBP_CUDA(cudaMemcpyAsync(num_clusters, num_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+        HBP_CUDA(cudaStreamSynchronize(st));
+        int herr = 0;
+        HBP_CUDA(cudaMemcpy(&herr, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr)
+            throw StatusError{HBP_ERR_NO_CONVERGENCE, "CRTrees gave up"};
+    });
+}
+
+hbp_status hbp_segment_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int *levels, void *stream)
+{
+    if (!c || !bgr || !levels)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 16);
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        c->arena.reset();
+        c->tmp.reset();
+        HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
+        c->have_pyr = false;
+        segment_image(bgr, W, H, c->pyr, c->arena, c->tmp, c->err_dev, st);
+        check_device_error(c);
+        c->have_pyr = true;
+        *levels = c->pyr.L;
+    });
+}
+
+hbp_status hbp_pyramid_levels(hbp_ctx *c, int *sizes, int max_levels)
+{
+    if (!c || !sizes || !c->have_pyr)
+        return fail(HBP_ERR_INVALID_ARG, "no pyramid");
+    for (int l = 0; l < c->pyr.L && l < max_levels; ++l)
+    {
+        sizes[2 * l] = c->pyr.N[l];
+        sizes[2 * l + 1] = c->pyr.E[l];
+    }
+    return HBP_OK;
+}
+
+hbp_status hbp_pyramid_copy(hbp_ctx *c, int *clus, float *mean, int *bd, int *bdl)
+{
+    if (!c || !c->have_pyr)
+        return fail(HBP_ERR_INVALID_ARG, "no pyramid");
+    return guarded([&] {
+        size_t tn = 0, te = 0;
+        for (int l = 0; l < c->pyr.L; ++l)
+        {
+            tn += c->pyr.N[l];
+            te += c->pyr.E[l];
+        }
+        HBP_CUDA(cudaStreamSynchronize(c->st));
+        if (clus)
+            HBP_CUDA(cudaMemcpy(clus, c->pyr.clus, sizeof(int) * tn, cudaMemcpyDeviceToHost));
+        if (mean)
+            HBP_CUDA(cudaMemcpy(mean, c->pyr.sums, sizeof(float) * 6 * tn, cudaMemcpyDeviceToHost));
+        if (bd)
+            HBP_CUDA(cudaMemcpy(bd, c->pyr.bd, sizeof(int2) * te, cudaMemcpyDeviceToHost));
+        if (bdl)
+            HBP_CUDA(cudaMemcpy(bdl, c->pyr.bdl, sizeof(int) * te, cudaMemcpyDeviceToHost));
+    });
+}
+
+hbp_status hbp_infer_d(hbp_ctx *c, const uint8_t *vol, const float *wta, int D, const hbp_params *prm,
+                       float *disp, float *plane, void *stream)
+{
+    if (!c || !vol || !wta || !disp || !c->have_pyr)
+        return fail(HBP_ERR_INVALID_ARG, "bad arguments or no pyramid");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        check_dims(c->pyr.W, c->pyr.H, D);
+        cudaStream_t st = pick(c, stream);
+        HbpParams q = to_params(prm);
+        c->tmp.reset();
+        hbp_infer(c->pyr, vol, volume_pitch(c->pyr.W), wta, D, q, disp, plane, c->tmp, st);
+    });
+}
+
+hbp_status hbp_lr_check_d(hbp_ctx *c, const float *dispL, const float *dispR, float *planeL,
+                          uint8_t *fail_mask, float *disp_out, int W, int H, void *stream)
+{
+    if (!c || !dispL || !dispR || !planeL || !fail_mask)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 2);
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        c->tmp.reset();
+        uint8_t *fail2 = c->tmp.alloc<uint8_t>((size_t)W * H);
+        launch_lr_check(dispL, dispR, planeL, fail_mask, fail2, W, H, st);
+        if (disp_out)
+            launch_plane_to_disp(planeL, disp_out, W, H, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_weighted_median_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *fail_mask,
+                                 float *plane, float *disp_out, int W, int H, void *stream)
+{
+    if (!c || !bgrL || !fail_mask || !plane)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 2);
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        c->tmp.reset();
+        float *copy = c->tmp.alloc<float>(3 * (size_t)W * H);
+        HBP_CUDA(cudaMemcpyAsync(copy, plane, sizeof(float) * 3 * W * H, cudaMemcpyDeviceToDevice, st));
+        launch_weighted_median(bgrL, fail_mask, copy, plane, W, H, c->wtab, c->tmp, st);
+        if (disp_out)
+            launch_plane_to_disp(plane, disp_out, W, H, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_driver_median_d(hbp_ctx *c, float *disp, int W, int H, void *stream)
+{
+    if (!c || !disp)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 2);
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        c->tmp.reset();
+        float *t = c->tmp.alloc<float>((size_t)W * H);
+        launch_driver_median(disp, t, W, H, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_run_pair(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
+                        const hbp_params *prm, float *disp_h, float *plane_h)
+{
+    if (!c || !bgrL || !bgrR || !disp_h)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    hbp_params def;
+    hbp_default_params(&def);
+    const hbp_params &p = prm ? *prm : def;
+    if (p.post < 0 || p.post > 2)
+        return fail(HBP_ERR_INVALID_ARG, "post must be 0, 1 or 2");
+    return guarded([&] {
+        check_dims(W, H, D);
+        HBP_CUDA(cudaSetDevice(c->device));
+        const long n = (long)W * H;
+        ensure_capacity(c, n, D);
+        cudaStream_t st = c->st;
+        Arena &a = c->arena;
+        a.reset();
+        c->tmp.reset();
+        c->have_pyr = false;
+        HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
+        const int Wp = volume_pitch(W);
+        const bool lr = p.post == 2;
+        uint8_t *dL = a.alloc<uint8_t>(3 * n), *dR = a.alloc<uint8_t>(3 * n);
+        uint32_t *cL = a.alloc<uint32_t>(n), *cR = a.alloc<uint32_t>(n);
+        uint8_t *vol = a.alloc<uint8_t>((size_t)D * H * Wp);
+        uint8_t *volR = lr ? a.alloc<uint8_t>((size_t)D * H * Wp) : nullptr;
+        float *wta = a.alloc<float>(n), *wtaR = lr ? a.alloc<float>(n) : nullptr;
+        float *disp = a.alloc<float>(n), *plane = a.alloc<float>(3 * n);
+        HBP_CUDA(cudaMemcpyAsync(dL, bgrL, 3 * n, cudaMemcpyHostToDevice, st));
+        HBP_CUDA(cudaMemcpyAsync(dR, bgrR, 3 * n, cudaMemcpyHostToDevice, st));
+        launch_cost(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR, st);
+        HbpParams q = to_params(&p);
+        size_t m = a.mark();
+        segment_image(dL, W, H, c->pyr, a, c->tmp, c->err_dev, st);
+        check_device_error(c);
+        c->tmp.reset();
+        hbp_infer(c->pyr, vol, Wp, wta, D, q, disp, plane, c->tmp, st);
+        if (lr)
+        {
+            a.rewind(m);
+            float *dispR = a.alloc<float>(n), *planeR = a.alloc<float>(3 * n);
+            uint8_t *fail1 = a.alloc<uint8_t>(n), *fail2 = a.alloc<uint8_t>(n);
+            float *plane2 = a.alloc<float>(3 * n);
+            Pyramid pr;
+            c->tmp.reset();
+            segment_image(dR, W, H, pr, a, c->tmp, c->err_dev, st);
+            check_device_error(c);
+            c->tmp.reset();
+            hbp_infer(pr, volR, Wp, wtaR, D, q, dispR, planeR, c->tmp, st);
+            launch_lr_check(disp, dispR, plane, fail1, fail2, W, H, st);
+            c->tmp.reset();
+            launch_weighted_median(dL, fail1, plane, plane2, W, H, c->wtab, c->tmp, st);
+            launch_plane_to_disp(plane2, disp, W, H, st);
+            plane = plane2;
+        }
+        else if (p.post == 1)
+        {
+            float *t = c->tmp.alloc<float>(n);
+            launch_driver_median(disp, t, W, H, st);
+        }
+        HBP_CUDA(cudaMemcpyAsync(disp_h, disp, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+        if (plane_h)
+            HBP_CUDA(cudaMemcpyAsync(plane_h, plane, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,122 @@
+// Internal interfaces of the B200 HBP-ISP engine (not part of the C-ABI).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hbp
+{
+
+constexpr int P = 4, K = 12;       // particles per slot group, slots per node
+constexpr int PC_CHUNK = 256;      // plane-cost chunk (32 slots x 8 deep)
+constexpr float CENSUS_TAU = 25.0f; // stereo_cost.cu:433
+
+// ---------------------------------------------------------------------------
+// Device memory: one slab per pair, carved with a bump allocator (no
+// cudaMalloc inside a request once the slab exists).
+struct Arena
+{
+    char *base = nullptr;
+    size_t cap = 0, off = 0;
+    bool owned = false;
+
+    void init(size_t bytes);
+    void attach(void *p, size_t bytes);
+    void release();
+    void reset() { off = 0; }
+    void *raw(size_t bytes, size_t align = 256);
+    template <typename T>
+    T *alloc(size_t n)
+    {
+        return static_cast<T *>(raw(sizeof(T) * (n ? n : 1)));
+    }
+    size_t mark() const { return off; }
+    void rewind(size_t m) { off = m; }
+};
+
+// Temporary device memory for scans/sorts, reused across calls on one stream.
+struct Scratch
+{
+    Arena *arena;
+};
+
+// ---------------------------------------------------------------------------
+// cost.cu
+int volume_pitch(int W);
+void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
+                 uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
+                 cudaStream_t st);
+
+// lab.cu
+void launch_lab(const uint8_t *bgr, int n, float4 *lab, cudaStream_t st);
+
+// scan_sort.cu
+size_t scan_scratch_bytes(long n);
+void exclusive_scan(const int *in, int *out, long n, int *total_dev, Arena &tmp, cudaStream_t st);
+// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of the
+// keys; results land in keys/vals (ping-pong through alt buffers).
+void radix_sort_pairs_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt, uint32_t *vals_alt,
+                          long n, int bits, Arena &tmp, cudaStream_t st);
+void radix_sort_keys_u64(uint64_t *keys, uint64_t *keys_alt, long n, int bits, Arena &tmp,
+                         cudaStream_t st);
+
+// crtrees.cu: component labels (0..n-1 in label order); returns the count
+// through num_dev (device int). err_dev receives DeviceErr codes.
+void crtrees_labels(const int *nn, int N, int *clus, int *num_dev, int *err_dev, Arena &tmp,
+                    cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Segmentation pyramid in the reference's ISP layout (segment.cu:884-905),
+// device resident.
+struct Pyramid
+{
+    int W = 0, H = 0, L = 0;
+    std::vector<int> N, E;                  // per level
+    std::vector<size_t> node_off, edge_off; // offsets into the concatenated arrays
+    std::vector<size_t> child_base, nb_base;
+    int *clus = nullptr;   // sum N: node -> parent
+    float *sums = nullptr; // 6 * sum N (per level channel-major: L, a, b, x, y, count)
+    int2 *bd = nullptr;    // sum E: (source, target), sorted by source
+    int *bdl = nullptr;    // sum E: boundary lengths
+    // derived per level: children grouped by parent (increasing child index)
+    // with offsets per parent, and CSR offsets of the edges by source
+    uint32_t *child = nullptr; // sum N
+    int *child_off = nullptr;  // per level N_{l+1} + 1 at child_base[l]
+    int *nb_off = nullptr;     // per level N_l + 1 at nb_base[l]
+};
+
+// segment.cu: SegHAC::run_ms with CentroidLink / 4-grid / sigma 0. Uses `a`
+// for the pyramid and `tmp` for temporaries; the host learns each level's size
+// (one small device-to-host read per level).
+void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
+                   int *err_dev, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// hbp.cu
+struct HbpParams
+{
+    float alpha = 1000.1f;
+    float tau_smooth = 0.6f;
+    int min_level = 2;
+    int msg_fp16 = 0;
+};
+
+// HBP_ISP::run_ms on one pyramid: disp (HW floats) and plane (HW x 3).
+void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta, int D,
+               const HbpParams &prm, float *disp, float *plane, Arena &a, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// post.cu
+void launch_lr_check(const float *dispL, const float *dispR, float *planeL, uint8_t *fail,
+                     uint8_t *fail2, int W, int H, cudaStream_t st);
+void launch_plane_to_disp(const float *plane, float *disp, int W, int H, cudaStream_t st);
+void median_weight_table(float *host766);
+void launch_weighted_median(const uint8_t *bgr, const uint8_t *fail, const float *plane_in,
+                            float *plane_out, int W, int H, const float *wtab, Arena &tmp,
+                            cudaStream_t st);
+void launch_driver_median(float *disp, float *tmp, int W, int H, cudaStream_t st);
+
+} // namespace hbp

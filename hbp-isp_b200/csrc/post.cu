@@ -1,0 +1,330 @@
+// Post-processing: left-right check with nearest-neighbour plane fill,
+// colour-weighted median over planes, plane -> disparity, and the single-pair
+// driver's 7-tap separable median. Reference: PostProcess (post_process.cu:
+// 4-185, :373-390; CPU/OpenMP there) and medianFilter
+// (main_stereo_hbp_isp.cu:120-192).
+#include <cfloat>
+#include <cmath>
+
+#include "engine.h"
+
+namespace hbp
+{
+namespace
+{
+__device__ __forceinline__ float get_z(const float *v, int x, int y)
+{
+    return v[0] * (float)x + v[1] * (float)y + v[2];
+}
+
+// doConsistencyCheck (post_process.cu:4-41), left view: fail where the right
+// disparity at int(x - d + 0.5f) differs by more than 1.5.
+__global__ void lr_fail_kernel(const float *dispL, const float *dispR, int W, int H, uint8_t *fail)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H)
+        return;
+    int y = i / W, x = i - y * W;
+    float ds = dispL[i];
+    uint8_t f = 0;
+    if (ds == ds)
+    {
+        int rx = (int)((float)x - ds * 1.0f + 0.5f);
+        if (rx >= 0 && rx < W && fabsf(dispR[y * W + rx] - ds) > 1.5f)
+            f = 255;
+    }
+    fail[i] = f;
+}
+
+// cv::dilate with a 3x3 box; samples outside the image do not take part.
+__global__ void dilate3_kernel(const uint8_t *in, int W, int H, uint8_t *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H)
+        return;
+    int y = i / W, x = i - y * W;
+    uint8_t m = 0;
+    for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+        {
+            int yy = y + dy, xx = x + dx;
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W)
+                m = max(m, in[yy * W + xx]);
+        }
+    out[i] = m;
+}
+
+// Horizontal NN-interpolation (post_process.cu:72-109): nearest pixel on
+// each side outside the dilated mask; keep the plane with the smaller
+// disparity at the failed pixel. Reads only pixels outside the dilated mask,
+// writes only failed pixels (a subset of it), so the update is in place.
+__global__ void lr_fill_kernel(const uint8_t *fail, const uint8_t *fail2, int W, int H, float *plane)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H || !fail[i])
+        return;
+    int y = i / W, x = i - y * W;
+    int xl = x, xr = x;
+    while (xl >= 0 && fail2[y * W + xl] == 255)
+        xl--;
+    while (xr < W && fail2[y * W + xr] == 255)
+        xr++;
+    const float *pl = xl >= 0 ? plane + 3 * (size_t)(y * W + xl) : nullptr;
+    const float *pr = xr < W ? plane + 3 * (size_t)(y * W + xr) : nullptr;
+    const float *pick;
+    if (!pl && !pr)
+        return;
+    else if (!pl)
+        pick = pr;
+    else if (!pr)
+        pick = pl;
+    else
+        pick = get_z(pl, x, y) < get_z(pr, x, y) ? pl : pr;
+    float a = pick[0], b = pick[1], c = pick[2];
+    plane[3 * (size_t)i] = a;
+    plane[3 * (size_t)i + 1] = b;
+    plane[3 * (size_t)i + 2] = c;
+}
+
+__global__ void plane_to_disp_kernel(const float *plane, int W, int H, float *disp)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H)
+        return;
+    int y = i / W, x = i - y * W;
+    disp[i] = get_z(plane + 3 * (size_t)i, x, y);
+}
+
+__global__ void compact_fail(const uint8_t *fail, int n, int *list, int *count)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && fail[i])
+        list[atomicAdd(count, 1)] = i;
+}
+
+// Weighted median (post_process.cu:127-185): one block per failed pixel.
+// Window samples (41x41 clipped) get weight expf(-sum|dBGR| / 10) and the
+// disparity of their plane at the pixel; the samples are sorted by
+// (disparity, window position) and the first one whose cumulative weight
+// exceeds half the total gives the plane. Weight sums are in double.
+// The colour distance sum|dBGR| is an integer 0..765, so the weights come
+// from a 766-entry table computed on the host with the C library's expf,
+// the function the reference's CPU code calls.
+constexpr int WM_T = 256, WM_N = 2048, WM_R = 20;
+__global__ void __launch_bounds__(WM_T)
+    weighted_median_kernel(const uint8_t *bgr, const int *list, int W, int H, const float *plane_in,
+                           float *plane_out, const float *wtab)
+{
+    __shared__ float zk[WM_N];
+    __shared__ int ik[WM_N];
+    __shared__ double part[WM_T];
+    __shared__ int found;
+    const int p = list[blockIdx.x];
+    const int y = p / W, x = p - y * W;
+    const int y0 = max(y - WM_R, 0), y1 = min(y + WM_R + 1, H);
+    const int x0 = max(x - WM_R, 0), x1 = min(x + WM_R + 1, W);
+    const int ww = x1 - x0, n = ww * (y1 - y0);
+    const uint8_t *s = bgr + 3 * (size_t)p;
+    const float s0 = s[0], s1 = s[1], s2 = s[2];
+    for (int j = threadIdx.x; j < WM_N; j += WM_T)
+    {
+        if (j < n)
+        {
+            int q = (y0 + j / ww) * W + x0 + j % ww;
+            zk[j] = get_z(plane_in + 3 * (size_t)q, x, y);
+            ik[j] = j;
+        }
+        else
+        {
+            zk[j] = FLT_MAX;
+            ik[j] = WM_N + j;
+        }
+    }
+    __syncthreads();
+    // bitonic sort by (z, index)
+    for (int k = 2; k <= WM_N; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1)
+        {
+            for (int t = threadIdx.x; t < WM_N; t += WM_T)
+            {
+                int u = t ^ j;
+                if (u > t)
+                {
+                    bool up = (t & k) == 0;
+                    float za = zk[t], zb = zk[u];
+                    int ia = ik[t], ib = ik[u];
+                    bool gt = za > zb || (za == zb && ia > ib);
+                    if (gt == up)
+                    {
+                        zk[t] = zb;
+                        zk[u] = za;
+                        ik[t] = ib;
+                        ik[u] = ia;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // weights in sorted order; block prefix sums in double (fixed order)
+    const int per = WM_N / WM_T; // 8 consecutive sorted samples per thread
+    double wv[per];
+    double tsum = 0.0;
+    for (int k = 0; k < per; ++k)
+    {
+        int j = threadIdx.x * per + k;
+        double w = 0.0;
+        if (j < n)
+        {
+            int src = ik[j];
+            int q = (y0 + src / ww) * W + x0 + src % ww;
+            const uint8_t *t = bgr + 3 * (size_t)q;
+            int absdiff = abs((int)s0 - (int)t[0]) + abs((int)s1 - (int)t[1]) + abs((int)s2 - (int)t[2]);
+            w = (double)wtab[absdiff];
+        }
+        wv[k] = w;
+        tsum += w;
+    }
+    part[threadIdx.x] = tsum;
+    if (threadIdx.x == 0)
+        found = 0x7fffffff;
+    __syncthreads();
+    // inclusive scan of per-thread sums (Hillis-Steele, fixed order)
+    for (int off = 1; off < WM_T; off <<= 1)
+    {
+        double v = threadIdx.x >= off ? part[threadIdx.x - off] : 0.0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    const double center = part[WM_T - 1] / 2.0;
+    double run = threadIdx.x ? part[threadIdx.x - 1] : 0.0;
+    for (int k = 0; k < per; ++k)
+    {
+        int j = threadIdx.x * per + k;
+        run += wv[k];
+        if (j < n && run > center)
+        {
+            atomicMin(&found, j);
+            break;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && found < n)
+    {
+        int src = ik[found];
+        int q = (y0 + src / ww) * W + x0 + src % ww;
+        plane_out[3 * (size_t)p] = plane_in[3 * (size_t)q];
+        plane_out[3 * (size_t)p + 1] = plane_in[3 * (size_t)q + 1];
+        plane_out[3 * (size_t)p + 2] = plane_in[3 * (size_t)q + 2];
+    }
+}
+
+__device__ __forceinline__ float median7(float *v)
+{
+    for (int j = 1; j < 7; ++j)
+    {
+        float t = v[j];
+        int i = j - 1;
+        while (i >= 0 && v[i] > t)
+        {
+            v[i + 1] = v[i];
+            i--;
+        }
+        v[i + 1] = t;
+    }
+    return v[3];
+}
+
+// medianFilter, horizontal pass: interior pixels of D into T (T starts zero).
+__global__ void median_h_kernel(const float *D, int W, int H, float *T)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H)
+        return;
+    int y = i / W, u = i - y * W;
+    if (u < 3 || u >= W - 3 || y < 3 || y >= H - 3)
+        return;
+    if (D[i] >= 0)
+    {
+        float v[7];
+        for (int k = 0; k < 7; ++k)
+            v[k] = D[i - 3 + k];
+        T[i] = median7(v);
+    }
+    else
+        T[i] = D[i];
+}
+
+// vertical pass: reads T (including its untouched zero border rows).
+__global__ void median_v_kernel(const float *T, int W, int H, float *D)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H)
+        return;
+    int y = i / W, u = i - y * W;
+    if (u < 3 || u >= W - 3 || y < 3 || y >= H - 3)
+        return;
+    if (D[i] >= 0)
+    {
+        float v[7];
+        for (int k = 0; k < 7; ++k)
+            v[k] = T[(y - 3 + k) * W + u];
+        D[i] = median7(v);
+    }
+}
+} // namespace
+
+void launch_lr_check(const float *dispL, const float *dispR, float *planeL, uint8_t *fail,
+                     uint8_t *fail2, int W, int H, cudaStream_t st)
+{
+    int n = W * H;
+    lr_fail_kernel<<<ceil_div(n, 256), 256, 0, st>>>(dispL, dispR, W, H, fail);
+    dilate3_kernel<<<ceil_div(n, 256), 256, 0, st>>>(fail, W, H, fail2);
+    lr_fill_kernel<<<ceil_div(n, 256), 256, 0, st>>>(fail, fail2, W, H, planeL);
+    HBP_LAUNCH_CHECK();
+}
+
+void launch_plane_to_disp(const float *plane, float *disp, int W, int H, cudaStream_t st)
+{
+    plane_to_disp_kernel<<<ceil_div(W * H, 256), 256, 0, st>>>(plane, W, H, disp);
+    HBP_LAUNCH_CHECK();
+}
+
+void median_weight_table(float *host766)
+{
+    for (int k = 0; k < 766; ++k)
+        host766[k] = std::exp(-(float)k / 10.0f);
+}
+
+void launch_weighted_median(const uint8_t *bgr, const uint8_t *fail, const float *plane_in,
+                            float *plane_out, int W, int H, const float *wtab, Arena &tmp,
+                            cudaStream_t st)
+{
+    int n = W * H;
+    size_t m = tmp.mark();
+    int *list = tmp.alloc<int>(n), *count = tmp.alloc<int>(1);
+    HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int), st));
+    HBP_CUDA(cudaMemcpyAsync(plane_out, plane_in, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    compact_fail<<<ceil_div(n, 256), 256, 0, st>>>(fail, n, list, count);
+    HBP_LAUNCH_CHECK();
+    int nf = 0;
+    HBP_CUDA(cudaMemcpyAsync(&nf, count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HBP_CUDA(cudaStreamSynchronize(st));
+    if (nf > 0)
+    {
+        weighted_median_kernel<<<nf, WM_T, 0, st>>>(bgr, list, W, H, plane_in, plane_out, wtab);
+        HBP_LAUNCH_CHECK();
+    }
+    tmp.rewind(m);
+}
+
+void launch_driver_median(float *disp, float *tmp, int W, int H, cudaStream_t st)
+{
+    int n = W * H;
+    HBP_CUDA(cudaMemsetAsync(tmp, 0, sizeof(float) * n, st));
+    median_h_kernel<<<ceil_div(n, 256), 256, 0, st>>>(disp, W, H, tmp);
+    median_v_kernel<<<ceil_div(n, 256), 256, 0, st>>>(tmp, W, H, disp);
+    HBP_LAUNCH_CHECK();
+}
+
+} // namespace hbp

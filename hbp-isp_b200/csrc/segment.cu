@@ -1,0 +1,346 @@
+// Image segmentation pyramid (SegHAC with CentroidLink, 4-neighbour grid,
+// sigma = 0, LabelISPFormat, target 1): reference segment.cu:1279-1321.
+//
+// Level l holds N_l nodes and E_l directed edges. Per level the loop runs
+// CRTrees on the 1-NN successor array, records the level in the reference's
+// ISP layout (segment.cu:884-905), then builds level l+1:
+//   * edges mapped to parents, sorted as (s, t) pairs, de-duplicated and
+//     stripped of self-loops; boundary lengths are summed by POSITION in the
+//     sorted order, because the reference sorts the pairs alone and leaves the
+//     length array in its old order (segment.cu:1061, :368-386);
+//   * inner distance max of the children (segment.cu:1116-1128);
+//   * child sums of (L, a, b, x, y, count), added in increasing child index
+//     (the reference uses float atomics, segment.cu:472-486);
+//   * centroid distance with the hinge on L, fused as the reference's device
+//     code fuses it, plus the penalty d += max(d - maxinner[t], 0)
+//     (segment.cu:508-534, :582-612);
+//   * per node the minimum over its out-edges, ties to the largest target
+//     (segment.cu:403-422, :1211-1231).
+#include <algorithm>
+
+#include "engine.h"
+
+namespace hbp
+{
+namespace
+{
+__device__ __forceinline__ float pix_dist(float4 s, float4 t)
+{
+    float dx = s.x - t.x, dy = s.y - t.y, dz = s.z - t.z;
+    float d = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+    return __fadd_rn(d, dx > 0.f ? dx : 0.f);
+}
+
+// compute_1nn_grid_k (segment.cu:57-195), num_nb = 4: neighbours up, down,
+// left, right; first strict minimum. Also writes the level-0 edge list
+// bd[4i+k] = (i, neighbour or i) and the level-0 sums (L, a, b, x, y, 1).
+__global__ void nn_grid_kernel(const float4 *__restrict__ lab, int W, int H, int *__restrict__ nn,
+                               float *__restrict__ dist_min, int2 *__restrict__ bd,
+                               int *__restrict__ bdl, float *__restrict__ sums)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = W * H;
+    if (i >= n)
+        return;
+    int y = i / W, x = i - y * W;
+    float4 s = lab[i];
+    int nb[4] = {y > 0 ? i - W : -1, y < H - 1 ? i + W : -1, x > 0 ? i - 1 : -1,
+                 x < W - 1 ? i + 1 : -1};
+    float best = 3.402823466e+38f;
+    int arg = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+    {
+        int t = nb[k];
+        bd[4 * i + k] = make_int2(i, t < 0 ? i : t);
+        bdl[4 * i + k] = 1;
+        if (t < 0)
+            continue;
+        float d = pix_dist(s, lab[t]);
+        if (d < best)
+        {
+            best = d;
+            arg = t;
+        }
+    }
+    nn[i] = arg;
+    dist_min[i] = best;
+    if (sums)
+    {
+        sums[i] = s.x;
+        sums[n + i] = s.y;
+        sums[2 * n + i] = s.z;
+        sums[3 * n + i] = (float)x;
+        sums[4 * n + i] = (float)y;
+        sums[5 * n + i] = s.w;
+    }
+}
+
+__global__ void map_edges(const int2 *__restrict__ bd, const int *__restrict__ clus, long E, int bits,
+                          uint64_t *__restrict__ keys)
+{
+    long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E)
+        return;
+    int2 v = bd[e];
+    keys[e] = ((uint64_t)(uint32_t)clus[v.x] << bits) | (uint32_t)clus[v.y];
+}
+
+__global__ void run_flags(const uint64_t *__restrict__ keys, long E, int bits, int *__restrict__ keep)
+{
+    long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E)
+        return;
+    uint64_t k = keys[e];
+    uint32_t s = (uint32_t)(k >> bits), t = (uint32_t)(k & ((1ull << bits) - 1));
+    bool last = (e == E - 1) || keys[e + 1] != k;
+    keep[e] = (last && s != t) ? 1 : 0;
+}
+
+// Kept run ends become the new edges; every non-self-loop element adds the
+// length stored at its sorted POSITION into its run's slot (integer atomics:
+// the order does not matter).
+__global__ void emit_edges(const uint64_t *__restrict__ keys, const int *__restrict__ keep,
+                           const int *__restrict__ slot, const int *__restrict__ bdl_old, long E,
+                           int bits, int2 *__restrict__ bd_new, int *__restrict__ bdl_new)
+{
+    long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E)
+        return;
+    uint64_t k = keys[e];
+    int s = (int)(k >> bits), t = (int)(k & ((1ull << bits) - 1));
+    if (s == t)
+        return;
+    int sl = slot[e];
+    atomicAdd(&bdl_new[sl], bdl_old[e]);
+    if (keep[e])
+        bd_new[sl] = make_int2(s, t);
+}
+
+__global__ void iota_u32(uint32_t *v, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        v[i] = (uint32_t)i;
+}
+
+__global__ void copy_keys(const int *clus, int n, uint32_t *k, int *count)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        k[i] = (uint32_t)clus[i];
+        atomicAdd(&count[clus[i]], 1);
+    }
+}
+
+// Per parent: sums of the children (children in increasing index, sequential
+// from 0) and the maximum of the children's dist_min (inner distance).
+__global__ void parent_sums(const uint32_t *__restrict__ child, const int *__restrict__ child_off,
+                            const float *__restrict__ sums_c, int Nc, const float *__restrict__ dmin_c,
+                            int Np, float *__restrict__ sums_p, float *__restrict__ dmax_p,
+                            float *__restrict__ mean_p)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= Np)
+        return;
+    int b = child_off[p], e = child_off[p + 1];
+    float acc[6] = {0, 0, 0, 0, 0, 0};
+    float mx = 0.0f;
+    for (int j = b; j < e; ++j)
+    {
+        int c = (int)child[j];
+#pragma unroll
+        for (int ch = 0; ch < 6; ++ch)
+            acc[ch] = __fadd_rn(acc[ch], sums_c[(size_t)ch * Nc + c]);
+        mx = fmaxf(mx, dmin_c[c]);
+    }
+#pragma unroll
+    for (int ch = 0; ch < 6; ++ch)
+        sums_p[(size_t)ch * Np + p] = acc[ch];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+        mean_p[(size_t)ch * Np + p] = __fdiv_rn(acc[ch], acc[5]);
+    dmax_p[p] = mx;
+}
+
+__global__ void edge_src_count(const int2 *__restrict__ bd, int E, int *__restrict__ count)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E)
+        atomicAdd(&count[bd[e].x], 1);
+}
+
+// One thread per node walks its out-edges (contiguous, targets ascending):
+// centroid distance + penalty, minimum, and the largest target among minima.
+__global__ void node_1nn(const int2 *__restrict__ bd, const int *__restrict__ off, int N,
+                         const float *__restrict__ mean, const float *__restrict__ dmax,
+                         int *__restrict__ nn, float *__restrict__ dist_min)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N)
+        return;
+    float ls = mean[s], as = mean[N + s], bs = mean[2 * N + s];
+    float best = 3.402823466e+38f;
+    int arg = 0;
+    for (int e = off[s]; e < off[s + 1]; ++e)
+    {
+        int t = bd[e].y;
+        float e0 = __fsub_rn(ls, mean[t]), e1 = __fsub_rn(as, mean[N + t]), e2 = __fsub_rn(bs, mean[2 * N + t]);
+        float h = e0 > 0.f ? e0 : 0.f;
+        float d = __fmaf_rn(e2, e2, __fmaf_rn(e1, e1, __fmaf_rn(e0, e0, h)));
+        float delta = __fsub_rn(d, dmax[t]);
+        if (delta > 0)
+            d = __fadd_rn(d, delta);
+        if (d < best)
+        {
+            best = d;
+            arg = t;
+        }
+        else if (d == best)
+            arg = t;
+    }
+    nn[s] = arg;
+    dist_min[s] = best;
+}
+
+int bits_for(long n)
+{
+    int b = 1;
+    while ((1l << b) < n)
+        ++b;
+    return b;
+}
+
+int read_int(const int *dev, cudaStream_t st)
+{
+    int h = 0;
+    HBP_CUDA(cudaMemcpyAsync(&h, dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HBP_CUDA(cudaStreamSynchronize(st));
+    return h;
+}
+} // namespace
+
+void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
+                   int *err_dev, cudaStream_t st)
+{
+    const int N0 = W * H;
+    pyr.W = W;
+    pyr.H = H;
+    pyr.L = 0;
+    pyr.N.clear();
+    pyr.E.clear();
+    pyr.node_off.clear();
+    pyr.edge_off.clear();
+    pyr.child_base.clear();
+    pyr.nb_base.clear();
+    // capacities of the concatenated ISP arrays (segment.hpp:276-283)
+    pyr.clus = a.alloc<int>(2 * (size_t)N0);
+    pyr.sums = a.alloc<float>(12 * (size_t)N0);
+    pyr.bd = a.alloc<int2>(8 * (size_t)N0);
+    pyr.bdl = a.alloc<int>(8 * (size_t)N0);
+    pyr.child = a.alloc<uint32_t>(2 * (size_t)N0);
+    pyr.child_off = a.alloc<int>(2 * (size_t)N0 + 64);
+    pyr.nb_off = a.alloc<int>(2 * (size_t)N0 + 64);
+
+    size_t m0 = tmp.mark();
+    float4 *lab = tmp.alloc<float4>(N0);
+    int *nn = tmp.alloc<int>(N0), *nn2 = tmp.alloc<int>(N0);
+    float *dmin = tmp.alloc<float>(N0), *dmin2 = tmp.alloc<float>(N0);
+    float *mean = tmp.alloc<float>(3 * (size_t)N0);
+    float *dmax = tmp.alloc<float>(N0);
+    int *count = tmp.alloc<int>(N0 + 1);
+    int *num_dev = tmp.alloc<int>(2);
+    uint64_t *keys = tmp.alloc<uint64_t>(4 * (size_t)N0), *keys_alt = tmp.alloc<uint64_t>(4 * (size_t)N0);
+    int *keep = tmp.alloc<int>(4 * (size_t)N0), *slot = tmp.alloc<int>(4 * (size_t)N0);
+    uint32_t *ck = tmp.alloc<uint32_t>(N0), *ck_alt = tmp.alloc<uint32_t>(N0),
+             *cv_alt = tmp.alloc<uint32_t>(N0);
+
+    launch_lab(bgr, N0, lab, st);
+    nn_grid_kernel<<<ceil_div(N0, 256), 256, 0, st>>>(lab, W, H, nn, dmin, pyr.bd, pyr.bdl, pyr.sums);
+    HBP_LAUNCH_CHECK();
+
+    int N = N0;
+    long E = 4l * N0;
+    size_t oc = 0, ob = 0, och = 0, onb = 0;
+    for (;;)
+    {
+        int *clus = pyr.clus + oc;
+        crtrees_labels(nn, N, clus, num_dev, err_dev, tmp, st);
+        int Nn = read_int(num_dev, st);
+        if (Nn < 1 || Nn > N)
+            throw StatusError{HBP_ERR_NO_CONVERGENCE, "crtrees produced an invalid cluster count"};
+        pyr.N.push_back(N);
+        pyr.E.push_back((int)E);
+        pyr.node_off.push_back(oc);
+        pyr.edge_off.push_back(ob);
+        pyr.L++;
+        // children of every parent in increasing child index; used for the
+        // sums here and by the spatial propagation of HBP (sort_clus,
+        // hbp_isp.cu:985-1001)
+        uint32_t *child = pyr.child + oc;
+        int *child_off = pyr.child_off + och;
+        pyr.child_base.push_back(och);
+        HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (Nn + 1), st));
+        copy_keys<<<ceil_div(N, 256), 256, 0, st>>>(clus, N, ck, count);
+        iota_u32<<<ceil_div(N, 256), 256, 0, st>>>(child, N);
+        HBP_LAUNCH_CHECK();
+        radix_sort_pairs_u32(ck, child, ck_alt, cv_alt, N, bits_for(Nn), tmp, st);
+        exclusive_scan(count, child_off, Nn + 1, nullptr, tmp, st);
+        och += Nn + 1;
+        // CSR by source of this level's edges (sorted by source at every level)
+        int *nb_off = pyr.nb_off + onb;
+        pyr.nb_base.push_back(onb);
+        HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (N + 1), st));
+        edge_src_count<<<ceil_div(E, 256), 256, 0, st>>>(pyr.bd + ob, (int)E, count);
+        HBP_LAUNCH_CHECK();
+        exclusive_scan(count, nb_off, N + 1, nullptr, tmp, st);
+        onb += N + 1;
+        if (Nn == 1)
+            break;
+
+        // next level's nodes and edges live right after this level's
+        float *sums_c = pyr.sums + 6 * oc;
+        float *sums_p = pyr.sums + 6 * (oc + N);
+        int2 *bd_c = pyr.bd + ob;
+        int *bdl_c = pyr.bdl + ob;
+        int2 *bd_p = pyr.bd + ob + E;
+        int *bdl_p = pyr.bdl + ob + E;
+        // reduce_boundary_dist
+        int bits = bits_for(Nn);
+        map_edges<<<ceil_div(E, 256), 256, 0, st>>>(bd_c, clus, E, bits, keys);
+        HBP_LAUNCH_CHECK();
+        radix_sort_keys_u64(keys, keys_alt, E, 2 * bits, tmp, st);
+        run_flags<<<ceil_div(E, 256), 256, 0, st>>>(keys, E, bits, keep);
+        HBP_LAUNCH_CHECK();
+        exclusive_scan(keep, slot, E, num_dev + 1, tmp, st);
+        int E2 = read_int(num_dev + 1, st);
+        if ((size_t)(ob + E + E2) > 8 * (size_t)N0 || E2 < 1)
+            throw StatusError{HBP_ERR_INTERNAL, "edge capacity exceeded"};
+        HBP_CUDA(cudaMemsetAsync(bdl_p, 0, sizeof(int) * E2, st));
+        emit_edges<<<ceil_div(E, 256), 256, 0, st>>>(keys, keep, slot, bdl_c, E, bits, bd_p, bdl_p);
+        HBP_LAUNCH_CHECK();
+        // sums, means, inner max (reduce_data_mean, compute_dist_inner_max)
+        parent_sums<<<ceil_div(Nn, 128), 128, 0, st>>>(child, child_off, sums_c, N, dmin, Nn, sums_p,
+                                                         dmax, mean);
+        HBP_LAUNCH_CHECK();
+        // CSR of the new edges for the per-node minimum
+        HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (Nn + 1), st));
+        edge_src_count<<<ceil_div(E2, 256), 256, 0, st>>>(bd_p, E2, count);
+        HBP_LAUNCH_CHECK();
+        exclusive_scan(count, slot, Nn + 1, nullptr, tmp, st);
+        node_1nn<<<ceil_div(Nn, 128), 128, 0, st>>>(bd_p, slot, Nn, mean, dmax, nn2, dmin2);
+        HBP_LAUNCH_CHECK();
+        std::swap(nn, nn2);
+        std::swap(dmin, dmin2);
+        oc += N;
+        ob += E;
+        N = Nn;
+        E = E2;
+        if (oc + N > 2 * (size_t)N0)
+            throw StatusError{HBP_ERR_INTERNAL, "node capacity exceeded"};
+    }
+    tmp.rewind(m0);
+}
+
+} // namespace hbp

@@ -1,0 +1,169 @@
+"""Python binding of the B200 HBP-ISP engine's C ABI (include/hbp_b200.h).
+
+Host-buffer entry points take numpy arrays; the ``*_d`` stage entry points
+take device tensors (torch) and pass their data pointers. The engine library
+must be built (``python hbp-isp_b200/build.py``); there is no fallback: a
+missing library raises ``EngineUnavailable``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libhbp_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "hbp_b200.h")
+
+P = C.c_void_p
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "admission rejected", 4: "no convergence",
+          5: "CUDA error", 6: "timeout", 7: "not ready", 8: "internal error"}
+
+
+class EngineUnavailable(RuntimeError):
+    pass
+
+
+class HbpError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("tau_smooth", C.c_float), ("min_level", C.c_int),
+                ("msg_fp16", C.c_int), ("post", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the engine library (raises EngineUnavailable if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EngineUnavailable(f"{LIB_PATH} not built; run python hbp-isp_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        L.hbp_last_error.restype = C.c_char_p
+        L.hbp_status_string.restype = C.c_char_p
+        L.hbp_ctx_stream.restype = P
+        L.hbp_ctx_create.argtypes = [C.c_int, C.c_long, C.c_int, C.POINTER(P)]
+        L.hbp_lab_d.argtypes = [P, P, C.c_long, P, P]
+        _lib = L
+    return _lib
+
+
+def exported_symbols_from_header(path: str = HEADER) -> list[str]:
+    """Function names declared in the C header."""
+    import re
+    txt = open(path).read()
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(hbp_\w+)\s*\(", txt, flags=re.M)))
+
+
+def _check(st: int):
+    if st != 0:
+        raise HbpError(st, lib().hbp_last_error().decode())
+
+
+def _p(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(P)
+    return P(a.data_ptr())  # torch tensor on the device
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().hbp_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def volume_pitch(W: int) -> int:
+    return lib().hbp_volume_pitch(W)
+
+
+class Context:
+    """One device context (stream + device memory slab). Not thread safe."""
+
+    def __init__(self, device: int = 0, max_pixels: int = 0, max_disp: int = 0):
+        h = P()
+        _check(lib().hbp_ctx_create(device, max_pixels, max_disp, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().hbp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return lib().hbp_ctx_stream(self.h) or 0
+
+    # ------------------------------------------------------------ whole pair
+    def run_pair(self, left: np.ndarray, right: np.ndarray, D: int, params: Params | None = None,
+                 want_plane: bool = False):
+        left = np.ascontiguousarray(left, np.uint8)
+        right = np.ascontiguousarray(right, np.uint8)
+        H, W = left.shape[:2]
+        disp = np.zeros((H, W), np.float32)
+        plane = np.zeros((H, W, 3), np.float32) if want_plane else None
+        prm = params or default_params()
+        _check(lib().hbp_run_pair(self.h, _p(left), _p(right), W, H, D, C.byref(prm), _p(disp), _p(plane)))
+        return (disp, plane) if want_plane else disp
+
+    # ------------------------------------------------------------ stages (device)
+    def cost_census_d(self, bgrL, bgrR, W, H, D, censusL, censusR, vol, wta, volR=None, wtaR=None):
+        _check(lib().hbp_cost_census_d(self.h, _p(bgrL), _p(bgrR), W, H, D, _p(censusL), _p(censusR),
+                                       _p(vol), _p(wta), _p(volR), _p(wtaR), None))
+
+    def lab_d(self, bgr, n, lab4):
+        _check(lib().hbp_lab_d(self.h, _p(bgr), n, _p(lab4), None))
+
+    def crtrees_d(self, nn, N, clus) -> int:
+        k = C.c_int(0)
+        _check(lib().hbp_crtrees_d(self.h, _p(nn), N, _p(clus), C.byref(k), None))
+        return k.value
+
+    def segment_d(self, bgr, W, H) -> int:
+        L = C.c_int(0)
+        _check(lib().hbp_segment_d(self.h, _p(bgr), W, H, C.byref(L), None))
+        return L.value
+
+    def pyramid(self) -> dict:
+        """The last pyramid in the reference's ISP layout (host arrays)."""
+        sizes = np.zeros(2 * 64, np.int32)
+        _check(lib().hbp_pyramid_levels(self.h, _p(sizes), 64))
+        sizes = sizes.reshape(64, 2)
+        L = int(np.count_nonzero(sizes[:, 0]))
+        sizes = sizes[:L].copy()
+        tn, te = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
+        clus = np.zeros(tn, np.int32)
+        mean = np.zeros(6 * tn, np.float32)
+        bd = np.zeros((te, 2), np.int32)
+        bdl = np.zeros(te, np.int32)
+        _check(lib().hbp_pyramid_copy(self.h, _p(clus), _p(mean), _p(bd), _p(bdl)))
+        return dict(level_sizes=sizes, clus=clus, mean=mean, bd=bd, bdl=bdl)
+
+    def infer_d(self, vol, wta, D, params: Params | None, disp, plane=None):
+        prm = params or default_params()
+        _check(lib().hbp_infer_d(self.h, _p(vol), _p(wta), D, C.byref(prm), _p(disp), _p(plane), None))
+
+    def lr_check_d(self, dispL, dispR, planeL, fail, disp_out, W, H):
+        _check(lib().hbp_lr_check_d(self.h, _p(dispL), _p(dispR), _p(planeL), _p(fail), _p(disp_out), W, H, None))
+
+    def weighted_median_d(self, bgrL, fail, plane, disp_out, W, H):
+        _check(lib().hbp_weighted_median_d(self.h, _p(bgrL), _p(fail), _p(plane), _p(disp_out), W, H, None))
+
+    def driver_median_d(self, disp, W, H):
+        _check(lib().hbp_driver_median_d(self.h, _p(disp), W, H, None))

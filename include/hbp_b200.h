@@ -1,0 +1,132 @@
+/*
+ * hbp_b200.h - C ABI of the B200 HBP-ISP stereo engine.
+ *
+ * The engine takes a rectified BGR8 pair and produces a disparity map with the
+ * method of HBP-ISP ("Hierarchical Belief Propagation on Image Segmentation
+ * Pyramid"). Each entry point below replaces one step of the reference's C++
+ * API (file:line into the reference tree) and keeps its meaning; the C++
+ * classes in include/hbp_isp/ restore the reference's class interface on top
+ * of these functions.
+ *
+ * Conventions: plain pointers and sizes only. Colour images are interleaved
+ * BGR uint8 (the reference reads channel x as blue, imutil.cu:11-13);
+ * disparity maps are H x W float32; plane maps are H x W x 3 float32 (a, b, c
+ * with d = a*x + b*y + c). Functions whose names end in _d take device
+ * pointers and an optional CUDA stream (cudaStream_t passed as void*, NULL =
+ * the context's stream); all others take host pointers. A context is used by
+ * one host thread at a time. Every call returns an hbp_status; on failure
+ * hbp_last_error() describes the cause.
+ */
+#ifndef HBP_B200_H
+#define HBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hbp_status
+{
+    HBP_OK = 0,
+    HBP_ERR_INVALID_ARG = 1,        /* bad size, pointer or parameter */
+    HBP_ERR_OUT_OF_MEMORY = 2,      /* device or pinned memory exhausted */
+    HBP_ERR_ADMISSION_REJECTED = 3, /* request exceeds the server's memory budget */
+    HBP_ERR_NO_CONVERGENCE = 4,     /* a bounded device loop gave up (CRTrees) */
+    HBP_ERR_CUDA = 5,               /* CUDA runtime error */
+    HBP_ERR_TIMEOUT = 6,            /* wait ended before the request finished */
+    HBP_ERR_NOT_READY = 7,          /* poll: request still running */
+    HBP_ERR_INTERNAL = 8            /* invariant violated (capacity, ...) */
+} hbp_status;
+
+typedef struct hbp_ctx hbp_ctx;
+
+/* Parameters of one run. Defaults (hbp_default_params) are the reference's
+ * Census run, test_stereo_hbp_isp.sh:4: alpha 1000.1, tau_smooth 0.6,
+ * min_level 2 (CentroidLink, 4-grid, sigma 0 are fixed). */
+typedef struct hbp_params
+{
+    float alpha;      /* data-term weight lambda (hbp_isp.hpp:353-363) */
+    float tau_smooth; /* smoothness truncation (hbp_isp.cu:349) */
+    int min_level;    /* finest pyramid level inferred (hbp_isp.cu:1328) */
+    int msg_fp16;     /* 1: BP messages stored as FP16 (FP32 arithmetic) */
+    int post;         /* 0: none; 1: driver 7-tap median (main_stereo_hbp_isp.cu:75);
+                         2: right view + LR check/fill + weighted median + plane->disp
+                            (main_bench_middv3.cu:189-219) */
+} hbp_params;
+
+void hbp_default_params(hbp_params *p);
+const char *hbp_status_string(hbp_status s);
+const char *hbp_last_error(void);
+
+/* Context: device, stream, device memory slab sized for images up to
+ * max_pixels x max_disp (0 = sized lazily on first use). */
+hbp_status hbp_ctx_create(int device, long max_pixels, int max_disp, hbp_ctx **out);
+void hbp_ctx_destroy(hbp_ctx *ctx);
+void *hbp_ctx_stream(hbp_ctx *ctx);
+
+/* ---------------------------------------------------------------- stages */
+
+/* StereoCost::compute_stereo_cost("Census") (stereo_cost.cu:421-445) with the
+ * grey conversion of the constructor (stereo_cost.cu:290-297): census of both
+ * views, uint8 cost volume vol[d][y][x] (row pitch hbp_volume_pitch(W)) with
+ * values min(popcount, 25), WTA disparity. With volR/wtaR non-NULL the
+ * right-view volume and WTA of StereoCost::cost_to_right (stereo_cost.cu:
+ * 488-516) are produced in the same pass. */
+int hbp_volume_pitch(int W);
+hbp_status hbp_cost_census_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H,
+                             int D, uint32_t *censusL, uint32_t *censusR, uint8_t *vol,
+                             float *wta, uint8_t *volR, float *wtaR, void *stream);
+
+/* BGR -> CIELAB float4 (L, a, b, 1) (imutil.cu:4-40, segment.cu:795-809). */
+hbp_status hbp_lab_d(hbp_ctx *ctx, const uint8_t *bgr, long n, float *lab4, void *stream);
+
+/* CRTrees::get_clus + compact_clus_label (CRTrees.cu:395-434, :467-483):
+ * connected components of the successor array nn (every entry in [0, N)),
+ * labelled 0..n-1; *num_clusters receives n. Synchronous. */
+hbp_status hbp_crtrees_d(hbp_ctx *ctx, const int *nn, int N, int *clus, int *num_clusters,
+                         void *stream);
+
+/* SegHAC(CentroidLink, 4, 0, LabelISPFormat, 1).run_ms() + ISPData
+ * (segment.cu:1279-1321, hbp_isp.hpp:24-46): builds the image segmentation
+ * pyramid of a device BGR image inside the context (replacing any previous
+ * one) and returns its number of levels. hbp_pyramid_levels gives per level
+ * (num_clus, num_bd); hbp_pyramid_copy copies the reference's ISP arrays
+ * (clus, mean sums [6][N_l], bd pairs, bdl, concatenated over levels) to host
+ * buffers of at least the summed sizes. */
+hbp_status hbp_segment_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int *levels, void *stream);
+hbp_status hbp_pyramid_levels(hbp_ctx *ctx, int *sizes, int max_levels);
+hbp_status hbp_pyramid_copy(hbp_ctx *ctx, int *clus, float *mean, int *bd, int *bdl);
+
+/* HBP_ISP(ISPData, StereoData, alpha, tau_smooth).run_ms(min_level)
+ * (hbp_isp.hpp:288-386, hbp_isp.cu:1313-1346) on the context's pyramid and a
+ * device cost volume / WTA from hbp_cost_census_d. Writes disparity (H x W)
+ * and plane labels (H x W x 3; may be NULL). */
+hbp_status hbp_infer_d(hbp_ctx *ctx, const uint8_t *vol, const float *wta, int D,
+                       const hbp_params *prm, float *disp, float *plane, void *stream);
+
+/* PostProcess::left_right_check + plane_label_to_disp (post_process.cu:4-110,
+ * :373-390): updates planeL in place, writes the failure mask (0/255) and the
+ * disparity of the updated planes. */
+hbp_status hbp_lr_check_d(hbp_ctx *ctx, const float *dispL, const float *dispR, float *planeL,
+                          uint8_t *fail, float *disp_out, int W, int H, void *stream);
+/* PostProcess::median_filter + plane_label_to_disp (post_process.cu:112-185). */
+hbp_status hbp_weighted_median_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *fail,
+                                 float *plane, float *disp_out, int W, int H, void *stream);
+/* medianFilter of the single-pair driver (main_stereo_hbp_isp.cu:120-192). */
+hbp_status hbp_driver_median_d(hbp_ctx *ctx, float *disp, int W, int H, void *stream);
+
+/* ------------------------------------------------------------ whole pair */
+
+/* The single-pair path of main_stereo_hbp_isp.cu:33-76 (post = 1) or of
+ * MidV3_LR, main_bench_middv3.cu:169-219 (post = 2), on host buffers:
+ * uploads the pair, runs every stage on the device and downloads the
+ * disparity (and planes when plane != NULL). */
+hbp_status hbp_run_pair(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H,
+                        int D, const hbp_params *prm, float *disp, float *plane);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HBP_B200_H */

@@ -1,0 +1,184 @@
+"""Parity of the B200 engine (through its C ABI) with the CPU oracle and with
+the reference's golden outputs. Requires a GPU."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SCENES = ["tiny_96x64_d32_s7", "small_160x120_d48_s11", "c1_450x375_d64_s1000"]
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def eng():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import hbp_b200 as E
+    ctx = E.Context(0)
+    yield E, ctx, torch
+    ctx.close()
+
+
+def load(golden_dir, name):
+    return dict(np.load(os.path.join(golden_dir, name + ".npz")))
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def run_cost(E, ctx, torch, L, R, D, right=False):
+    H, W = L.shape[:2]
+    Wp = E.volume_pitch(W)
+    dL, dR = dev(torch, L), dev(torch, R)
+    cL = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+    cR = torch.zeros_like(cL)
+    vol = torch.zeros(D * H * Wp, dtype=torch.uint8, device="cuda")
+    wta = torch.zeros(H * W, dtype=torch.float32, device="cuda")
+    volR = torch.zeros_like(vol) if right else None
+    wtaR = torch.zeros_like(wta) if right else None
+    ctx.cost_census_d(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR)
+    torch.cuda.synchronize()
+    strip = lambda v: v.cpu().numpy().reshape(D, H, Wp)[:, :, :W].reshape(D, H * W)
+    out = dict(censusL=cL.cpu().numpy().view(np.uint32).reshape(H, W),
+               censusR=cR.cpu().numpy().view(np.uint32).reshape(H, W),
+               vol=strip(vol), wta=wta.cpu().numpy().reshape(H, W), vol_dev=vol, wta_dev=wta)
+    if right:
+        out.update(volR=strip(volR), wtaR=wtaR.cpu().numpy().reshape(H, W), volR_dev=volR, wtaR_dev=wtaR)
+    return out
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_cost_volume_bit_exact(eng, golden_dir, name):
+    import pyoracle as O
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L, R, D = z["left"], z["right"], int(z["D"])
+    H, W = L.shape[:2]
+    g = run_cost(E, ctx, torch, L, R, D, right=True)
+    assert sha(g["censusL"]) == str(z["sha_censusL"]) and sha(g["censusR"]) == str(z["sha_censusR"])
+    assert sha(g["vol"].astype(np.float32)) == str(z["sha_vol_f32"])
+    assert np.array_equal(g["wta"].astype(np.uint16), z["wta"])
+    assert sha(g["volR"].astype(np.float32)) == str(z["sha_vol_right"])
+    assert np.array_equal(g["wtaR"].astype(np.uint16), z["wta_right"])
+    cs = O.cost_stage(L, R, D)
+    assert np.array_equal(g["vol"], cs["vol"]) and np.array_equal(g["wta"], cs["wta"])
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_lab_bit_exact(eng, golden_dir, name):
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L = z["left"]
+    n = L.shape[0] * L.shape[1]
+    lab = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
+    ctx.lab_d(dev(torch, L), n, lab)
+    torch.cuda.synchronize()
+    assert sha(lab.cpu().numpy().reshape(L.shape[0], L.shape[1], 4)) == str(z["sha_lab"])
+
+
+def test_crtrees_reference_graphs(eng, golden_dir):
+    E, ctx, torch = eng
+    z = load(golden_dir, "crtrees_graphs")
+    nums = z["nums"]
+    for i in range(len(nums)):
+        g = z[f"g{i}"]
+        out = torch.zeros(len(g), dtype=torch.int32, device="cuda")
+        k = ctx.crtrees_d(dev(torch, g), len(g), out)
+        assert k == nums[i], i
+        assert np.array_equal(out.cpu().numpy(), z[f"c{i}"]), i
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_pyramid_bit_exact(eng, golden_dir, name):
+    """Labels/edges/lengths equal the reference's at every level; node sums equal
+    the oracle's bit for bit (same child order)."""
+    import pyoracle as O
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L = z["left"]
+    H, W = L.shape[:2]
+    ctx.segment_d(dev(torch, L), W, H)
+    g = ctx.pyramid()
+    o = O.segment(O.lab(L))
+    assert np.array_equal(g["level_sizes"], o["level_sizes"])
+    assert np.array_equal(g["level_sizes"], z["level_sizes"])
+    for k in ("clus", "bd", "bdl"):
+        assert np.array_equal(g[k], o[k]), k
+    assert np.array_equal(g["mean"].view(np.uint32), o["mean"].view(np.uint32))
+    if "seg_clus" in z:
+        assert np.array_equal(g["clus"], z["seg_clus"])
+        assert np.array_equal(g["bdl"], z["seg_bdl"])
+
+
+@pytest.mark.parametrize("name", SCENES[:2])
+def test_hbp_bit_exact_vs_oracle(eng, golden_dir, name):
+    """Same pyramid, volume and WTA in: the engine's disparity and planes equal
+    the float oracle's bit for bit."""
+    import pyoracle as O
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L, R, D = z["left"], z["right"], int(z["D"])
+    H, W = L.shape[:2]
+    g = run_cost(E, ctx, torch, L, R, D)
+    ctx.segment_d(dev(torch, L), W, H)
+    pyr = ctx.pyramid()
+    disp = torch.zeros(H * W, dtype=torch.float32, device="cuda")
+    plane = torch.zeros(H * W * 3, dtype=torch.float32, device="cuda")
+    ctx.infer_d(g["vol_dev"], g["wta_dev"], D, E.default_params(), disp, plane)
+    torch.cuda.synchronize()
+    od, op, steps, _, _ = O.hbp(pyr, g["vol"], g["wta"], W, H, D)
+    gd = disp.cpu().numpy().reshape(H, W)
+    gp = plane.cpu().numpy().reshape(H, W, 3)
+    assert np.array_equal(gd.view(np.uint32), od.view(np.uint32)), float(np.mean(gd != od))
+    assert np.array_equal(gp.view(np.uint32), op.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", SCENES[:2])
+def test_post_process_vs_reference(eng, golden_dir, name):
+    """LR check + fill and the weighted median on the reference's own left/right
+    HBP results reproduce the reference's post-processed disparity."""
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L = z["left"]
+    H, W = L.shape[:2]
+    dL, dR = dev(torch, z["disp"]), dev(torch, z["disp_right"])
+    pl = dev(torch, z["plane"].astype(np.float32))
+    fail = torch.zeros(H * W, dtype=torch.uint8, device="cuda")
+    dout = torch.zeros(H * W, dtype=torch.float32, device="cuda")
+    ctx.lr_check_d(dL, dR, pl, fail, dout, W, H)
+    assert np.array_equal(dout.cpu().numpy().reshape(H, W), z["lr_disp"])
+    ctx.weighted_median_d(dev(torch, L), fail, pl, dout, W, H)
+    got = dout.cpu().numpy().reshape(H, W)
+    assert np.array_equal(got, z["post_disp"]), int((got != z["post_disp"]).sum())
+
+
+def test_driver_median_vs_oracle(eng):
+    import pyoracle as O
+    E, ctx, torch = eng
+    rng = np.random.default_rng(3)
+    d = rng.uniform(0, 60, (70, 90)).astype(np.float32)
+    d[rng.uniform(size=d.shape) < 0.05] = -1.0
+    t = dev(torch, d)
+    ctx.driver_median_d(t, 90, 70)
+    assert np.array_equal(t.cpu().numpy(), O.driver_median(d))
+
+
+@pytest.mark.parametrize("name", SCENES[:2])
+def test_run_pair_matches_oracle_pipeline(eng, golden_dir, name):
+    """The whole single-pair path through the host-buffer entry point equals the
+    oracle's pipeline (driver median included) bit for bit."""
+    import pyoracle as O
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L, R, D = z["left"], z["right"], int(z["D"])
+    disp = ctx.run_pair(L, R, D, E.default_params(post=1))
+    ref = O.driver_median(O.pipeline(L, R, D)["disp"])
+    assert np.array_equal(disp.view(np.uint32), ref.view(np.uint32)), float(np.mean(disp != ref))
