@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 HBP-ISP stereo engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one pass of the stereo path (census cost volume, segmentation
+pyramid, hierarchical BP, driver median) over a batch of 16 synthetic
+rectified pairs of 720x496 with D = 128: the quarter-scale batch workload.
+The scenes are seeded piecewise-planar synthetic pairs standing in for the
+Middlebury images the reference benchmarks on (data: "synthetic").
+
+One JSON line on rank 0:
+  value       pairs/s with the pairs already in device memory (hbp_run_batch_d)
+  e2e         pairs/s through hbp_run_pair on pinned host buffers (uploads the
+              pair and downloads the disparity inside the timed region), with
+              per-pair p50/p99 latency
+  roofline    the data-cost kernel (the dominant kernel): algorithmic bytes of
+              its launches / their CUDA-event time over the timed region
+              (first pair of every batch), against the measured HBM copy peak
+  cpu_baseline the CPU oracle (a port of the reference path, all host cores) on
+              one pair of the same workload
+  gpu_launches kernels this library launched inside the timed region
+With N > 1 (torchrun), every rank runs its own 16 pairs (replicas, weak
+scaling); the time is the max over ranks.
+
+--impl reference runs the reference's own build (oracle/_ref/libhbpref.so,
+compiled from the reference sources) through its classes, one pair per step,
+on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hbp-isp_b200"))
+
+METRIC = "pairs/s and p50/p99 latency at 720×496×D128, FP16-msg served vs plain FP32 path"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=16)
+    ap.add_argument("--W", type=int, default=720)
+    ap.add_argument("--H", type=int, default=496)
+    ap.add_argument("--D", type=int, default=128)
+    ap.add_argument("--fp16", type=int, default=0, help="store BP messages as FP16")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def make_pairs(n, W, H, D, seed0):
+    from scenes import make_scene
+    return [make_scene(W, H, D, seed0 + i) for i in range(n)]
+
+
+def cpu_baseline(scene, W, H, D):
+    """Oracle (CPU port of the reference path) on one pair, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    res = O.pipeline(scene.left, scene.right, D)
+    O.driver_median(res["disp"])
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "pairs/s", "cores": cores, "kind": "port",
+            "sample": f"1 pair {W}x{H} D{D} (seed {scene.seed}) through the CPU oracle, "
+                      f"OpenMP on {cores} threads, {dt:.1f} s"}
+
+
+def run_reference(args, rank):
+    """Reference arm: the reference's own build on the pairs of this workload."""
+    if rank != 0:
+        return
+    import ctypes as C
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libhbpref.so")
+    if not os.path.exists(lib_path):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhbpref.so not built "
+                          "(make -C oracle/ref needs the reference sources)"}))
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import pyoracle as O
+    from make_golden import RefLib
+    ref = RefLib(lib_path)
+    W, H, D = args.W, args.H, args.D
+    scenes = make_pairs(args.warmup + args.steps, W, H, D, 1000)
+    times = []
+    for i, s in enumerate(scenes):
+        t0 = time.perf_counter()
+        disp, _, _ = ref.hbp_pair(s.left, s.right, D)
+        O.driver_median(disp)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    val = len(times) / tot
+    lat = sorted(t * 1e3 for t in times)
+    out = {
+        "metric": METRIC, "value": val, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"1 synthetic pair {W}x{H} D{D} per step (sample of the 16-pair batch), "
+                               "reference build (its CUDA kernels, SegHAC/StereoCost/HBP_ISP classes) "
+                               "+ driver median", "W": W, "H": H, "D": D},
+        "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+        "cpu_baseline": {"value": val, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                         "sample": "one pair per step through the reference's own build, driven by one "
+                                   "host thread; the reference runs this path as CUDA kernels on the GPU"},
+        "e2e": {"value": val, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import hbp_b200 as E
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    W, H, D, NP = args.W, args.H, args.D, args.pairs
+    scenes = make_pairs(NP, W, H, D, 1000 + rank * NP)
+    ctx = E.Context(local, W * H, D)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    prm = E.default_params(msg_fp16=args.fp16, post=1)
+
+    dL = [torch.from_numpy(s.left).cuda() for s in scenes]
+    dR = [torch.from_numpy(s.right).cuda() for s in scenes]
+    disp = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in scenes]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    import ctypes as C
+    arrL = (C.c_void_p * NP)(*[t.data_ptr() for t in dL])
+    arrR = (C.c_void_p * NP)(*[t.data_ptr() for t in dR])
+    arrD = (C.c_void_p * NP)(*[t.data_ptr() for t in disp])
+
+    def step():
+        E._check(E.lib().hbp_run_batch_d(ctx.h, NP, arrL, arrR, W, H, D, C.byref(prm), arrD, None))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ------------------------------------------------------------ timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    E._check(E.lib().hbp_profile_enable(ctx.h, 2))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = E.lib().hbp_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.random_(0, 255)  # evict L2 between steps (not timed)
+            ev[k][0].record(stream)
+        step()
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = E.lib().hbp_launch_count() - l0
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    pms, plaunch, pbytes = C.c_double(), C.c_long(), C.c_double()
+    E._check(E.lib().hbp_profile_read(ctx.h, C.byref(pms), C.byref(plaunch), C.byref(pbytes)))
+    E._check(E.lib().hbp_profile_enable(ctx.h, 0))
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    total_pairs = NP * args.steps * world
+    value = total_pairs / (t_max / 1e3)
+
+    # ------------------------------------------------------------ end to end
+    e2e = None
+    lat = []
+    if not args.no_e2e:
+        pinL = [torch.from_numpy(s.left).pin_memory() for s in scenes]
+        pinR = [torch.from_numpy(s.right).pin_memory() for s in scenes]
+        out = torch.empty((H, W), dtype=torch.float32).pin_memory()
+        ctx.run_pair(pinL[0].numpy(), pinR[0].numpy(), D, prm)  # warm
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            for i in range(NP):
+                a = time.perf_counter()
+                E._check(E.lib().hbp_run_pair(ctx.h, C.c_void_p(pinL[i].data_ptr()), C.c_void_p(pinR[i].data_ptr()),
+                                              W, H, D, C.byref(prm), C.c_void_p(out.data_ptr()), None))
+                lat.append((time.perf_counter() - a) * 1e3)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": NP * args.steps * world / el, "unit": "pairs/s",
+               "h2d_bytes_per_step": NP * 2 * 3 * W * H, "d2h_bytes_per_step": NP * 4 * W * H}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(scenes[0], W, H, D)
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        achieved = (pbytes.value / (pms.value / 1e3)) / 1e9 if pms.value > 0 else None
+        lat.sort()
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "pairs/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f16-msg" if args.fp16 else "f32",
+            "data": "synthetic",
+            "config": {"workload": f"{NP} synthetic pairs {W}x{H} D{D} per step: census cost volume, "
+                                   "segmentation pyramid, HBP (min_level 2), driver median",
+                       "pairs_per_step": NP, "W": W, "H": H, "D": D,
+                       "msg": "fp16" if args.fp16 else "fp32", "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB buffer written between timed steps"},
+            "latency_ms": {"p50": lat[len(lat) // 2] if lat else None,
+                           "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None},
+            "roofline": {"kernel": "plane_cost_kernel (data cost of 4 candidate planes per pixel)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": None, "launches_timed": plaunch.value,
+                         "avg_launch_us": 1e3 * pms.value / max(1, plaunch.value)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "e2e": e2e,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

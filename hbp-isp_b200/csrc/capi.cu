@@ -10,6 +10,8 @@
 
 namespace hbp
 {
+std::atomic<long> g_launches{0};
+
 void Arena::init(size_t bytes)
 {
     release();
@@ -68,6 +70,8 @@ struct hbp_ctx
     float *wtab = nullptr; // weighted-median weight table (766 floats)
     long cap_pixels = 0;
     int cap_disp = 0;
+    KernelProf prof;
+    int prof_mode = 0; // 0 off, 1 every pair, 2 first pair of each batch call
 };
 
 namespace
@@ -149,9 +153,10 @@ void check_dims(int W, int H, int D)
         throw StatusError{HBP_ERR_INVALID_ARG, "need 16 <= W,H <= 65535 and 2 <= D <= min(1024, W-1)"};
 }
 
-HbpParams to_params(const hbp_params *p)
+HbpParams to_params(const hbp_params *p, KernelProf *prof = nullptr)
 {
     HbpParams q;
+    q.prof = prof;
     if (p)
     {
         q.alpha = p->alpha;
@@ -160,6 +165,60 @@ HbpParams to_params(const hbp_params *p)
         q.msg_fp16 = p->msg_fp16;
     }
     return q;
+}
+
+// The whole single-pair path on device inputs (main_stereo_hbp_isp.cu:33-76
+// for post 0/1, main_bench_middv3.cu:169-219 for post 2). Inputs and outputs
+// are caller buffers; intermediates come from the context's slabs, which the
+// caller has reset. Returns the plane buffer that holds the final planes.
+const float *pipeline_device(hbp_ctx *c, const uint8_t *dL, const uint8_t *dR, int W, int H, int D,
+                             const hbp_params &p, float *disp, float *plane)
+{
+    const long n = (long)W * H;
+    cudaStream_t st = c->st;
+    Arena &a = c->arena;
+    c->tmp.reset();
+    c->have_pyr = false;
+    HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
+    const int Wp = volume_pitch(W);
+    const bool lr = p.post == 2;
+    uint32_t *cL = a.alloc<uint32_t>(n), *cR = a.alloc<uint32_t>(n);
+    uint8_t *vol = a.alloc<uint8_t>((size_t)D * H * Wp);
+    uint8_t *volR = lr ? a.alloc<uint8_t>((size_t)D * H * Wp) : nullptr;
+    float *wta = a.alloc<float>(n), *wtaR = lr ? a.alloc<float>(n) : nullptr;
+    launch_cost(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR, st);
+    HbpParams q = to_params(&p, &c->prof);
+    size_t m = a.mark();
+    segment_image(dL, W, H, c->pyr, a, c->tmp, c->err_dev, st);
+    check_device_error(c);
+    c->tmp.reset();
+    hbp_infer(c->pyr, vol, Wp, wta, D, q, disp, plane, c->tmp, st);
+    if (lr)
+    {
+        a.rewind(m);
+        float *dispR = a.alloc<float>(n), *planeR = a.alloc<float>(3 * n);
+        uint8_t *fail1 = a.alloc<uint8_t>(n), *fail2 = a.alloc<uint8_t>(n);
+        float *plane2 = a.alloc<float>(3 * n);
+        Pyramid pr;
+        c->tmp.reset();
+        segment_image(dR, W, H, pr, a, c->tmp, c->err_dev, st);
+        check_device_error(c);
+        c->tmp.reset();
+        q.prof = nullptr;
+        hbp_infer(pr, volR, Wp, wtaR, D, q, dispR, planeR, c->tmp, st);
+        launch_lr_check(disp, dispR, plane, fail1, fail2, W, H, st);
+        c->tmp.reset();
+        launch_weighted_median(dL, fail1, plane, plane2, W, H, c->wtab, c->tmp, st);
+        launch_plane_to_disp(plane2, disp, W, H, st);
+        return plane2;
+    }
+    if (p.post == 1)
+    {
+        c->tmp.reset();
+        float *t = c->tmp.alloc<float>(n);
+        launch_driver_median(disp, t, W, H, st);
+    }
+    return plane;
 }
 } // namespace
 
@@ -439,55 +498,72 @@ hbp_status hbp_run_pair(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, in
         const long n = (long)W * H;
         ensure_capacity(c, n, D);
         cudaStream_t st = c->st;
-        Arena &a = c->arena;
-        a.reset();
-        c->tmp.reset();
-        c->have_pyr = false;
-        HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
-        const int Wp = volume_pitch(W);
-        const bool lr = p.post == 2;
-        uint8_t *dL = a.alloc<uint8_t>(3 * n), *dR = a.alloc<uint8_t>(3 * n);
-        uint32_t *cL = a.alloc<uint32_t>(n), *cR = a.alloc<uint32_t>(n);
-        uint8_t *vol = a.alloc<uint8_t>((size_t)D * H * Wp);
-        uint8_t *volR = lr ? a.alloc<uint8_t>((size_t)D * H * Wp) : nullptr;
-        float *wta = a.alloc<float>(n), *wtaR = lr ? a.alloc<float>(n) : nullptr;
-        float *disp = a.alloc<float>(n), *plane = a.alloc<float>(3 * n);
+        c->arena.reset();
+        uint8_t *dL = c->arena.alloc<uint8_t>(3 * n), *dR = c->arena.alloc<uint8_t>(3 * n);
+        float *disp = c->arena.alloc<float>(n), *plane = c->arena.alloc<float>(3 * n);
         HBP_CUDA(cudaMemcpyAsync(dL, bgrL, 3 * n, cudaMemcpyHostToDevice, st));
         HBP_CUDA(cudaMemcpyAsync(dR, bgrR, 3 * n, cudaMemcpyHostToDevice, st));
-        launch_cost(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR, st);
-        HbpParams q = to_params(&p);
-        size_t m = a.mark();
-        segment_image(dL, W, H, c->pyr, a, c->tmp, c->err_dev, st);
-        check_device_error(c);
-        c->tmp.reset();
-        hbp_infer(c->pyr, vol, Wp, wta, D, q, disp, plane, c->tmp, st);
-        if (lr)
-        {
-            a.rewind(m);
-            float *dispR = a.alloc<float>(n), *planeR = a.alloc<float>(3 * n);
-            uint8_t *fail1 = a.alloc<uint8_t>(n), *fail2 = a.alloc<uint8_t>(n);
-            float *plane2 = a.alloc<float>(3 * n);
-            Pyramid pr;
-            c->tmp.reset();
-            segment_image(dR, W, H, pr, a, c->tmp, c->err_dev, st);
-            check_device_error(c);
-            c->tmp.reset();
-            hbp_infer(pr, volR, Wp, wtaR, D, q, dispR, planeR, c->tmp, st);
-            launch_lr_check(disp, dispR, plane, fail1, fail2, W, H, st);
-            c->tmp.reset();
-            launch_weighted_median(dL, fail1, plane, plane2, W, H, c->wtab, c->tmp, st);
-            launch_plane_to_disp(plane2, disp, W, H, st);
-            plane = plane2;
-        }
-        else if (p.post == 1)
-        {
-            float *t = c->tmp.alloc<float>(n);
-            launch_driver_median(disp, t, W, H, st);
-        }
+        const float *planeo = pipeline_device(c, dL, dR, W, H, D, p, disp, plane);
         HBP_CUDA(cudaMemcpyAsync(disp_h, disp, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
         if (plane_h)
-            HBP_CUDA(cudaMemcpyAsync(plane_h, plane, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
+            HBP_CUDA(cudaMemcpyAsync(plane_h, planeo, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
         HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_run_batch_d(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, const uint8_t *const *bgrR,
+                           int W, int H, int D, const hbp_params *prm, float *const *disp,
+                           float *const *plane)
+{
+    if (!c || npairs < 0 || (npairs && (!bgrL || !bgrR || !disp)))
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    hbp_params def;
+    hbp_default_params(&def);
+    const hbp_params &p = prm ? *prm : def;
+    if (p.post < 0 || p.post > 2)
+        return fail(HBP_ERR_INVALID_ARG, "post must be 0, 1 or 2");
+    return guarded([&] {
+        check_dims(W, H, D);
+        HBP_CUDA(cudaSetDevice(c->device));
+        const long n = (long)W * H;
+        ensure_capacity(c, n, D);
+        for (int i = 0; i < npairs; ++i)
+        {
+            if (!bgrL[i] || !bgrR[i] || !disp[i])
+                throw StatusError{HBP_ERR_INVALID_ARG, "null pair pointer"};
+            c->arena.reset();
+            c->prof.on = c->prof_mode == 1 || (c->prof_mode == 2 && i == 0);
+            float *pl = plane && plane[i] ? plane[i] : c->arena.alloc<float>(3 * n);
+            const float *planeo = pipeline_device(c, bgrL[i], bgrR[i], W, H, D, p, disp[i], pl);
+            if (plane && plane[i] && planeo != pl)
+                HBP_CUDA(cudaMemcpyAsync(pl, planeo, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, c->st));
+        }
+        HBP_CUDA(cudaStreamSynchronize(c->st));
+    });
+}
+
+long hbp_launch_count(void) { return g_launches.load(); }
+
+hbp_status hbp_profile_enable(hbp_ctx *c, int on)
+{
+    if (!c)
+        return fail(HBP_ERR_INVALID_ARG, "null context");
+    if (on < 0 || on > 2)
+        return fail(HBP_ERR_INVALID_ARG, "profile mode must be 0, 1 or 2");
+    c->prof_mode = on;
+    c->prof.on = on != 0;
+    c->prof.reset();
+    return HBP_OK;
+}
+
+hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *bytes)
+{
+    if (!c || !ms || !launches || !bytes)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        *ms = c->prof.total_ms();
+        *launches = c->prof.launches;
+        *bytes = c->prof.bytes;
     });
 }
 

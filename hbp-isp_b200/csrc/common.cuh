@@ -1,6 +1,7 @@
 // Shared device/host helpers of the B200 HBP-ISP engine.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
@@ -36,6 +37,10 @@ struct StatusError
 };
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Number of kernels this library has launched (reported by the benchmark).
+extern std::atomic<long> g_launches;
+inline void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // Device-side error word: kernels that give up a bounded wait or meet an
 // impossible size record a code here instead of trapping; the host reads it.

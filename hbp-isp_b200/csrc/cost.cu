@@ -189,11 +189,13 @@ void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, 
 {
     dim3 cb(CT_W, CT_H), cg(ceil_div(W, CT_W), ceil_div(H, CT_H));
     census_pair_kernel<<<cg, cb, 0, st>>>(bgrL, bgrR, W, H, cL, cR);
+    note_launch();
     HBP_LAUNCH_CHECK();
     const int Wp = volume_pitch(W);
     size_t smem = sizeof(uint32_t) * 2 * (HM_SEG + D);
     dim3 hg(ceil_div(W, HM_SEG), H);
     hamming_wta_kernel<<<hg, HM_THREADS, smem, st>>>(cL, cR, W, H, D, Wp, vol, wta, volR, wtaR);
+    note_launch();
     HBP_LAUNCH_CHECK();
 }
 

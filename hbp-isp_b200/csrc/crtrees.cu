@@ -265,13 +265,16 @@ void crtrees_labels(const int *nn, int N, int *clus, int *num_dev, int *err_dev,
     void *args[] = {(void *)&nn, (void *)&N, (void *)&b, (void *)&label, (void *)&flags, (void *)&gb,
                     (void *)&err_dev};
     HBP_CUDA(cudaLaunchCooperativeKernel((const void *)crtrees_kernel, dim3(nb), dim3(CR_T), args, 0, st));
+    note_launch();
     // compact_clus_label: rank labels in increasing order
     int *used = b.C, *pos = b.Nb; // reuse
     HBP_CUDA(cudaMemsetAsync(used, 0, sizeof(int) * N, st));
     mark_used<<<ceil_div(N, 256), 256, 0, st>>>(label, N, used);
+    note_launch();
     HBP_LAUNCH_CHECK();
     exclusive_scan(used, pos, N, num_dev, tmp, st);
     remap_labels<<<ceil_div(N, 256), 256, 0, st>>>(label, pos, N, clus);
+    note_launch();
     HBP_LAUNCH_CHECK();
     tmp.rewind(m);
 }

@@ -96,12 +96,52 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
 
 // ---------------------------------------------------------------------------
 // hbp.cu
+// Event timing of the data-cost kernel (the dominant kernel) for the
+// roofline report: every launch is bracketed by events while enabled.
+struct KernelProf
+{
+    bool on = false;
+    std::vector<cudaEvent_t> ev; // start/stop pairs, reused
+    size_t used = 0;
+    double bytes = 0; // algorithmic bytes of the timed launches
+    long launches = 0;
+    void reset()
+    {
+        used = 0;
+        bytes = 0;
+        launches = 0;
+    }
+    void mark(cudaStream_t st)
+    {
+        if (used == ev.size())
+        {
+            cudaEvent_t e;
+            HBP_CUDA(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+        HBP_CUDA(cudaEventRecord(ev[used++], st));
+    }
+    double total_ms()
+    {
+        double t = 0;
+        for (size_t i = 0; i + 1 < used; i += 2)
+        {
+            float ms = 0;
+            HBP_CUDA(cudaEventSynchronize(ev[i + 1]));
+            HBP_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+            t += ms;
+        }
+        return t;
+    }
+};
+
 struct HbpParams
 {
     float alpha = 1000.1f;
     float tau_smooth = 0.6f;
     int min_level = 2;
     int msg_fp16 = 0;
+    KernelProf *prof = nullptr;
 };
 
 // HBP_ISP::run_ms on one pyramid: disp (HW floats) and plane (HW x 3).

@@ -687,6 +687,7 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
     uint32_t *kt = a.alloc<uint32_t>(HW), *ka = a.alloc<uint32_t>(HW), *va = a.alloc<uint32_t>(HW);
     int *cnt = a.alloc<int>(HW + 1);
     iota_int<<<blocks(HW, 256), 256, 0, st>>>(im, HW);
+    note_launch();
     HBP_LAUNCH_CHECK();
     for (int l = 0; l < L; ++l)
     {
@@ -707,8 +708,10 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
             uint32_t *pix = a.alloc<uint32_t>(HW);
             int *pix_off = a.alloc<int>(N + 1);
             iota_xy<<<blocks(HW, 256), 256, 0, st>>>(kt, pix, im, W, HW);
+            note_launch();
             HBP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (N + 1), st));
             count_keys<<<blocks(HW, 256), 256, 0, st>>>(im, HW, cnt);
+            note_launch();
             HBP_LAUNCH_CHECK();
             int bits = 1;
             while ((1 << bits) < N)
@@ -718,17 +721,22 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
             int *chunk_off = a.alloc<int>(N + 1);
             int *nch_total = a.alloc<int>(1);
             chunk_counts<<<blocks(N + 1, 256), 256, 0, st>>>(pix_off, N, cnt);
+            note_launch();
             exclusive_scan(cnt, chunk_off, N + 1, nch_total, a, st);
             d.nchunks = read_dev_int(nch_total, st);
             int *chunk_node = a.alloc<int>(d.nchunks);
             chunk_fill<<<blocks(N, 256), 256, 0, st>>>(chunk_off, N, chunk_node);
+            note_launch();
             HBP_LAUNCH_CHECK();
             int *rev = a.alloc<int>(E);
             reverse_ids<<<blocks(E, 256), 256, 0, st>>>(d.bd, d.nb_off, E, rev);
+            note_launch();
             float *ml = a.alloc<float>(3 * (size_t)N), *mx = a.alloc<float>(N), *my = a.alloc<float>(N);
             level_means<<<blocks(N, 256), 256, 0, st>>>(pyr.sums + 6 * pyr.node_off[l], N, mx, my, ml);
+            note_launch();
             float *dc = a.alloc<float>(2 * (size_t)E);
             edge_weights<<<blocks(E, 256), 256, 0, st>>>(d.bd, E, N, ml, mx, my, dc);
+            note_launch();
             HBP_LAUNCH_CHECK();
             d.pix = pix;
             d.pix_off = pix_off;
@@ -754,6 +762,7 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
         if (l + 1 < L)
         {
             compose_im_clus<<<blocks(HW, 256), 256, 0, st>>>(im, d.clus, HW, im2);
+            note_launch();
             HBP_LAUNCH_CHECK();
             std::swap(im, im2);
         }
@@ -766,14 +775,31 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
 
     auto cost_slots = [&](const LevelDev &d, int sb) {
         plane_cost_kernel<<<blocks((long)d.nchunks * 32, 256), 256, 0, st>>>(d, c, sb, pc);
+        note_launch();
         finalize_cost_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, pc, sb);
+        note_launch();
         HBP_LAUNCH_CHECK();
     };
+    KernelProf *prof = prm.prof && prm.prof->on ? prm.prof : nullptr;
     auto bp_step = [&](const LevelDev &d) {
+        if (prof)
+            prof->mark(st);
         plane_cost_kernel<<<blocks((long)d.nchunks * 32, 256), 256, 0, st>>>(d, c, 2 * P, pc);
+        note_launch();
+        if (prof)
+        {
+            prof->mark(st);
+            // compulsory bytes: per pixel its packed id (4 B) and two volume
+            // bytes per candidate; per node 4 planes in and 4 costs out
+            prof->bytes += (double)HW * (4 + 2 * P) + (double)d.N * P * (16 + 4);
+            prof->launches++;
+        }
         bp_edge_kernel<<<blocks(d.E, BE), dim3(BE, K), 0, st>>>(d, c, msg, msg_t);
+        note_launch();
         bp_node_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, pc, msg_t);
+        note_launch();
         bp_edge2_kernel<<<blocks(d.E, 128), 128, 0, st>>>(d, msg_t, msg);
+        note_launch();
         HBP_LAUNCH_CHECK();
     };
 
@@ -783,10 +809,12 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
         const LevelDev &d = lv[li], &h = lv[li + 1];
         HBP_CUDA(cudaMemsetAsync(msg, 0, sizeof(float) * (size_t)d.E * K, st));
         init_level_kernel<<<blocks(std::max(d.N, d.Nh), 128), 128, 0, st>>>(d, h, s_nb, s_ransac, s_child);
+        note_launch();
         HBP_LAUNCH_CHECK();
         cost_slots(d, 0);
         cost_slots(d, P);
         copy_cost_to_belief<<<blocks((long)d.N * K, 256), 256, 0, st>>>(d);
+        note_launch();
         HBP_LAUNCH_CHECK();
         const int iter_bp = 10 + 10 * li;
         float max_dz = (float)D / 2.0f * (float)li / (float)L;
@@ -797,17 +825,25 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
             for (int it = 0;; ++it)
             {
                 if (it <= 3)
+                {
                     ransac_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, c, s_ransac);
+                    note_launch();
+                }
                 else if (it <= 4)
                 {
                     select_child_kernel<<<blocks(h.N, 128), 128, 0, st>>>(d, h, s_child);
+                    note_launch();
                     neighbor_kernel<<<blocks(h.N, 128), 128, 0, st>>>(h, s_nb, buf);
+                    note_launch();
                     buf_to_candidates<<<blocks(h.N, 128), 128, 0, st>>>(h, buf);
+                    note_launch();
                     set_candidate_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, h);
+                    note_launch();
                 }
                 else if (it <= iter_random && max_dz >= 0.01f)
                 {
                     random_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, s_ransac, max_dz, max_dn);
+                    note_launch();
                     max_dz /= 2.0f;
                     max_dn /= 2.0f;
                 }
@@ -820,6 +856,7 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
     }
     const LevelDev &d = lv[m];
     map_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, c, disp, plane_out);
+    note_launch();
     HBP_LAUNCH_CHECK();
     HBP_CUDA(cudaStreamSynchronize(st));
     a.rewind(mark);

@@ -40,6 +40,7 @@ __global__ void lab_kernel(const uint8_t *__restrict__ bgr, int n, float4 *__res
 void launch_lab(const uint8_t *bgr, int n, float4 *lab, cudaStream_t st)
 {
     lab_kernel<<<ceil_div(n, 256), 256, 0, st>>>(bgr, n, lab);
+    note_launch();
     HBP_LAUNCH_CHECK();
 }
 } // namespace hbp

@@ -279,14 +279,18 @@ void launch_lr_check(const float *dispL, const float *dispR, float *planeL, uint
 {
     int n = W * H;
     lr_fail_kernel<<<ceil_div(n, 256), 256, 0, st>>>(dispL, dispR, W, H, fail);
+    note_launch();
     dilate3_kernel<<<ceil_div(n, 256), 256, 0, st>>>(fail, W, H, fail2);
+    note_launch();
     lr_fill_kernel<<<ceil_div(n, 256), 256, 0, st>>>(fail, fail2, W, H, planeL);
+    note_launch();
     HBP_LAUNCH_CHECK();
 }
 
 void launch_plane_to_disp(const float *plane, float *disp, int W, int H, cudaStream_t st)
 {
     plane_to_disp_kernel<<<ceil_div(W * H, 256), 256, 0, st>>>(plane, W, H, disp);
+    note_launch();
     HBP_LAUNCH_CHECK();
 }
 
@@ -306,6 +310,7 @@ void launch_weighted_median(const uint8_t *bgr, const uint8_t *fail, const float
     HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int), st));
     HBP_CUDA(cudaMemcpyAsync(plane_out, plane_in, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st));
     compact_fail<<<ceil_div(n, 256), 256, 0, st>>>(fail, n, list, count);
+    note_launch();
     HBP_LAUNCH_CHECK();
     int nf = 0;
     HBP_CUDA(cudaMemcpyAsync(&nf, count, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -313,6 +318,7 @@ void launch_weighted_median(const uint8_t *bgr, const uint8_t *fail, const float
     if (nf > 0)
     {
         weighted_median_kernel<<<nf, WM_T, 0, st>>>(bgr, list, W, H, plane_in, plane_out, wtab);
+        note_launch();
         HBP_LAUNCH_CHECK();
     }
     tmp.rewind(m);
@@ -323,7 +329,9 @@ void launch_driver_median(float *disp, float *tmp, int W, int H, cudaStream_t st
     int n = W * H;
     HBP_CUDA(cudaMemsetAsync(tmp, 0, sizeof(float) * n, st));
     median_h_kernel<<<ceil_div(n, 256), 256, 0, st>>>(disp, W, H, tmp);
+    note_launch();
     median_v_kernel<<<ceil_div(n, 256), 256, 0, st>>>(tmp, W, H, disp);
+    note_launch();
     HBP_LAUNCH_CHECK();
 }
 

@@ -85,12 +85,14 @@ void scan_rec(const int *in, int *out, long n, Arena &tmp, cudaStream_t st)
     long tiles = (n + STILE - 1) / STILE;
     int *sums = tmp.alloc<int>(tiles);
     scan_tiles<<<(int)tiles, ST, 0, st>>>(in, out, n, sums);
+    note_launch();
     HBP_LAUNCH_CHECK();
     if (tiles > 1)
     {
         int *soff = tmp.alloc<int>(tiles);
         scan_rec(sums, soff, tiles, tmp, st);
         add_tile_offsets<<<ceil_div(n, 256), 256, 0, st>>>(out, n, soff);
+        note_launch();
         HBP_LAUNCH_CHECK();
     }
 }
@@ -183,11 +185,13 @@ void radix_sort_impl(KT *keys, uint32_t *vals, KT *keys_alt, uint32_t *vals_alt,
     {
         int shift = 8 * p;
         radix_hist<KT><<<ntiles, RT, 0, st>>>(ka, n, shift, hist, ntiles);
+        note_launch();
         HBP_LAUNCH_CHECK();
         size_t m2 = tmp.mark();
         scan_rec(hist, offs, (long)256 * ntiles, tmp, st);
         tmp.rewind(m2);
         radix_scatter<KT, HAS_VAL><<<ntiles, RT, 0, st>>>(ka, va, kb, vb, n, shift, offs, ntiles);
+        note_launch();
         HBP_LAUNCH_CHECK();
         std::swap(ka, kb);
         std::swap(va, vb);
@@ -210,6 +214,7 @@ void exclusive_scan(const int *in, int *out, long n, int *total_dev, Arena &tmp,
     if (total_dev)
     {
         write_total<<<1, 1, 0, st>>>(in, out, n, total_dev);
+        note_launch();
         HBP_LAUNCH_CHECK();
     }
     tmp.rewind(m);

@@ -258,6 +258,7 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
 
     launch_lab(bgr, N0, lab, st);
     nn_grid_kernel<<<ceil_div(N0, 256), 256, 0, st>>>(lab, W, H, nn, dmin, pyr.bd, pyr.bdl, pyr.sums);
+    note_launch();
     HBP_LAUNCH_CHECK();
 
     int N = N0;
@@ -283,7 +284,9 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         pyr.child_base.push_back(och);
         HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (Nn + 1), st));
         copy_keys<<<ceil_div(N, 256), 256, 0, st>>>(clus, N, ck, count);
+        note_launch();
         iota_u32<<<ceil_div(N, 256), 256, 0, st>>>(child, N);
+        note_launch();
         HBP_LAUNCH_CHECK();
         radix_sort_pairs_u32(ck, child, ck_alt, cv_alt, N, bits_for(Nn), tmp, st);
         exclusive_scan(count, child_off, Nn + 1, nullptr, tmp, st);
@@ -293,6 +296,7 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         pyr.nb_base.push_back(onb);
         HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (N + 1), st));
         edge_src_count<<<ceil_div(E, 256), 256, 0, st>>>(pyr.bd + ob, (int)E, count);
+        note_launch();
         HBP_LAUNCH_CHECK();
         exclusive_scan(count, nb_off, N + 1, nullptr, tmp, st);
         onb += N + 1;
@@ -309,9 +313,11 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         // reduce_boundary_dist
         int bits = bits_for(Nn);
         map_edges<<<ceil_div(E, 256), 256, 0, st>>>(bd_c, clus, E, bits, keys);
+        note_launch();
         HBP_LAUNCH_CHECK();
         radix_sort_keys_u64(keys, keys_alt, E, 2 * bits, tmp, st);
         run_flags<<<ceil_div(E, 256), 256, 0, st>>>(keys, E, bits, keep);
+        note_launch();
         HBP_LAUNCH_CHECK();
         exclusive_scan(keep, slot, E, num_dev + 1, tmp, st);
         int E2 = read_int(num_dev + 1, st);
@@ -319,17 +325,21 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
             throw StatusError{HBP_ERR_INTERNAL, "edge capacity exceeded"};
         HBP_CUDA(cudaMemsetAsync(bdl_p, 0, sizeof(int) * E2, st));
         emit_edges<<<ceil_div(E, 256), 256, 0, st>>>(keys, keep, slot, bdl_c, E, bits, bd_p, bdl_p);
+        note_launch();
         HBP_LAUNCH_CHECK();
         // sums, means, inner max (reduce_data_mean, compute_dist_inner_max)
         parent_sums<<<ceil_div(Nn, 128), 128, 0, st>>>(child, child_off, sums_c, N, dmin, Nn, sums_p,
                                                          dmax, mean);
+        note_launch();
         HBP_LAUNCH_CHECK();
         // CSR of the new edges for the per-node minimum
         HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (Nn + 1), st));
         edge_src_count<<<ceil_div(E2, 256), 256, 0, st>>>(bd_p, E2, count);
+        note_launch();
         HBP_LAUNCH_CHECK();
         exclusive_scan(count, slot, Nn + 1, nullptr, tmp, st);
         node_1nn<<<ceil_div(Nn, 128), 128, 0, st>>>(bd_p, slot, Nn, mean, dmax, nn2, dmin2);
+        note_launch();
         HBP_LAUNCH_CHECK();
         std::swap(nn, nn2);
         std::swap(dmin, dmin2);

@@ -126,6 +126,25 @@ hbp_status hbp_driver_median_d(hbp_ctx *ctx, float *disp, int W, int H, void *st
 hbp_status hbp_run_pair(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H,
                         int D, const hbp_params *prm, float *disp, float *plane);
 
+/* A batch of same-size pairs whose images already sit in device memory
+ * (arrays of npairs device pointers, held on the host); plane may be NULL or
+ * hold NULL entries. Same path and outputs as hbp_run_pair per pair. */
+hbp_status hbp_run_batch_d(hbp_ctx *ctx, int npairs, const uint8_t *const *bgrL,
+                           const uint8_t *const *bgrR, int W, int H, int D, const hbp_params *prm,
+                           float *const *disp, float *const *plane);
+
+/* -------------------------------------------------------- measurement */
+
+/* Number of kernels the library has launched since it was loaded. */
+long hbp_launch_count(void);
+/* While enabled, launches of the data-cost kernel (the dominant kernel of the
+ * path) are bracketed by CUDA events on the context stream: mode 1 times every
+ * launch, mode 2 only those of the first pair of each hbp_run_batch_d call
+ * (0 = off). Read returns the summed device time, the launch count and the
+ * algorithmic bytes of the timed launches. Enabling resets the totals. */
+hbp_status hbp_profile_enable(hbp_ctx *ctx, int on);
+hbp_status hbp_profile_read(hbp_ctx *ctx, double *ms, long *launches, double *bytes);
+
 #ifdef __cplusplus
 }
 #endif
