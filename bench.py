@@ -246,6 +246,9 @@ def main():
         dist.barrier()
     launches = E.lib().hbp_launch_count() - l0
     clk = clocks.stop()
+    ph = (C.c_double * 4)()
+    E._check(E.lib().hbp_last_phase_ms(ctx.h, ph))
+    phases = {"prepare": ph[0], "bp": ph[1], "post": ph[2], "total": ph[3]}
     ms = sum(a.elapsed_time(b) for a, b in ev)
     pms, plaunch, pbytes = C.c_double(), C.c_long(), C.c_double()
     E._check(E.lib().hbp_profile_read(ctx.h, C.byref(pms), C.byref(plaunch), C.byref(pbytes)))
@@ -322,6 +325,7 @@ def main():
             "clocks": clk,
             "e2e": e2e,
             "gpu_launches": launches,
+            "phase_ms_last_step": phases,
         }
         print(json.dumps(line))
     if dist:

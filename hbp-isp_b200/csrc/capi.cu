@@ -3,8 +3,12 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <new>
 #include <string>
+#include <cstdlib>
+#include <chrono>
+#include <thread>
 
 #include "engine.h"
 
@@ -58,25 +62,50 @@ void *Arena::raw(size_t bytes, size_t align)
 
 using namespace hbp;
 
-struct hbp_ctx
+// Per-stream state: one lane runs one pair at a time. The context itself is
+// lane 0 (used by the stage entry points); batches add lanes so that pairs
+// run concurrently, each lane driven by its own host thread.
+struct Lane
 {
     int device = 0;
     cudaStream_t st = nullptr;
     Arena arena; // pipeline buffers and pyramid
-    Arena tmp;   // scratch of sorts / scans / segmentation
+    Arena tmp;   // scratch of sorts / scans / segmentation / BP levels
     Pyramid pyr;
     bool have_pyr = false;
     int *err_dev = nullptr;
-    float *wtab = nullptr; // weighted-median weight table (766 floats)
     long cap_pixels = 0;
     int cap_disp = 0;
+    int bp_blocks = 0; // grid of the persistent BP kernel (0 = whole device)
     KernelProf prof;
-    int prof_mode = 0; // 0 off, 1 every pair, 2 first pair of each batch call
+};
+
+// Device memory of one pair while its batch is in flight: cost volume(s),
+// pyramid(s), per-level BP data and outputs of the right view.
+struct Slot
+{
+    Arena mem;
+    long cap_pixels = 0;
+    int cap_disp = 0;
+    Pyramid pyr, pyrR;
+    ViewPlan plan, planR;
+    float *dispR = nullptr, *planeR = nullptr, *plane = nullptr;
+};
+
+struct hbp_ctx : Lane
+{
+    float *wtab = nullptr; // weighted-median weight table (766 floats)
+    int prof_mode = 0;     // 0 off, 1 every pair, 2 first pair of each batch call
+    int max_lanes = 8;
+    std::vector<std::unique_ptr<Lane>> lanes; // extra lanes (1..)
+    std::vector<std::unique_ptr<Slot>> slots;
+    double phase_ms[4] = {0, 0, 0, 0}; // last batch: prepare, bp, post, total
 };
 
 namespace
 {
 thread_local std::string g_err;
+thread_local std::string g_lane_err; // message of a failed batch lane
 
 hbp_status fail(hbp_status s, const std::string &msg)
 {
@@ -117,7 +146,7 @@ size_t slab_bytes(long pixels, int D)
 }
 size_t tmp_bytes(long pixels) { return (size_t)pixels * 480 + ((size_t)64 << 20); }
 
-void ensure_capacity(hbp_ctx *c, long pixels, int D)
+void ensure_capacity(Lane *c, long pixels, int D)
 {
     if (pixels <= c->cap_pixels && D <= c->cap_disp)
         return;
@@ -132,7 +161,7 @@ void ensure_capacity(hbp_ctx *c, long pixels, int D)
     c->cap_disp = nd;
 }
 
-void check_device_error(hbp_ctx *c)
+void check_device_error(Lane *c)
 {
     int h = 0;
     HBP_CUDA(cudaMemcpyAsync(&h, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -167,58 +196,134 @@ HbpParams to_params(const hbp_params *p, KernelProf *prof = nullptr)
     return q;
 }
 
-// The whole single-pair path on device inputs (main_stereo_hbp_isp.cu:33-76
-// for post 0/1, main_bench_middv3.cu:169-219 for post 2). Inputs and outputs
-// are caller buffers; intermediates come from the context's slabs, which the
-// caller has reset. Returns the plane buffer that holds the final planes.
-const float *pipeline_device(hbp_ctx *c, const uint8_t *dL, const uint8_t *dR, int W, int H, int D,
-                             const hbp_params &p, float *disp, float *plane)
+void ensure_slot(Slot *sl, long pixels, int D)
+{
+    if (pixels <= sl->cap_pixels && D <= sl->cap_disp)
+        return;
+    long np = std::max(pixels, sl->cap_pixels);
+    int nd = std::max(D, sl->cap_disp);
+    sl->mem.init(slab_bytes(np, nd));
+    sl->cap_pixels = np;
+    sl->cap_disp = nd;
+}
+
+// Stages of one pair before BP (main_stereo_hbp_isp.cu:33-64; right view of
+// main_bench_middv3.cu:189-202 when post == 2): cost volume(s), segmentation
+// pyramid(s) and BP level setup, all on the lane's stream; persistent data in
+// the pair's slot.
+void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint8_t *dR, int W, int H,
+                  int D, const hbp_params &p, float *disp, float *plane)
 {
     const long n = (long)W * H;
-    cudaStream_t st = c->st;
-    Arena &a = c->arena;
-    c->tmp.reset();
-    c->have_pyr = false;
-    HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
-    const int Wp = volume_pitch(W);
+    cudaStream_t st = L->st;
+    Arena &a = sl->mem;
+    a.reset();
+    L->tmp.reset();
+    HBP_CUDA(cudaMemsetAsync(L->err_dev, 0, sizeof(int), st));
+    const int Dp = volume_pitch(D);
     const bool lr = p.post == 2;
     uint32_t *cL = a.alloc<uint32_t>(n), *cR = a.alloc<uint32_t>(n);
-    uint8_t *vol = a.alloc<uint8_t>((size_t)D * H * Wp);
-    uint8_t *volR = lr ? a.alloc<uint8_t>((size_t)D * H * Wp) : nullptr;
+    uint8_t *vol = a.alloc<uint8_t>((size_t)Dp * n);
+    uint8_t *volR = lr ? a.alloc<uint8_t>((size_t)Dp * n) : nullptr;
     float *wta = a.alloc<float>(n), *wtaR = lr ? a.alloc<float>(n) : nullptr;
-    launch_cost(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR, st);
-    HbpParams q = to_params(&p, &c->prof);
-    size_t m = a.mark();
-    segment_image(dL, W, H, c->pyr, a, c->tmp, c->err_dev, st);
-    check_device_error(c);
-    c->tmp.reset();
-    hbp_infer(c->pyr, vol, Wp, wta, D, q, disp, plane, c->tmp, st);
+    sl->plane = plane ? plane : a.alloc<float>(3 * n);
+    {
+        NvtxRange r("cost_volume");
+        launch_cost(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR, st);
+    }
+    HbpParams q = to_params(&p);
+    {
+        NvtxRange r("segmentation");
+        segment_image(dL, W, H, sl->pyr, a, L->tmp, L->err_dev, st);
+        check_device_error(L);
+    }
+    L->tmp.reset();
+    {
+        NvtxRange r("bp_setup");
+        hbp_prepare(sl->pyr, vol, Dp, wta, D, q, disp, sl->plane, a, L->tmp, st, sl->plan);
+    }
     if (lr)
     {
-        a.rewind(m);
-        float *dispR = a.alloc<float>(n), *planeR = a.alloc<float>(3 * n);
-        uint8_t *fail1 = a.alloc<uint8_t>(n), *fail2 = a.alloc<uint8_t>(n);
-        float *plane2 = a.alloc<float>(3 * n);
-        Pyramid pr;
-        c->tmp.reset();
-        segment_image(dR, W, H, pr, a, c->tmp, c->err_dev, st);
-        check_device_error(c);
-        c->tmp.reset();
-        q.prof = nullptr;
-        hbp_infer(pr, volR, Wp, wtaR, D, q, dispR, planeR, c->tmp, st);
-        launch_lr_check(disp, dispR, plane, fail1, fail2, W, H, st);
-        c->tmp.reset();
-        launch_weighted_median(dL, fail1, plane, plane2, W, H, c->wtab, c->tmp, st);
-        launch_plane_to_disp(plane2, disp, W, H, st);
-        return plane2;
+        sl->dispR = a.alloc<float>(n);
+        sl->planeR = a.alloc<float>(3 * n);
+        L->tmp.reset();
+        segment_image(dR, W, H, sl->pyrR, a, L->tmp, L->err_dev, st);
+        check_device_error(L);
+        L->tmp.reset();
+        hbp_prepare(sl->pyrR, volR, Dp, wtaR, D, q, sl->dispR, sl->planeR, a, L->tmp, st, sl->planR);
     }
-    if (p.post == 1)
+    HBP_CUDA(cudaStreamSynchronize(st));
+}
+
+// Stages after BP: the driver's median (post 1) or LR check + fill, weighted
+// median and plane -> disparity (post 2). Returns the final plane buffer.
+const float *finish_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, int W, int H,
+                         const hbp_params &p, float *disp)
+{
+    const long n = (long)W * H;
+    cudaStream_t st = L->st;
+    if (p.post == 2)
     {
-        c->tmp.reset();
-        float *t = c->tmp.alloc<float>(n);
+        size_t m = sl->mem.mark();
+        uint8_t *fail1 = sl->mem.alloc<uint8_t>(n), *fail2 = sl->mem.alloc<uint8_t>(n);
+        float *plane2 = sl->mem.alloc<float>(3 * n);
+        launch_lr_check(disp, sl->dispR, sl->plane, fail1, fail2, W, H, st);
+        L->tmp.reset();
+        launch_weighted_median(dL, fail1, sl->plane, plane2, W, H, ctx->wtab, L->tmp, st);
+        launch_plane_to_disp(plane2, disp, W, H, st);
+        HBP_CUDA(cudaMemcpyAsync(sl->plane, plane2, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, st));
+        sl->mem.rewind(m);
+    }
+    else if (p.post == 1)
+    {
+        L->tmp.reset();
+        float *t = L->tmp.alloc<float>(n);
         launch_driver_median(disp, t, W, H, st);
     }
-    return plane;
+    return sl->plane;
+}
+
+void lane_init(Lane *l, int device)
+{
+    l->device = device;
+    HBP_CUDA(cudaSetDevice(device));
+    HBP_CUDA(cudaStreamCreateWithFlags(&l->st, cudaStreamNonBlocking));
+    HBP_CUDA(cudaMalloc(&l->err_dev, sizeof(int) * 4));
+    HBP_CUDA(cudaMemset(l->err_dev, 0, sizeof(int) * 4));
+}
+
+void lane_release(Lane *l)
+{
+    if (l->st)
+        cudaStreamSynchronize(l->st);
+    l->arena.release();
+    l->tmp.release();
+    if (l->err_dev)
+        cudaFree(l->err_dev);
+    if (l->st)
+        cudaStreamDestroy(l->st);
+    l->st = nullptr;
+    l->err_dev = nullptr;
+}
+
+Slot *slot_at(hbp_ctx *c, int i)
+{
+    while ((int)c->slots.size() <= i)
+        c->slots.push_back(std::make_unique<Slot>());
+    return c->slots[i].get();
+}
+
+Lane *lane_at(hbp_ctx *c, int i)
+{
+    if (i == 0)
+        return c;
+    while ((int)c->lanes.size() < i)
+    {
+        auto l = std::make_unique<Lane>();
+        lane_init(l.get(), c->device);
+        c->lanes.push_back(std::move(l));
+    }
+    return c->lanes[i - 1].get();
 }
 } // namespace
 
@@ -263,11 +368,9 @@ hbp_status hbp_ctx_create(int device, long max_pixels, int max_disp, hbp_ctx **o
     if (!c)
         return fail(HBP_ERR_OUT_OF_MEMORY, "host allocation failed");
     hbp_status s = guarded([&] {
-        c->device = device;
-        HBP_CUDA(cudaSetDevice(device));
-        HBP_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
-        HBP_CUDA(cudaMalloc(&c->err_dev, sizeof(int) * 4));
-        HBP_CUDA(cudaMemset(c->err_dev, 0, sizeof(int) * 4));
+        lane_init(c, device);
+        if (const char *e = std::getenv("HBP_LANES"))
+            c->max_lanes = std::max(1, std::min(64, std::atoi(e)));
         float tab[766];
         median_weight_table(tab);
         HBP_CUDA(cudaMalloc(&c->wtab, sizeof(tab)));
@@ -289,22 +392,21 @@ void hbp_ctx_destroy(hbp_ctx *c)
     if (!c)
         return;
     cudaSetDevice(c->device);
-    if (c->st)
-        cudaStreamSynchronize(c->st);
-    c->arena.release();
-    c->tmp.release();
-    if (c->err_dev)
-        cudaFree(c->err_dev);
+    for (auto &l : c->lanes)
+        lane_release(l.get());
+    c->lanes.clear();
+    for (auto &sl : c->slots)
+        sl->mem.release();
+    c->slots.clear();
     if (c->wtab)
         cudaFree(c->wtab);
-    if (c->st)
-        cudaStreamDestroy(c->st);
+    lane_release(c);
     delete c;
 }
 
 void *hbp_ctx_stream(hbp_ctx *c) { return c ? (void *)c->st : nullptr; }
 
-int hbp_volume_pitch(int W) { return volume_pitch(W); }
+int hbp_volume_pitch(int D) { return volume_pitch(D); }
 
 hbp_status hbp_cost_census_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
                              uint32_t *censusL, uint32_t *censusR, uint8_t *vol, float *wta,
@@ -421,9 +523,15 @@ hbp_status hbp_infer_d(hbp_ctx *c, const uint8_t *vol, const float *wta, int D, 
         HBP_CUDA(cudaSetDevice(c->device));
         check_dims(c->pyr.W, c->pyr.H, D);
         cudaStream_t st = pick(c, stream);
-        HbpParams q = to_params(prm);
+        HbpParams q = to_params(prm, c->prof.on ? &c->prof : nullptr);
+        Slot *sl = slot_at(c, 0);
+        ensure_slot(sl, (long)c->pyr.W * c->pyr.H, D);
+        sl->mem.reset();
         c->tmp.reset();
-        hbp_infer(c->pyr, vol, volume_pitch(c->pyr.W), wta, D, q, disp, plane, c->tmp, st);
+        hbp_prepare(c->pyr, vol, volume_pitch(D), wta, D, q, disp, plane, sl->mem, c->tmp, st, sl->plan);
+        c->tmp.reset();
+        std::vector<ViewPlan *> views{&sl->plan};
+        hbp_run_views(views, q, c->tmp, st);
     });
 }
 
@@ -482,6 +590,92 @@ hbp_status hbp_driver_median_d(hbp_ctx *c, float *disp, int W, int H, void *stre
     });
 }
 
+namespace
+{
+// Every pair of a batch: preparation on the lanes (one host thread each),
+// batched BP of all views on lane 0, then the post stages per pair.
+void run_pairs(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, const uint8_t *const *bgrR, int W,
+               int H, int D, const hbp_params &p, float *const *disp, float *const *plane)
+{
+    const long n = (long)W * H;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t0) {
+        return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    };
+    for (double &x : c->phase_ms)
+        x = 0;
+    const auto t_all = clk::now();
+    const int views_per_pair = p.post == 2 ? 2 : 1;
+    const int group = 32 / views_per_pair; // pairs per BP batch
+    for (int g0 = 0; g0 < npairs; g0 += group)
+    {
+        const int ng = std::min(group, npairs - g0);
+        const int nl = std::max(1, std::min(c->max_lanes, ng));
+        std::vector<Lane *> lanes(nl);
+        for (int k = 0; k < nl; ++k)
+        {
+            lanes[k] = lane_at(c, k);
+            ensure_capacity(lanes[k], n, D);
+        }
+        for (int i = 0; i < ng; ++i)
+            ensure_slot(slot_at(c, i), n, D);
+        std::vector<hbp_status> st(nl, HBP_OK);
+        std::vector<std::string> msg(nl);
+        const auto t_prep = clk::now();
+        auto work = [&](int k) {
+            st[k] = guarded([&] {
+                HBP_CUDA(cudaSetDevice(c->device));
+                for (int i = k; i < ng; i += nl)
+                    prepare_pair(c, lanes[k], c->slots[i].get(), bgrL[g0 + i], bgrR[g0 + i], W, H, D, p,
+                                 disp[g0 + i], plane ? plane[g0 + i] : nullptr);
+            });
+            if (st[k] != HBP_OK)
+                msg[k] = g_err;
+        };
+        std::vector<std::thread> th;
+        for (int k = 1; k < nl; ++k)
+            th.emplace_back(work, k);
+        work(0);
+        for (auto &t : th)
+            t.join();
+        for (int k = 0; k < nl; ++k)
+            if (st[k] != HBP_OK)
+            {
+                g_lane_err = "lane " + std::to_string(k) + ": " + msg[k];
+                throw StatusError{st[k], g_lane_err.c_str()};
+            }
+        c->phase_ms[0] += ms_since(t_prep);
+        const auto t_bp = clk::now();
+        std::vector<ViewPlan *> views;
+        for (int i = 0; i < ng; ++i)
+        {
+            views.push_back(&c->slots[i]->plan);
+            if (p.post == 2)
+                views.push_back(&c->slots[i]->planR);
+        }
+        HbpParams q = to_params(&p, c->prof_mode ? &c->prof : nullptr);
+        c->prof.on = c->prof_mode != 0;
+        c->tmp.reset();
+        {
+            NvtxRange r("bp");
+            hbp_run_views(views, q, c->tmp, c->st);
+        }
+        c->phase_ms[1] += ms_since(t_bp);
+        const auto t_post = clk::now();
+        NvtxRange rp("post");
+        for (int i = 0; i < ng; ++i)
+        {
+            const float *po = finish_pair(c, c, c->slots[i].get(), bgrL[g0 + i], W, H, p, disp[g0 + i]);
+            if (plane && plane[g0 + i] && po != plane[g0 + i])
+                HBP_CUDA(cudaMemcpyAsync(plane[g0 + i], po, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, c->st));
+        }
+        HBP_CUDA(cudaStreamSynchronize(c->st));
+        c->phase_ms[2] += ms_since(t_post);
+    }
+    c->phase_ms[3] = ms_since(t_all);
+}
+} // namespace
+
 hbp_status hbp_run_pair(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
                         const hbp_params *prm, float *disp_h, float *plane_h)
 {
@@ -503,10 +697,24 @@ hbp_status hbp_run_pair(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, in
         float *disp = c->arena.alloc<float>(n), *plane = c->arena.alloc<float>(3 * n);
         HBP_CUDA(cudaMemcpyAsync(dL, bgrL, 3 * n, cudaMemcpyHostToDevice, st));
         HBP_CUDA(cudaMemcpyAsync(dR, bgrR, 3 * n, cudaMemcpyHostToDevice, st));
-        const float *planeo = pipeline_device(c, dL, dR, W, H, D, p, disp, plane);
+        HBP_CUDA(cudaStreamSynchronize(st));
+        const uint8_t *pl[1] = {dL}, *pr[1] = {dR};
+        float *pd[1] = {disp}, *pp[1] = {plane};
+        int keep = c->max_lanes;
+        c->max_lanes = 1;
+        try
+        {
+            run_pairs(c, 1, pl, pr, W, H, D, p, pd, pp);
+        }
+        catch (...)
+        {
+            c->max_lanes = keep;
+            throw;
+        }
+        c->max_lanes = keep;
         HBP_CUDA(cudaMemcpyAsync(disp_h, disp, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
         if (plane_h)
-            HBP_CUDA(cudaMemcpyAsync(plane_h, planeo, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
+            HBP_CUDA(cudaMemcpyAsync(plane_h, plane, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
         HBP_CUDA(cudaStreamSynchronize(st));
     });
 }
@@ -522,27 +730,34 @@ hbp_status hbp_run_batch_d(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, c
     const hbp_params &p = prm ? *prm : def;
     if (p.post < 0 || p.post > 2)
         return fail(HBP_ERR_INVALID_ARG, "post must be 0, 1 or 2");
+    for (int i = 0; i < npairs; ++i)
+        if (!bgrL[i] || !bgrR[i] || !disp[i])
+            return fail(HBP_ERR_INVALID_ARG, "null pair pointer");
     return guarded([&] {
         check_dims(W, H, D);
         HBP_CUDA(cudaSetDevice(c->device));
-        const long n = (long)W * H;
-        ensure_capacity(c, n, D);
-        for (int i = 0; i < npairs; ++i)
-        {
-            if (!bgrL[i] || !bgrR[i] || !disp[i])
-                throw StatusError{HBP_ERR_INVALID_ARG, "null pair pointer"};
-            c->arena.reset();
-            c->prof.on = c->prof_mode == 1 || (c->prof_mode == 2 && i == 0);
-            float *pl = plane && plane[i] ? plane[i] : c->arena.alloc<float>(3 * n);
-            const float *planeo = pipeline_device(c, bgrL[i], bgrR[i], W, H, D, p, disp[i], pl);
-            if (plane && plane[i] && planeo != pl)
-                HBP_CUDA(cudaMemcpyAsync(pl, planeo, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, c->st));
-        }
-        HBP_CUDA(cudaStreamSynchronize(c->st));
+        run_pairs(c, npairs, bgrL, bgrR, W, H, D, p, disp, plane);
     });
 }
 
+hbp_status hbp_set_lanes(hbp_ctx *c, int lanes)
+{
+    if (!c || lanes < 1 || lanes > 64)
+        return fail(HBP_ERR_INVALID_ARG, "lanes must be in [1, 64]");
+    c->max_lanes = lanes;
+    return HBP_OK;
+}
+
 long hbp_launch_count(void) { return g_launches.load(); }
+
+hbp_status hbp_last_phase_ms(hbp_ctx *c, double *out4)
+{
+    if (!c || !out4)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    for (int i = 0; i < 4; ++i)
+        out4[i] = c->phase_ms[i];
+    return HBP_OK;
+}
 
 hbp_status hbp_profile_enable(hbp_ctx *c, int on)
 {
@@ -553,6 +768,8 @@ hbp_status hbp_profile_enable(hbp_ctx *c, int on)
     c->prof_mode = on;
     c->prof.on = on != 0;
     c->prof.reset();
+    for (auto &l : c->lanes)
+        l->prof.reset();
     return HBP_OK;
 }
 
@@ -564,6 +781,7 @@ hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *byte
         *ms = c->prof.total_ms();
         *launches = c->prof.launches;
         *bytes = c->prof.bytes;
+
     });
 }
 

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "hbp_b200.h"
+#include <nvtx3/nvToolsExt.h>
 
 namespace hbp
 {
@@ -115,5 +116,13 @@ __device__ __forceinline__ int warp_sum_int(int v)
         v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+
+// NVTX range for profilers (stage and pyramid level names); no cost when no
+// tool is attached.
+struct NvtxRange
+{
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 } // namespace hbp

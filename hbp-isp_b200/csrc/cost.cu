@@ -7,10 +7,11 @@
 // HammingDistanceCostKernel (:148-207), cost_u1_to_f1_transpose (:209-228),
 // WTA_D_k (:248-280); right view: cost_to_right (:471-516).
 //
-// Layout: vol[d][y][x] with row pitch Wp = round_up(W, 16) bytes, so every
-// (d, y) row starts 16-byte aligned and the Hamming kernel stores 4 pixels per
-// 32-bit word. Values are min(popcount, 25) (exact in 8 bits; the reference's
-// float volume holds the same integers).
+// Layout: pixel-major vol[y][x][d] with Dp = round_up(D, 16) bytes per pixel
+// (entries d >= D are 0), so the data-cost kernel finds V[d] and V[d+1] of all
+// of a pixel's candidate planes in one 32-byte sector. Values are
+// min(popcount, 25) (exact in 8 bits; the reference's float volume holds the
+// same integers).
 #include "engine.h"
 
 namespace hbp
@@ -78,21 +79,24 @@ __global__ void __launch_bounds__(CT_W *CT_H)
     cR[(size_t)y * W + x] = b;
 }
 
-constexpr int HM_THREADS = 128, HM_PX = 4, HM_SEG = HM_THREADS * HM_PX; // 512 px per block
+constexpr int HM_THREADS = 128; // one pixel per thread, 128 pixels per block
 
-// One block = one 512-pixel row segment. Shared memory holds the left census
-// of the segment plus D columns to the right (right view) and the right
-// census of the segment plus D columns to the left (clamped at the image
-// border, which reproduces the reference's use of cR[row][0] for x-d < 0).
+// One block = 128 consecutive pixels of a row; thread = pixel. Shared memory
+// holds the left census of the segment plus D columns to the right (right
+// view) and the right census of the segment plus D columns to the left
+// (clamped at the image border, which reproduces the reference's use of
+// cR[row][0] for x-d < 0). Each thread writes its Dp cost bytes contiguously
+// in 16-byte words (pixel-major, like the reference's u8 volume
+// [px][D_align]).
 __global__ void __launch_bounds__(HM_THREADS)
     hamming_wta_kernel(const uint32_t *__restrict__ cL, const uint32_t *__restrict__ cR, int W,
-                       int H, int D, int Wp, uint8_t *__restrict__ vol, float *__restrict__ wta,
+                       int H, int D, int Dp, uint8_t *__restrict__ vol, float *__restrict__ wta,
                        uint8_t *__restrict__ volR, float *__restrict__ wtaR)
 {
     extern __shared__ uint32_t sm[];
     const int y = blockIdx.y;
-    const int xs = blockIdx.x * HM_SEG;
-    const int span = HM_SEG + D;
+    const int xs = blockIdx.x * HM_THREADS;
+    const int span = HM_THREADS + D;
     uint32_t *sLc = sm;        // cL[xs + i], i in [0, span)  (clamped to W-1)
     uint32_t *sRc = sm + span; // cR[xs - D + i], i in [0, span) (clamped to 0 / W-1)
     const uint32_t *rowL = cL + (size_t)y * W, *rowR = cR + (size_t)y * W;
@@ -104,84 +108,74 @@ __global__ void __launch_bounds__(HM_THREADS)
         sRc[i] = rowR[gr];
     }
     __syncthreads();
-    const int lx = threadIdx.x * HM_PX; // local x of the first of 4 pixels
-    const int x = xs + lx;
+    const int lx = threadIdx.x, x = xs + lx;
     if (x >= W)
         return;
-    const size_t plane = (size_t)H * Wp;
-    uint8_t *vrow = vol + (size_t)y * Wp + x;
-    uint32_t cl[HM_PX];
-#pragma unroll
-    for (int j = 0; j < HM_PX; ++j)
-        cl[j] = sLc[lx + j];
-    int best[HM_PX], arg[HM_PX];
-#pragma unroll
-    for (int j = 0; j < HM_PX; ++j)
+    const size_t px = (size_t)y * W + x;
+    const uint32_t cl = sLc[lx];
+    uint4 *out = reinterpret_cast<uint4 *>(vol + px * Dp);
+    int best = 1 << 30, arg = 0;
+    for (int d0 = 0; d0 < Dp; d0 += 16)
     {
-        best[j] = 1 << 30;
-        arg[j] = 0;
-    }
-    for (int d = 0; d < D; ++d)
-    {
-        uint32_t word = 0;
+        uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
-        for (int j = 0; j < HM_PX; ++j)
+        for (int j = 0; j < 16; ++j)
         {
-            // cR[max(x + j - d, 0)]: local index (lx + j - d) + D in sRc
-            int c = __popc(cl[j] ^ sRc[lx + j - d + D]);
-            c = c < 25 ? c : 25;
-            if (c < best[j])
+            int d = d0 + j;
+            int c = 0;
+            if (d < D)
             {
-                best[j] = c;
-                arg[j] = d;
+                // cR[max(x - d, 0)]: local index (lx - d) + D in sRc
+                c = __popc(cl ^ sRc[lx - d + D]);
+                c = c < 25 ? c : 25;
+                if (c < best)
+                {
+                    best = c;
+                    arg = d;
+                }
             }
-            word |= (uint32_t)c << (8 * j);
+            w[j >> 2] |= (uint32_t)c << (8 * (j & 3));
         }
-        *reinterpret_cast<uint32_t *>(vrow + (size_t)d * plane) = word;
+        out[d0 >> 4] = make_uint4(w[0], w[1], w[2], w[3]);
     }
-#pragma unroll
-    for (int j = 0; j < HM_PX; ++j)
-        if (x + j < W)
-            wta[(size_t)y * W + x + j] = (float)arg[j];
+    wta[px] = (float)arg;
     if (!volR)
         return;
-    // Right view: VR[d][y][x] = V[d][y][min(x + d, W - 1)] (convert_vol_L2R_k
+    // Right view: VR[y][x][d] = V[y][min(x + d, W - 1)][d] (convert_vol_L2R_k
     // followed by fill_out_of_view_k).
-    uint8_t *vrowR = volR + (size_t)y * Wp + x;
-#pragma unroll
-    for (int j = 0; j < HM_PX; ++j)
+    uint4 *outR = reinterpret_cast<uint4 *>(volR + px * Dp);
+    best = 1 << 30;
+    arg = 0;
+    for (int d0 = 0; d0 < Dp; d0 += 16)
     {
-        best[j] = 1 << 30;
-        arg[j] = 0;
-    }
-    for (int d = 0; d < D; ++d)
-    {
-        uint32_t word = 0;
+        uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
-        for (int j = 0; j < HM_PX; ++j)
+        for (int j = 0; j < 16; ++j)
         {
-            int xl = min(x + j + d, W - 1);      // source column in the left view
-            int xr = max(xl - d, 0);             // its match in the right view
-            int c = __popc(sLc[xl - xs] ^ sRc[xr - xs + D]);
-            c = c < 25 ? c : 25;
-            if (c < best[j])
+            int d = d0 + j;
+            int c = 0;
+            if (d < D)
             {
-                best[j] = c;
-                arg[j] = d;
+                int xl = min(x + d, W - 1); // source column in the left view
+                int xr = max(xl - d, 0);    // its match in the right view
+                c = __popc(sLc[xl - xs] ^ sRc[xr - xs + D]);
+                c = c < 25 ? c : 25;
+                if (c < best)
+                {
+                    best = c;
+                    arg = d;
+                }
             }
-            word |= (uint32_t)c << (8 * j);
+            w[j >> 2] |= (uint32_t)c << (8 * (j & 3));
         }
-        *reinterpret_cast<uint32_t *>(vrowR + (size_t)d * plane) = word;
+        outR[d0 >> 4] = make_uint4(w[0], w[1], w[2], w[3]);
     }
-#pragma unroll
-    for (int j = 0; j < HM_PX; ++j)
-        if (x + j < W)
-            wtaR[(size_t)y * W + x + j] = (float)arg[j];
+    wtaR[px] = (float)arg;
 }
 
 } // namespace
 
-int volume_pitch(int W) { return (W + 15) / 16 * 16; }
+int volume_pitch(int D) { return (D + 15) / 16 * 16; }
 
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
@@ -191,10 +185,10 @@ void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, 
     census_pair_kernel<<<cg, cb, 0, st>>>(bgrL, bgrR, W, H, cL, cR);
     note_launch();
     HBP_LAUNCH_CHECK();
-    const int Wp = volume_pitch(W);
-    size_t smem = sizeof(uint32_t) * 2 * (HM_SEG + D);
-    dim3 hg(ceil_div(W, HM_SEG), H);
-    hamming_wta_kernel<<<hg, HM_THREADS, smem, st>>>(cL, cR, W, H, D, Wp, vol, wta, volR, wtaR);
+    const int Dp = volume_pitch(D);
+    size_t smem = sizeof(uint32_t) * 2 * (HM_THREADS + D);
+    dim3 hg(ceil_div(W, HM_THREADS), H);
+    hamming_wta_kernel<<<hg, HM_THREADS, smem, st>>>(cL, cR, W, H, D, Dp, vol, wta, volR, wtaR);
     note_launch();
     HBP_LAUNCH_CHECK();
 }

@@ -231,8 +231,9 @@ int coop_blocks(int N)
         HBP_CUDA(cudaGetDevice(&dev));
         HBP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         HBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crtrees_kernel, CR_T, 0));
-        // leave room for concurrent work on other streams
-        max_blocks = sms * (per_sm > 2 ? 2 : per_sm);
+        // one block per SM: leaves room for concurrent lanes (each lane may
+        // run its own cooperative CRTrees launch)
+        max_blocks = sms * (per_sm > 1 ? 1 : per_sm);
         if (max_blocks < 1)
             max_blocks = 1;
     }

@@ -45,7 +45,7 @@ struct Scratch
 
 // ---------------------------------------------------------------------------
 // cost.cu
-int volume_pitch(int W);
+int volume_pitch(int D); // bytes per pixel of the pixel-major volume
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
                  cudaStream_t st);
@@ -144,9 +144,29 @@ struct HbpParams
     KernelProf *prof = nullptr;
 };
 
-// HBP_ISP::run_ms on one pyramid: disp (HW floats) and plane (HW x 3).
-void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta, int D,
-               const HbpParams &prm, float *disp, float *plane, Arena &a, cudaStream_t st);
+
+
+// One view ready for BP: per-level device data, BP buffers and its sizes.
+struct ViewPlan
+{
+    struct Impl;
+    Impl *impl;
+    int L = 0, min_level = 0, D = 0, HW = 0;
+    std::vector<int> levelN, levelE, levelC; // nodes, edges, data-cost chunks per level
+    ViewPlan();
+    ~ViewPlan();
+    ViewPlan(const ViewPlan &) = delete;
+    ViewPlan &operator=(const ViewPlan &) = delete;
+};
+
+// Level setup of one view (persistent data in `persist`, temporaries in `tmp`);
+// BP writes disparity (HW floats) and planes (HW x 3, may be null) there.
+void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wta, int D,
+                 const HbpParams &prm, float *disp, float *plane, Arena &persist, Arena &tmp,
+                 cudaStream_t st, ViewPlan &vp);
+// HBP_ISP::run_ms for up to 32 prepared views at once (same min_level).
+void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &tmp,
+                   cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // post.cu

@@ -22,6 +22,7 @@
 // like the CPU oracle.
 #include <algorithm>
 #include <cfloat>
+#include <cstdio>
 #include <vector>
 
 #include "engine.h"
@@ -54,9 +55,9 @@ struct LevelDev
 
 struct Common
 {
-    int W, H, D, Wp;
+    int W, H, D, Dp;
     float lambda, tau, tau_smooth;
-    const uint8_t *vol; // [D][H][Wp]
+    const uint8_t *vol; // [H][W][Dp]
     const float *wta;   // HW
 };
 
@@ -73,9 +74,9 @@ __device__ __forceinline__ float pixel_cost(const Common &c, int x, int y, float
         cost = c.tau;
     else
     {
-        const size_t plane = (size_t)c.H * c.Wp, o = (size_t)y * c.Wp + x;
-        float v0 = (float)c.vol[(size_t)d * plane + o];
-        float v1 = (float)c.vol[(size_t)(d + 1) * plane + o];
+        const uint8_t *pv = c.vol + ((size_t)y * c.W + x) * c.Dp + d;
+        float v0 = (float)pv[0];
+        float v1 = (float)pv[1];
         cost = ((float)(d + 1) - d_f) * v0 + (d_f - (float)d) * v1;
     }
     return c.lambda * cost;
@@ -197,18 +198,176 @@ __device__ __forceinline__ float4 fit_plane(float Ax, float Ay, float Az, float 
     return make_float4(-nx, -ny, nx * Ax + ny * Ay + Az, 0.f);
 }
 
-// ransac_candidate_plane (hbp_isp.cu:592-640) with make_three_diff_id (:504-529).
-__global__ void ransac_kernel(LevelDev lv, Common c, uint32_t *s_ransac)
+
+
+// ---------------------------------------------------------------------------
+// Batched BP. A batch holds up to MAXV views (one view = one pyramid + cost
+// volume; a pair contributes one, or two with the right view). Every kernel
+// below serves one BP phase of every participating view at once: items
+// (nodes, chunks, edges) of the views are laid end to end and each thread or
+// warp finds its view from the prefix table of the launch's step descriptor.
+//
+// A BP step of the reference (generate_plane, compute_plane_cost,
+// belief_propagation; hbp_isp.cu:1206-1311) runs as
+//   node phase   select of the previous step (aggregate_belief_k,
+//                get_belief_order, select_belief) fused with the step's RANSAC
+//                or random-adjust candidates, one thread per node;
+//   [spatial]    select_child, neighbor, set_candidate (one thread per parent
+//                or node);
+//   data cost    read_plane_cost + the per-node reduction, one group of 4..32
+//                lanes per chunk;
+//   edge phase   passing_msg + smooth_msg + normalize_msg, one thread per
+//                edge, with the previous step's messages pulled through
+//                ping_pang_msg + select_msg (msg[e] = msg_t[rev e] compacted by
+//                the kept slots of e's target).
+struct ViewBufs
 {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= lv.N)
+    float *msgt[2]; // [E][K] ping-pong
+    float4 *pc[2];  // chunk partial costs ping-pong
+    uint32_t *s_child, *s_nb, *s_ransac[2];
+    float4 *buf; // [Nmax][P] spatial candidates
+};
+
+struct ViewDev
+{
+    Common c;
+    const LevelDev *lv; // [L]
+    ViewBufs b;
+    float *disp, *plane_out;
+    int L;
+};
+
+constexpr int MAXV = 32;
+
+struct Task
+{
+    const ViewDev *vd;             // the view's record in device memory
+    const LevelDev *lvl, *lvh;     // its level li and li+1 records
+    int v, li;
+    int first;        // first BP step of the level: no select, zero messages
+    int rb, pb, mb;   // seed buffer read / cost partials written / messages written
+    float max_dz, max_dn;
+};
+
+enum NodeMode
+{
+    NODE_SELECT = 0,
+    NODE_SELECT_RANSAC = 1,
+    NODE_SELECT_RANDOM = 2
+};
+
+struct StepDesc
+{
+    int nt, gs, mode;
+    int pre[MAXV + 1];
+    Task t[MAXV];
+};
+
+__device__ __forceinline__ int find_task(const StepDesc &d, int item)
+{
+    int k = 0;
+    while (k + 1 < d.nt && item >= d.pre[k + 1])
+        ++k;
+    return k;
+}
+
+// Select of node n (aggregate_belief_k, get_belief_order, select_belief;
+// hbp_isp.cu:405-417, :432-472): belief = cost + out-edge messages in edge
+// order; a slot's rank counts the slots that beat it (a later slot loses
+// ties); slots ranked < P move to the front in slot order, in place.
+__device__ __forceinline__ void select_thread(const LevelDev &l, int n, const float4 *pc, const float *msgt)
+{
+    float cs[K], b[K];
+    float *cst = l.cost + (size_t)n * K;
+#pragma unroll
+    for (int k = 0; k < 2 * P; ++k)
+        cs[k] = cst[k];
+    {
+        int c0 = l.chunk_off[n], c1 = l.chunk_off[n + 1];
+        float4 a = pc[c0];
+        for (int ch = c0 + 1; ch < c1; ++ch)
+        {
+            float4 q = pc[ch];
+            a.x = a.x + q.x;
+            a.y = a.y + q.y;
+            a.z = a.z + q.z;
+            a.w = a.w + q.w;
+        }
+        cs[8] = a.x;
+        cs[9] = a.y;
+        cs[10] = a.z;
+        cs[11] = a.w;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        b[k] = cs[k];
+    for (int e = l.nb_off[n]; e < l.nb_off[n + 1]; ++e)
+    {
+        const float4 *m4 = reinterpret_cast<const float4 *>(msgt + (size_t)e * K);
+        float4 m0 = m4[0], m1 = m4[1], m2 = m4[2];
+        b[0] = b[0] + m0.x;
+        b[1] = b[1] + m0.y;
+        b[2] = b[2] + m0.z;
+        b[3] = b[3] + m0.w;
+        b[4] = b[4] + m1.x;
+        b[5] = b[5] + m1.y;
+        b[6] = b[6] + m1.z;
+        b[7] = b[7] + m1.w;
+        b[8] = b[8] + m2.x;
+        b[9] = b[9] + m2.y;
+        b[10] = b[10] + m2.z;
+        b[11] = b[11] + m2.w;
+    }
+    int ord[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        ord[k] = 0;
+#pragma unroll
+    for (int i = 0; i < K - 1; ++i)
+#pragma unroll
+        for (int j = i + 1; j < K; ++j)
+        {
+            if (b[j] < b[i])
+                ord[i]++;
+            else
+                ord[j]++;
+        }
+    float *bl = l.belief + (size_t)n * K;
+    float4 *pl = l.plane + (size_t)n * K;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        bl[k] = b[k];
+        cst[k] = cs[k];
+    }
+    int nb = 0;
+    unsigned long long kl = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (ord[k] < P)
+        {
+            if (nb != k)
+            {
+                pl[nb] = pl[k];
+                bl[nb] = b[k];
+                cst[nb] = cs[k];
+            }
+            kl |= (unsigned long long)k << (4 + 4 * nb);
+            nb++;
+        }
+    l.keep[n] = kl | (unsigned long long)nb;
+}
+
+__device__ __forceinline__ void ransac_thread(const LevelDev &l, const Common &c, int n, uint32_t s,
+                                              uint32_t *s_out)
+{
+    // ransac_candidate_plane + make_three_diff_id + fit_plane_from_points
+    // (hbp_isp.cu:504-548, :592-640)
+    const int cn = l.pix_off[n + 1] - l.pix_off[n], cp = l.pix_off[n];
+    if (cn <= 0)
         return;
-    const int cn = lv.pix_off[n + 1] - lv.pix_off[n], cp = lv.pix_off[n];
-    if (cn <= 0) // every node owns a pixel; guard the modulo all the same
-        return;
-    uint32_t s = s_ransac[n];
     uint32_t xy[3] = {0, 0, 0};
-    for (int p = 2 * P; p < 3 * P; ++p)
+    for (int p = 0; p < P; ++p)
     {
         s = lcg(s);
         int p0 = (int)(s % (uint32_t)cn);
@@ -230,9 +389,9 @@ __global__ void ransac_kernel(LevelDev lv, Common c, uint32_t *s_ransac)
             else if (p2 == p1)
                 p2 = (p0 == cn - 2) ? cn - 1 : cn - 2;
         }
-        xy[0] = lv.pix[cp + p0];
-        xy[1] = lv.pix[cp + p1];
-        xy[2] = lv.pix[cp + p2];
+        xy[0] = l.pix[cp + p0];
+        xy[1] = l.pix[cp + p1];
+        xy[2] = l.pix[cp + p2];
         float X[3], Y[3], Z[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
@@ -242,23 +401,20 @@ __global__ void ransac_kernel(LevelDev lv, Common c, uint32_t *s_ransac)
             Y[k] = (float)y;
             Z[k] = c.wta[(size_t)y * c.W + x];
         }
-        lv.plane[(size_t)n * K + p] = fit_plane(X[0], Y[0], Z[0], X[1], Y[1], Z[1], X[2], Y[2], Z[2]);
+        l.plane[(size_t)n * K + 2 * P + p] = fit_plane(X[0], Y[0], Z[0], X[1], Y[1], Z[1], X[2], Y[2], Z[2]);
     }
-    lv.pid[n] = make_int4((int)xy[0], (int)xy[1], (int)xy[2], 0);
-    s_ransac[n] = s;
+    l.pid[n] = make_int4((int)xy[0], (int)xy[1], (int)xy[2], 0);
+    *s_out = s;
 }
 
-// random_candidate_plane + normalize_plane (hbp_isp.cu:495-503, :641-674).
-__global__ void random_kernel(LevelDev lv, uint32_t *s_ransac, float max_dz, float max_dn)
+__device__ __forceinline__ void random_thread(const LevelDev &l, int n, uint32_t s, uint32_t *s_out,
+                                              float max_dz, float max_dn)
 {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= lv.N)
-        return;
-    uint32_t s = s_ransac[n];
-    const float x = lv.mx[n], y = lv.my[n];
+    // random_candidate_plane + normalize_plane (hbp_isp.cu:495-503, :641-674)
+    const float x = l.mx[n], y = l.my[n];
     for (int p = 2 * P; p < 3 * P; ++p)
     {
-        float4 pl = lv.plane[(size_t)n * K + p];
+        float4 pl = l.plane[(size_t)n * K + p];
         float z = pl.x * x + pl.y * y + pl.z;
         s = lcg(s);
         float dz = (float)s / 2147483648.0f * max_dz;
@@ -278,356 +434,411 @@ __global__ void random_kernel(LevelDev lv, uint32_t *s_ransac, float max_dz, flo
         pl.z += dnz;
         float a = -pl.x / pl.z, b = -pl.y / pl.z;
         float cc = z - a * x - b * y;
-        lv.plane[(size_t)n * K + p] = make_float4(a, b, cc, 0.f);
+        l.plane[(size_t)n * K + p] = make_float4(a, b, cc, 0.f);
     }
-    s_ransac[n] = s;
+    *s_out = s;
 }
 
-// select_child_plane (hbp_isp.cu:705-726): parent takes random children's
-// slot-0 planes as its candidates.
-__global__ void select_child_kernel(LevelDev lv, LevelDev h, uint32_t *s_child)
+__global__ void __launch_bounds__(128) k_node(const ViewDev *__restrict__ V, StepDesc d)
 {
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= h.N)
+    int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= d.pre[d.nt])
         return;
-    int cn = lv.child_off[id + 1] - lv.child_off[id], cp = lv.child_off[id];
-    if (cn <= 0) // every parent has a child; guard the modulo all the same
+    const Task &t = d.t[find_task(d, item)];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    const int n = item - d.pre[find_task(d, item)];
+    if (!t.first)
+        select_thread(l, n, v.b.pc[t.pb ^ 1], v.b.msgt[t.mb ^ 1]);
+    if (d.mode == NODE_SELECT_RANSAC)
+        ransac_thread(l, v.c, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n]);
+    else if (d.mode == NODE_SELECT_RANDOM)
+        random_thread(l, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n], t.max_dz, t.max_dn);
+}
+
+// select_child_plane (hbp_isp.cu:705-726), one thread per parent
+__global__ void __launch_bounds__(128) k_child(const ViewDev *__restrict__ V, StepDesc d)
+{
+    int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= d.pre[d.nt])
         return;
-    uint32_t s = s_child[id];
+    int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl, &h = *t.lvh;
+    int id = item - d.pre[ti];
+    int cn = l.child_off[id + 1] - l.child_off[id], cp = l.child_off[id];
+    if (cn <= 0)
+        return;
+    uint32_t s = v.b.s_child[id];
     for (int p = 0; p < P; ++p)
     {
         s = lcg(s);
-        int ch = (int)lv.child[cp + (int)(s % (uint32_t)cn)];
-        h.plane[(size_t)id * K + 2 * P + p] = lv.plane[(size_t)ch * K];
+        int ch = (int)l.child[cp + (int)(s % (uint32_t)cn)];
+        h.plane[(size_t)id * K + 2 * P + p] = l.plane[(size_t)ch * K];
     }
-    s_child[id] = s;
+    v.b.s_child[id] = s;
 }
 
-// neighbor_candidate_plane (hbp_isp.cu:676-703), on the parent level, seeded
-// with the state kept per parent index.
-__global__ void neighbor_kernel(LevelDev h, uint32_t *s_nb, float4 *buf)
+// neighbor_candidate_plane (hbp_isp.cu:676-703) on the parent level, seeded
+// with the state kept per parent index
+__global__ void __launch_bounds__(128) k_neighbor(const ViewDev *__restrict__ V, StepDesc d)
 {
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= h.N)
+    int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= d.pre[d.nt])
         return;
+    int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &h = *t.lvh;
+    int id = item - d.pre[ti];
     int nbn = h.nb_off[id + 1] - h.nb_off[id], nbp = h.nb_off[id];
-    if (nbn <= 0) // a level with two or more nodes is connected; guard anyway
+    if (nbn <= 0)
     {
         for (int p = 0; p < P; ++p)
-            buf[(size_t)id * P + p] = h.plane[(size_t)id * K + 2 * P + p];
+            v.b.buf[(size_t)id * P + p] = h.plane[(size_t)id * K + 2 * P + p];
         return;
     }
-    uint32_t s = s_nb[id];
+    uint32_t s = v.b.s_nb[id];
     for (int p = 0; p < P; ++p)
     {
         s = lcg(s);
-        int t = h.bd[nbp + (int)(s % (uint32_t)nbn)].y;
-        buf[(size_t)id * P + p] = h.plane[(size_t)t * K + 2 * P + p];
+        int tt = h.bd[nbp + (int)(s % (uint32_t)nbn)].y;
+        v.b.buf[(size_t)id * P + p] = h.plane[(size_t)tt * K + 2 * P + p];
     }
-    s_nb[id] = s;
+    v.b.s_nb[id] = s;
 }
 
-__global__ void buf_to_candidates(LevelDev h, const float4 *buf)
+// set_candidate_plane_k (hbp_isp.cu:727-741): children take the parent's
+// spatial candidates
+__global__ void __launch_bounds__(128) k_set_cand(const ViewDev *__restrict__ V, StepDesc d)
 {
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= h.N)
+    int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= d.pre[d.nt])
         return;
+    int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    int n = item - d.pre[ti];
+    int pn = l.clus[n];
     for (int p = 0; p < P; ++p)
-        h.plane[(size_t)id * K + 2 * P + p] = buf[(size_t)id * P + p];
+        l.plane[(size_t)n * K + 2 * P + p] = v.b.buf[(size_t)pn * P + p];
 }
 
-// set_candidate_plane_k (hbp_isp.cu:727-741)
-__global__ void set_candidate_kernel(LevelDev lv, LevelDev h)
+// Data cost of 4 planes over one chunk with a group of GS lanes. The value is
+// the engine's 32-slot reduction: slot j accumulates the chunk's pixels j,
+// j+32, ... sequentially; the 32 slots are combined by an xor butterfly with
+// offsets 16..1. Lane r of the group holds slots r + GS*u; butterfly levels
+// with offset >= GS pair slots inside the lane, the others pair lanes by
+// shuffles, so every group size gives the same sums.
+template <int GS>
+__device__ __forceinline__ float4 group_cost(const LevelDev &l, const Common &c, int n, int ch, const float4 pl[4],
+                                             int r, bool valid)
 {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= lv.N)
-        return;
-    int pc = lv.clus[n];
-    for (int p = 2 * P; p < 3 * P; ++p)
-        lv.plane[(size_t)n * K + p] = h.plane[(size_t)pc * K + p];
-}
-
-// ---------------------------------------------------------------------------
-// data cost: one warp per chunk of 256 pixels of one node, 4 planes at once.
-__global__ void __launch_bounds__(256) plane_cost_kernel(LevelDev lv, Common c, int sb, float4 *pc)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= lv.nchunks)
-        return;
-    const int n = lv.chunk_node[warp];
-    const int start = lv.pix_off[n] + (warp - lv.chunk_off[n]) * PC_CHUNK;
-    const int end = min(start + PC_CHUNK, lv.pix_off[n + 1]);
-    float4 pl[4];
+    constexpr int SL = 32 / GS;
+    float acc[SL][4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-        pl[k] = lv.plane[(size_t)n * K + sb + k];
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int s = 0; s < PC_CHUNK / 32; ++s)
-    {
-        int idx = start + lane + 32 * s;
-        if (idx < end)
-        {
-            uint32_t xy = lv.pix[idx];
-            int x = px_x(xy), y = px_y(xy);
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                acc[k] = acc[k] + pixel_cost(c, x, y, pl[k]);
-        }
-    }
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1)
+    for (int u = 0; u < SL; ++u)
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            acc[k] = acc[k] + __shfl_xor_sync(0xffffffffu, acc[k], off);
-    if (lane == 0)
-        pc[warp] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-}
-
-__device__ __forceinline__ float4 node_cost(const LevelDev &lv, const float4 *pc, int n)
-{
-    int c0 = lv.chunk_off[n], c1 = lv.chunk_off[n + 1];
-    float4 a = pc[c0];
-    for (int c = c0 + 1; c < c1; ++c)
-    {
-        float4 b = pc[c];
-        a.x = a.x + b.x;
-        a.y = a.y + b.y;
-        a.z = a.z + b.z;
-        a.w = a.w + b.w;
-    }
-    return a;
-}
-
-__global__ void finalize_cost_kernel(LevelDev lv, const float4 *pc, int sb)
-{
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= lv.N)
-        return;
-    float4 a = node_cost(lv, pc, n);
-    float *cst = lv.cost + (size_t)n * K + sb;
-    cst[0] = a.x;
-    cst[1] = a.y;
-    cst[2] = a.z;
-    cst[3] = a.w;
-}
-
-// ---------------------------------------------------------------------------
-// BP step, part 1 (passing_msg_k + smooth_msg_k + normalize_msg_k,
-// hbp_isp.cu:273-355): block = 32 edges x 12 slots of the source.
-constexpr int BE = 32;
-__global__ void __launch_bounds__(BE *K) bp_edge_kernel(LevelDev lv, Common c, const float *msg, float *msg_t)
-{
-    __shared__ float out[K][BE + 1];
-    __shared__ float mean[BE];
-    const int tx = threadIdx.x, y = threadIdx.y;
-    const int e = blockIdx.x * BE + tx;
-    const bool valid = e < lv.E;
+            acc[u][k] = 0.f;
     if (valid)
     {
-        int2 st = lv.bd[e];
-        int4 ps4 = lv.pid[st.x], pt4 = lv.pid[st.y];
-        uint32_t pts[6] = {(uint32_t)ps4.x, (uint32_t)ps4.y, (uint32_t)ps4.z,
-                           (uint32_t)pt4.x, (uint32_t)pt4.y, (uint32_t)pt4.z};
-        float X[6], Y[6];
+        const int start = l.pix_off[n] + (ch - l.chunk_off[n]) * PC_CHUNK;
+        const int end = min(start + PC_CHUNK, l.pix_off[n + 1]);
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
+        for (int u = 0; u < SL; ++u)
         {
-            X[i] = (float)px_x(pts[i]);
-            Y[i] = (float)px_y(pts[i]);
+            const int j = r + GS * u;
+#pragma unroll
+            for (int dd = 0; dd < PC_CHUNK / 32; ++dd)
+            {
+                int idx = start + j + 32 * dd;
+                if (idx < end)
+                {
+                    uint32_t xy = l.pix[idx];
+                    int x = px_x(xy), y = px_y(xy);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        acc[u][k] = acc[u][k] + pixel_cost(c, x, y, pl[k]);
+                }
+            }
         }
-        float dist_color = fmaxf(lv.dc[e], 0.01f);
-        float dist_pos = fmaxf(lv.dc[lv.E + e], 1.0f);
-        float c0 = dist_color * (float)lv.bdl[e];
-        float4 ps = lv.plane[(size_t)st.x * K + y];
-        const float4 *pt_base = lv.plane + (size_t)st.y * K;
-        const float *bt = lv.belief + (size_t)st.y * K;
-        const float *me = msg + (size_t)e * K;
-        float acc = 0.f, mn = FLT_MAX;
+    }
+#pragma unroll
+    for (int off = 16; off >= GS; off >>= 1)
+    {
+        const int ku = off / GS;
+        float nw[SL][4];
+#pragma unroll
+        for (int u = 0; u < SL; ++u)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                nw[u][k] = acc[u][k] + acc[u ^ ku][k];
+#pragma unroll
+        for (int u = 0; u < SL; ++u)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                acc[u][k] = nw[u][k];
+    }
+    float v[4] = {acc[0][0], acc[0][1], acc[0][2], acc[0][3]};
+#pragma unroll
+    for (int off = GS / 2; off >= 1; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] = v[k] + __shfl_xor_sync(0xffffffffu, v[k], off);
+    return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// COST_INIT: priors of the parent's best slots (init_bp + copy_prior_plane,
+// hbp_isp.cu:56-73, :930-950); COST_STEP: candidates in slots 8-11.
+enum CostMode
+{
+    COST_INIT = 0,
+    COST_STEP = 1
+};
+
+template <int GS>
+__global__ void __launch_bounds__(256) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
+{
+    const int lane = threadIdx.x & 31;
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) / GS;
+    const int r = lane % GS;
+    const bool valid = item < d.pre[d.nt];
+    int ti = valid ? find_task(d, item) : 0;
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    int ch = valid ? item - d.pre[ti] : 0;
+    int n = valid ? l.chunk_node[ch] : 0;
+    float4 pl[4];
+    if (valid)
+    {
+        if (mode == COST_INIT)
+        {
+            const LevelDev &h = *t.lvh;
+            int pn = l.clus[n];
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                pl[p] = h.plane[(size_t)pn * K + p];
+        }
+        else
+        {
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                pl[p] = l.plane[(size_t)n * K + 2 * P + p];
+        }
+    }
+    float4 cc = group_cost<GS>(l, v.c, n, ch, pl, r, valid);
+    if (valid && r == 0)
+    {
+        v.b.pc[t.pb][ch] = cc;
+        if (mode == COST_INIT && ch == l.chunk_off[n])
+        {
+            for (int k = 0; k < K; ++k)
+                l.plane[(size_t)n * K + k] = pl[k % P];
+            v.b.s_nb[n] = (uint32_t)l.nb_off[n];
+            v.b.s_ransac[t.rb][n] = (uint32_t)l.pix_off[n];
+        }
+    }
+}
+
+// init_bp, continued: costs of the prior slots, belief = cost, child seeds.
+__global__ void __launch_bounds__(128) k_init_nodes(const ViewDev *__restrict__ V, StepDesc d)
+{
+    int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= d.pre[d.nt])
+        return;
+    int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    int n = item - d.pre[ti];
+    if (n < l.N)
+    {
+        int c0 = l.chunk_off[n], c1 = l.chunk_off[n + 1];
+        const float4 *pc = v.b.pc[t.pb];
+        float4 a = pc[c0];
+        for (int ch = c0 + 1; ch < c1; ++ch)
+        {
+            float4 q = pc[ch];
+            a.x = a.x + q.x;
+            a.y = a.y + q.y;
+            a.z = a.z + q.z;
+            a.w = a.w + q.w;
+        }
+        float *cs = l.cost + (size_t)n * K;
+        float *bl = l.belief + (size_t)n * K;
+        cs[0] = cs[4] = a.x;
+        cs[1] = cs[5] = a.y;
+        cs[2] = cs[6] = a.z;
+        cs[3] = cs[7] = a.w;
+        for (int k = 0; k < K; ++k)
+            bl[k] = cs[k];
+    }
+    if (n < l.Nh)
+        v.b.s_child[n] = (uint32_t)l.child_off[n];
+}
+
+// passing_msg_k + smooth_msg_k + normalize_msg_k (hbp_isp.cu:273-355), one
+// thread per edge
+__global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, StepDesc d)
+{
+    int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= d.pre[d.nt])
+        return;
+    int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    const Common &c = v.c;
+    const int e = item - d.pre[ti];
+    int2 st = l.bd[e];
+    int4 ps4 = l.pid[st.x], pt4 = l.pid[st.y];
+    uint32_t pts[6] = {(uint32_t)ps4.x, (uint32_t)ps4.y, (uint32_t)ps4.z,
+                       (uint32_t)pt4.x, (uint32_t)pt4.y, (uint32_t)pt4.z};
+    float X[6], Y[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+    {
+        X[i] = (float)px_x(pts[i]);
+        Y[i] = (float)px_y(pts[i]);
+    }
+    float dist_color = fmaxf(l.dc[e], 0.01f);
+    float dist_pos = fmaxf(l.dc[l.E + e], 1.0f);
+    float c0 = dist_color * (float)l.bdl[e];
+    const float *bt = l.belief + (size_t)st.y * K;
+    float mp[2 * P];
+    if (t.first)
+    {
+#pragma unroll
+        for (int p = 0; p < 2 * P; ++p)
+            mp[p] = bt[p] - 0.0f;
+    }
+    else
+    {
+        unsigned long long kl = l.keep[st.y];
+        int cnt = (int)(kl & 15ull);
+        const float *src = v.b.msgt[t.mb ^ 1] + (size_t)l.rev[e] * K;
+        float vv[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            vv[k] = src[k];
 #pragma unroll
         for (int p = 0; p < 2 * P; ++p)
         {
-            if (p == P)
+            int sidx = p < cnt ? (int)((kl >> (4 + 4 * p)) & 15ull) : p;
+            float m = vv[0];
+#pragma unroll
+            for (int k = 1; k < K; ++k)
+                if (k == sidx)
+                    m = vv[k];
+            mp[p] = bt[p] - m;
+        }
+    }
+    float4 pt[2 * P];
+#pragma unroll
+    for (int p = 0; p < 2 * P; ++p)
+        pt[p] = l.plane[(size_t)st.y * K + p];
+    // Each group's minimum over t's labels p of mp[p] + c0 * phi: c0 * phi is
+    // >= 0 and float addition is monotone, so a label whose mp[p] is not
+    // below the running minimum cannot lower it. Labels are visited in
+    // increasing mp (NaN last) and the scan stops at the first such label;
+    // the minimum, hence the message, is the reference's.
+    int ordr[2 * P];
+    float key[2 * P];
+#pragma unroll
+    for (int p = 0; p < 2 * P; ++p)
+    {
+        ordr[p] = p;
+        key[p] = mp[p] == mp[p] ? mp[p] : INFINITY;
+    }
+#pragma unroll
+    for (int g = 0; g < 2; ++g)
+    {
+        const int b = g * P;
+        auto cswap = [&](int i, int j) {
+            if (key[b + j] < key[b + i])
             {
-                acc = acc + mn;
-                mn = FLT_MAX;
+                float tk = key[b + i];
+                key[b + i] = key[b + j];
+                key[b + j] = tk;
+                int to = ordr[b + i];
+                ordr[b + i] = ordr[b + j];
+                ordr[b + j] = to;
             }
-            float4 pt = pt_base[p];
-            float dx = ps.x - pt.x, dy = ps.y - pt.y, dz = ps.z - pt.z;
-            float phi = fabsf(dx * X[0] + dy * Y[0] + dz);
-#pragma unroll
-            for (int i = 1; i < 6; ++i)
-                phi = phi + fabsf(dx * X[i] + dy * Y[i] + dz);
-            phi = fminf(phi / 3.0f / dist_pos, c.tau_smooth);
-            float m = (bt[p] - me[p]) + c0 * phi;
-            if (m < mn)
-                mn = m;
-        }
-        acc = acc + mn;
-        out[y][tx] = acc;
+        };
+        cswap(0, 1);
+        cswap(2, 3);
+        cswap(0, 2);
+        cswap(1, 3);
+        cswap(1, 2);
     }
-    __syncthreads();
-    if (valid && y == 0)
+    float out[K];
+    float sum = 0.f;
+#pragma unroll
+    for (int y = 0; y < K; ++y)
     {
-        float s = 0.f;
+        float4 ps = l.plane[(size_t)st.x * K + y];
+        float acc = 0.f;
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            s = s + out[k][tx];
-        mean[tx] = s / (float)K;
-    }
-    __syncthreads();
-    if (valid)
-        msg_t[(size_t)e * K + y] = out[y][tx] - mean[tx];
-}
-
-// BP step, part 2 (aggregate_belief_k, get_belief_order, select_belief,
-// hbp_isp.cu:405-417, :432-472): per node, beliefs = cost + out-edge
-// messages (edge order), rank the 12 slots by pairwise counting (a later slot
-// loses ties), keep the slots ranked < P in slot order.
-__global__ void bp_node_kernel(LevelDev lv, const float4 *pc, const float *msg_t)
-{
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= lv.N)
-        return;
-    float4 cn = node_cost(lv, pc, n);
-    float *cst = lv.cost + (size_t)n * K;
-    cst[8] = cn.x;
-    cst[9] = cn.y;
-    cst[10] = cn.z;
-    cst[11] = cn.w;
-    float b[K], cs[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-        cs[k] = cst[k];
-        b[k] = cs[k];
-    }
-    for (int e = lv.nb_off[n]; e < lv.nb_off[n + 1]; ++e)
-    {
-        const float *m = msg_t + (size_t)e * K;
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            b[k] = b[k] + m[k];
-    }
-    int ord[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        ord[k] = 0;
-#pragma unroll
-    for (int i = 0; i < K - 1; ++i)
-#pragma unroll
-        for (int j = i + 1; j < K; ++j)
+        for (int g = 0; g < 2; ++g)
         {
-            if (b[j] < b[i])
-                ord[i]++;
-            else
-                ord[j]++;
-        }
-    float4 *pl = lv.plane + (size_t)n * K;
-    float *bl = lv.belief + (size_t)n * K;
-    float4 pls[K];
+            float mn = FLT_MAX;
 #pragma unroll
-    for (int k = 0; k < K; ++k)
-        pls[k] = pl[k];
-    int nb = 0;
-    unsigned long long keep = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        if (ord[k] < P)
-        {
-            keep |= (unsigned long long)k << (4 + 4 * nb);
-            nb++;
-        }
-    keep |= (unsigned long long)nb;
-    // final slot j: j < nb ? kept[j] : j (in-place compaction of the reference)
-#pragma unroll
-    for (int j = 0; j < K; ++j)
-    {
-        int src = j < nb ? (int)((keep >> (4 + 4 * j)) & 15ull) : j;
-        float4 p4 = pls[0];
-        float bb = b[0], cc = cs[0];
-#pragma unroll
-        for (int k = 1; k < K; ++k)
-            if (k == src)
+            for (int k = 0; k < P; ++k)
             {
-                p4 = pls[k];
-                bb = b[k];
-                cc = cs[k];
+                const int q = g * P + k;
+                if (k > 0 && key[q] >= mn)
+                    break;
+                const int p = ordr[q];
+                float4 tp = pt[0];
+#pragma unroll
+                for (int j = 1; j < 2 * P; ++j)
+                    if (j == p)
+                        tp = pt[j];
+                float mpp = mp[0];
+#pragma unroll
+                for (int j = 1; j < 2 * P; ++j)
+                    if (j == p)
+                        mpp = mp[j];
+                float dx = ps.x - tp.x, dy = ps.y - tp.y, dz = ps.z - tp.z;
+                float phi = fabsf(dx * X[0] + dy * Y[0] + dz);
+#pragma unroll
+                for (int i = 1; i < 6; ++i)
+                    phi = phi + fabsf(dx * X[i] + dy * Y[i] + dz);
+                phi = fminf(phi / 3.0f / dist_pos, c.tau_smooth);
+                float m = mpp + c0 * phi;
+                if (m < mn)
+                    mn = m;
             }
-        pl[j] = p4;
-        bl[j] = bb;
-        cst[j] = cc;
-    }
-    lv.keep[n] = keep;
-}
-
-// BP step, part 3 (ping_pang_msg_k + select_msg, hbp_isp.cu:419-429,
-// :474-493): msg[rev(e)] receives msg_t[e] compacted by the kept slots of
-// e's source (the target of rev(e)).
-__global__ void bp_edge2_kernel(LevelDev lv, const float *msg_t, float *msg)
-{
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= lv.E)
-        return;
-    unsigned long long keep = lv.keep[lv.bd[e].x];
-    int nb = (int)(keep & 15ull);
-    const float *src = msg_t + (size_t)e * K;
-    float v[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        v[k] = src[k];
-    float *dst = msg + (size_t)lv.rev[e] * K;
-#pragma unroll
-    for (int j = 0; j < K; ++j)
-    {
-        int s = j < nb ? (int)((keep >> (4 + 4 * j)) & 15ull) : j;
-        float o = v[0];
-#pragma unroll
-        for (int k = 1; k < K; ++k)
-            if (k == s)
-                o = v[k];
-        dst[j] = o;
-    }
-}
-
-// init_bp (hbp_isp.cu:930-950): priors from the parent's best slots, seeds
-// from the CSR offsets.
-__global__ void init_level_kernel(LevelDev lv, LevelDev h, uint32_t *s_nb, uint32_t *s_ransac,
-                                  uint32_t *s_child)
-{
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < lv.N)
-    {
-        int pc = lv.clus[n];
-        for (int p = 0; p < P; ++p)
-        {
-            float4 pr = h.plane[(size_t)pc * K + p];
-            lv.plane[(size_t)n * K + p] = pr;
-            lv.plane[(size_t)n * K + P + p] = pr;
-            lv.plane[(size_t)n * K + 2 * P + p] = pr;
+            acc = acc + mn;
         }
-        s_nb[n] = (uint32_t)lv.nb_off[n];
-        s_ransac[n] = (uint32_t)lv.pix_off[n];
+        out[y] = acc;
+        sum = sum + acc;
     }
-    if (n < lv.Nh)
-        s_child[n] = (uint32_t)lv.child_off[n];
+    float mean = sum / (float)K;
+    float4 *o = reinterpret_cast<float4 *>(v.b.msgt[t.mb] + (size_t)e * K);
+    o[0] = make_float4(out[0] - mean, out[1] - mean, out[2] - mean, out[3] - mean);
+    o[1] = make_float4(out[4] - mean, out[5] - mean, out[6] - mean, out[7] - mean);
+    o[2] = make_float4(out[8] - mean, out[9] - mean, out[10] - mean, out[11] - mean);
 }
 
-__global__ void copy_cost_to_belief(LevelDev lv)
+// map_msg (hbp_isp.cu:783-841), one warp per node of the finest level
+__global__ void __launch_bounds__(128) k_map(const ViewDev *__restrict__ V, StepDesc d)
 {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < (long)lv.N * K)
-        lv.belief[i] = lv.cost[i];
-}
-
-// map_msg (hbp_isp.cu:783-841): first slot among 0..3 with the minimum
-// belief; per pixel d = clamp(a*x + b*y + c, 0, D-1) and the plane (a, b, c).
-__global__ void map_kernel(LevelDev lv, Common c, float *disp, float *plane_out)
-{
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= lv.N)
+    const int lane = threadIdx.x & 31;
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (item >= d.pre[d.nt])
         return;
-    const float *bl = lv.belief + (size_t)n * K;
+    int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    const Common &c = v.c;
+    int n = item - d.pre[ti];
+    const float *bl = l.belief + (size_t)n * K;
     float mn = bl[0];
     for (int p = 1; p < P; ++p)
         mn = fminf(mn, bl[p]);
@@ -638,20 +849,20 @@ __global__ void map_kernel(LevelDev lv, Common c, float *disp, float *plane_out)
             mp = p;
             break;
         }
-    float4 pl = lv.plane[(size_t)n * K + mp];
-    for (int j = lv.pix_off[n]; j < lv.pix_off[n + 1]; ++j)
+    float4 pl = l.plane[(size_t)n * K + mp];
+    for (int j = l.pix_off[n] + lane; j < l.pix_off[n + 1]; j += 32)
     {
-        uint32_t xy = lv.pix[j];
+        uint32_t xy = l.pix[j];
         int x = px_x(xy), y = px_y(xy);
-        float d = pl.x * (float)x + pl.y * (float)y + pl.z;
-        d = fminf(fmaxf(d, 0.f), (float)(c.D - 1));
+        float dd = pl.x * (float)x + pl.y * (float)y + pl.z;
+        dd = fminf(fmaxf(dd, 0.f), (float)(c.D - 1));
         size_t id = (size_t)y * c.W + x;
-        disp[id] = d;
-        if (plane_out)
+        v.disp[id] = dd;
+        if (v.plane_out)
         {
-            plane_out[3 * id] = pl.x;
-            plane_out[3 * id + 1] = pl.y;
-            plane_out[3 * id + 2] = pl.z;
+            v.plane_out[3 * id] = pl.x;
+            v.plane_out[3 * id + 1] = pl.y;
+            v.plane_out[3 * id + 2] = pl.z;
         }
     }
 }
@@ -667,8 +878,24 @@ int read_dev_int(const int *p, cudaStream_t st)
 }
 } // namespace
 
-void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta, int D,
-               const HbpParams &prm, float *disp, float *plane_out, Arena &a, cudaStream_t st)
+// ---------------------------------------------------------------------------
+// host side
+struct ViewPlan::Impl
+{
+    ViewDev vd;
+    std::vector<LevelDev> lv;
+};
+
+ViewPlan::ViewPlan() : impl(new Impl) {}
+ViewPlan::~ViewPlan() { delete impl; }
+
+// Per-level setup of one view (HBP_ISP constructor and the first loop of
+// run_ms: setup_D4, reverse_bd_id, compute_dist_color_pos, sort_clus;
+// hbp_isp.cu:871-891, :952-1019), the BP buffers, and the view descriptor.
+// Persistent data go to `persist`, sort/scan temporaries to `tmp`.
+void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wta, int D,
+                 const HbpParams &prm, float *disp, float *plane_out, Arena &persist, Arena &tmp,
+                 cudaStream_t st, ViewPlan &vp)
 {
     const int L = pyr.L, W = pyr.W, H = pyr.H, HW = W * H;
     const int m = prm.min_level;
@@ -677,22 +904,28 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
     if ((int)pyr.N.size() != L || (int)pyr.E.size() != L || (int)pyr.node_off.size() != L ||
         (int)pyr.edge_off.size() != L || (int)pyr.child_base.size() != L || (int)pyr.nb_base.size() != L)
         throw StatusError{HBP_ERR_INTERNAL, "pyramid bookkeeping inconsistent"};
-    Common c{W, H, D, Wp, prm.alpha, CENSUS_TAU, prm.tau_smooth, vol, wta};
-
-    size_t mark = a.mark();
-    std::vector<LevelDev> lv(L);
-    int Nmax = 0, Emax = 0, CHmax = 0;
-    // pixel -> node per level, composed from level 0
-    int *im = a.alloc<int>(HW), *im2 = a.alloc<int>(HW);
-    uint32_t *kt = a.alloc<uint32_t>(HW), *ka = a.alloc<uint32_t>(HW), *va = a.alloc<uint32_t>(HW);
-    int *cnt = a.alloc<int>(HW + 1);
+    Common c{W, H, D, Dp, prm.alpha, CENSUS_TAU, prm.tau_smooth, vol, wta};
+    std::vector<LevelDev> &lv = vp.impl->lv;
+    lv.assign(L, LevelDev{});
+    vp.L = L;
+    vp.min_level = m;
+    vp.D = D;
+    vp.HW = HW;
+    vp.levelN.assign(L, 0);
+    vp.levelE.assign(L, 0);
+    vp.levelC.assign(L, 0);
+    int Nmax = 1, Emax = 1, CHmax = 1;
+    size_t tm = tmp.mark();
+    int *im = tmp.alloc<int>(HW), *im2 = tmp.alloc<int>(HW);
+    uint32_t *kt = tmp.alloc<uint32_t>(HW), *ka = tmp.alloc<uint32_t>(HW), *va = tmp.alloc<uint32_t>(HW);
+    int *cnt = tmp.alloc<int>(HW + 1);
+    int *nch_total = tmp.alloc<int>(1);
     iota_int<<<blocks(HW, 256), 256, 0, st>>>(im, HW);
     note_launch();
     HBP_LAUNCH_CHECK();
     for (int l = 0; l < L; ++l)
     {
         LevelDev &d = lv[l];
-        d = LevelDev{};
         d.N = pyr.N[l];
         d.E = pyr.E[l];
         d.Nh = l + 1 < L ? pyr.N[l + 1] : 1;
@@ -702,11 +935,13 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
         d.nb_off = pyr.nb_off + pyr.nb_base[l];
         d.child = pyr.child + pyr.node_off[l];
         d.child_off = pyr.child_off + pyr.child_base[l];
+        vp.levelN[l] = d.N;
+        vp.levelE[l] = d.E;
         if (l >= m)
         {
             const int N = d.N, E = d.E;
-            uint32_t *pix = a.alloc<uint32_t>(HW);
-            int *pix_off = a.alloc<int>(N + 1);
+            uint32_t *pix = persist.alloc<uint32_t>(HW);
+            int *pix_off = persist.alloc<int>(N + 1);
             iota_xy<<<blocks(HW, 256), 256, 0, st>>>(kt, pix, im, W, HW);
             note_launch();
             HBP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (N + 1), st));
@@ -716,25 +951,25 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
             int bits = 1;
             while ((1 << bits) < N)
                 ++bits;
-            radix_sort_pairs_u32(kt, pix, ka, va, HW, bits, a, st);
-            exclusive_scan(cnt, pix_off, N + 1, nullptr, a, st);
-            int *chunk_off = a.alloc<int>(N + 1);
-            int *nch_total = a.alloc<int>(1);
+            radix_sort_pairs_u32(kt, pix, ka, va, HW, bits, tmp, st);
+            exclusive_scan(cnt, pix_off, N + 1, nullptr, tmp, st);
+            int *chunk_off = persist.alloc<int>(N + 1);
             chunk_counts<<<blocks(N + 1, 256), 256, 0, st>>>(pix_off, N, cnt);
             note_launch();
-            exclusive_scan(cnt, chunk_off, N + 1, nch_total, a, st);
+            exclusive_scan(cnt, chunk_off, N + 1, nch_total, tmp, st);
             d.nchunks = read_dev_int(nch_total, st);
-            int *chunk_node = a.alloc<int>(d.nchunks);
+            vp.levelC[l] = d.nchunks;
+            int *chunk_node = persist.alloc<int>(d.nchunks);
             chunk_fill<<<blocks(N, 256), 256, 0, st>>>(chunk_off, N, chunk_node);
             note_launch();
             HBP_LAUNCH_CHECK();
-            int *rev = a.alloc<int>(E);
+            int *rev = persist.alloc<int>(E);
             reverse_ids<<<blocks(E, 256), 256, 0, st>>>(d.bd, d.nb_off, E, rev);
             note_launch();
-            float *ml = a.alloc<float>(3 * (size_t)N), *mx = a.alloc<float>(N), *my = a.alloc<float>(N);
+            float *ml = tmp.alloc<float>(3 * (size_t)N), *mx = persist.alloc<float>(N), *my = persist.alloc<float>(N);
             level_means<<<blocks(N, 256), 256, 0, st>>>(pyr.sums + 6 * pyr.node_off[l], N, mx, my, ml);
             note_launch();
-            float *dc = a.alloc<float>(2 * (size_t)E);
+            float *dc = persist.alloc<float>(2 * (size_t)E);
             edge_weights<<<blocks(E, 256), 256, 0, st>>>(d.bd, E, N, ml, mx, my, dc);
             note_launch();
             HBP_LAUNCH_CHECK();
@@ -746,15 +981,16 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
             d.dc = dc;
             d.mx = mx;
             d.my = my;
-            d.plane = a.alloc<float4>((size_t)N * K);
-            d.cost = a.alloc<float>((size_t)N * K);
-            d.belief = a.alloc<float>((size_t)N * K);
-            d.pid = a.alloc<int4>(N);
-            d.keep = a.alloc<unsigned long long>(N);
+            d.plane = persist.alloc<float4>((size_t)N * K);
+            d.cost = persist.alloc<float>((size_t)N * K);
+            d.belief = persist.alloc<float>((size_t)N * K);
+            d.pid = persist.alloc<int4>(N);
+            d.keep = persist.alloc<unsigned long long>(N);
             HBP_CUDA(cudaMemsetAsync(d.plane, 0, sizeof(float4) * N * K, st));
             HBP_CUDA(cudaMemsetAsync(d.cost, 0, sizeof(float) * N * K, st));
             HBP_CUDA(cudaMemsetAsync(d.belief, 0, sizeof(float) * N * K, st));
             HBP_CUDA(cudaMemsetAsync(d.pid, 0, sizeof(int4) * N, st));
+            HBP_CUDA(cudaMemsetAsync(d.keep, 0, sizeof(unsigned long long) * N, st));
             Nmax = std::max(Nmax, N);
             Emax = std::max(Emax, E);
             CHmax = std::max(CHmax, d.nchunks);
@@ -767,99 +1003,260 @@ void hbp_infer(const Pyramid &pyr, const uint8_t *vol, int Wp, const float *wta,
             std::swap(im, im2);
         }
     }
-    float *msg = a.alloc<float>((size_t)Emax * K), *msg_t = a.alloc<float>((size_t)Emax * K);
-    float4 *pc = a.alloc<float4>(CHmax);
-    uint32_t *s_child = a.alloc<uint32_t>(Nmax), *s_nb = a.alloc<uint32_t>(Nmax),
-             *s_ransac = a.alloc<uint32_t>(Nmax);
-    float4 *buf = a.alloc<float4>((size_t)Nmax * P);
-
-    auto cost_slots = [&](const LevelDev &d, int sb) {
-        plane_cost_kernel<<<blocks((long)d.nchunks * 32, 256), 256, 0, st>>>(d, c, sb, pc);
-        note_launch();
-        finalize_cost_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, pc, sb);
-        note_launch();
-        HBP_LAUNCH_CHECK();
-    };
-    KernelProf *prof = prm.prof && prm.prof->on ? prm.prof : nullptr;
-    auto bp_step = [&](const LevelDev &d) {
-        if (prof)
-            prof->mark(st);
-        plane_cost_kernel<<<blocks((long)d.nchunks * 32, 256), 256, 0, st>>>(d, c, 2 * P, pc);
-        note_launch();
-        if (prof)
-        {
-            prof->mark(st);
-            // compulsory bytes: per pixel its packed id (4 B) and two volume
-            // bytes per candidate; per node 4 planes in and 4 costs out
-            prof->bytes += (double)HW * (4 + 2 * P) + (double)d.N * P * (16 + 4);
-            prof->launches++;
-        }
-        bp_edge_kernel<<<blocks(d.E, BE), dim3(BE, K), 0, st>>>(d, c, msg, msg_t);
-        note_launch();
-        bp_node_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, pc, msg_t);
-        note_launch();
-        bp_edge2_kernel<<<blocks(d.E, 128), 128, 0, st>>>(d, msg_t, msg);
-        note_launch();
-        HBP_LAUNCH_CHECK();
-    };
-
-    // top level: planes zero, messages and beliefs zero (hbp_isp.cu:1333-1337)
-    for (int li = L - 2; li >= m; --li)
+    ViewDev &vd = vp.impl->vd;
+    vd.c = c;
+    vd.L = L;
+    LevelDev *lv_dev = persist.alloc<LevelDev>(L);
+    HBP_CUDA(cudaMemcpyAsync(lv_dev, lv.data(), sizeof(LevelDev) * L, cudaMemcpyHostToDevice, st));
+    vd.lv = lv_dev;
+    for (int k = 0; k < 2; ++k)
     {
-        const LevelDev &d = lv[li], &h = lv[li + 1];
-        HBP_CUDA(cudaMemsetAsync(msg, 0, sizeof(float) * (size_t)d.E * K, st));
-        init_level_kernel<<<blocks(std::max(d.N, d.Nh), 128), 128, 0, st>>>(d, h, s_nb, s_ransac, s_child);
-        note_launch();
-        HBP_LAUNCH_CHECK();
-        cost_slots(d, 0);
-        cost_slots(d, P);
-        copy_cost_to_belief<<<blocks((long)d.N * K, 256), 256, 0, st>>>(d);
-        note_launch();
-        HBP_LAUNCH_CHECK();
+        vd.b.msgt[k] = persist.alloc<float>((size_t)Emax * K);
+        vd.b.pc[k] = persist.alloc<float4>(CHmax);
+        vd.b.s_ransac[k] = persist.alloc<uint32_t>(Nmax);
+    }
+    vd.b.s_child = persist.alloc<uint32_t>(Nmax);
+    vd.b.s_nb = persist.alloc<uint32_t>(Nmax);
+    vd.b.buf = persist.alloc<float4>((size_t)Nmax * P);
+    vd.disp = disp;
+    vd.plane_out = plane_out;
+    HBP_CUDA(cudaStreamSynchronize(st)); // lv (host) feeds the copy above
+    tmp.rewind(tm);
+}
+
+namespace
+{
+struct TaskState
+{
+    int v, li, step = 0, rb = 0;
+    float max_dz = 0, max_dn = 0;
+};
+
+int pick_group(double avg_chunk_px)
+{
+    if (avg_chunk_px > 96)
+        return 32;
+    if (avg_chunk_px > 48)
+        return 16;
+    if (avg_chunk_px > 16)
+        return 8;
+    return 4;
+}
+
+void launch_cost(const ViewDev *V, const StepDesc &d, int mode, cudaStream_t st)
+{
+    long threads = (long)d.pre[d.nt] * d.gs;
+    int nb = blocks(threads, 256);
+    switch (d.gs)
+    {
+    case 4: k_cost<4><<<nb, 256, 0, st>>>(V, d, mode); break;
+    case 8: k_cost<8><<<nb, 256, 0, st>>>(V, d, mode); break;
+    case 16: k_cost<16><<<nb, 256, 0, st>>>(V, d, mode); break;
+    default: k_cost<32><<<nb, 256, 0, st>>>(V, d, mode); break;
+    }
+    note_launch();
+}
+} // namespace
+
+// HBP_ISP::run_ms for every view of the batch (hbp_isp.cu:1313-1346): levels
+// coarse to fine in lockstep, views whose pyramid is shallower join when
+// their top level is reached; random-adjust steps run for the views whose
+// max_dz is still above the end threshold.
+void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &tmp,
+                   cudaStream_t st)
+{
+    const int nv = (int)views.size();
+    if (nv == 0)
+        return;
+    if (nv > MAXV)
+        throw StatusError{HBP_ERR_INVALID_ARG, "too many views in one BP batch"};
+    const int m = prm.min_level;
+    size_t mark = tmp.mark();
+    std::vector<ViewDev> vh(nv);
+    int maxL = 0;
+    for (int i = 0; i < nv; ++i)
+    {
+        vh[i] = views[i]->impl->vd;
+        maxL = std::max(maxL, views[i]->L);
+        if (views[i]->min_level != m)
+            throw StatusError{HBP_ERR_INVALID_ARG, "views of one batch share min_level"};
+    }
+    ViewDev *V = tmp.alloc<ViewDev>(nv);
+    HBP_CUDA(cudaMemcpyAsync(V, vh.data(), sizeof(ViewDev) * nv, cudaMemcpyHostToDevice, st));
+    KernelProf *prof = prm.prof && prm.prof->on ? prm.prof : nullptr;
+    long prof_step = 0;
+
+    auto desc = [&](const std::vector<TaskState *> &ts, int what, bool first) {
+        // what: 0 nodes, 1 chunks, 2 edges, 3 parents, 4 max(nodes, parents)
+        StepDesc d{};
+        d.nt = (int)ts.size();
+        d.pre[0] = 0;
+        double px = 0, chs = 0;
+        for (int k = 0; k < d.nt; ++k)
+        {
+            const TaskState &s = *ts[k];
+            const ViewPlan &vp = *views[s.v];
+            int n = vp.levelN[s.li], e = vp.levelE[s.li], ch = vp.levelC[s.li];
+            int nh = s.li + 1 < vp.L ? vp.levelN[s.li + 1] : 1;
+            int cnt = what == 0 ? n : what == 1 ? ch : what == 2 ? e : what == 3 ? nh : std::max(n, nh);
+            d.pre[k + 1] = d.pre[k] + cnt;
+            Task &t = d.t[k];
+            t.vd = V + s.v;
+            t.lvl = vh[s.v].lv + s.li;
+            t.lvh = s.li + 1 < vp.L ? vh[s.v].lv + s.li + 1 : t.lvl;
+            t.v = s.v;
+            t.li = s.li;
+            t.first = first ? 1 : 0;
+            t.rb = s.rb;
+            t.pb = s.step & 1;
+            t.mb = s.step & 1;
+            t.max_dz = s.max_dz;
+            t.max_dn = s.max_dn;
+            px += vp.HW;
+            chs += ch;
+        }
+        d.gs = pick_group(chs > 0 ? px / chs : 256);
+        return d;
+    };
+    auto timed = [&](bool on, auto &&f) {
+        if (on)
+            prof->mark(st);
+        f();
+        if (on)
+            prof->mark(st);
+    };
+
+    std::vector<TaskState> state(nv);
+    for (int li = maxL - 2; li >= m; --li)
+    {
+        std::vector<TaskState *> act;
+        for (int i = 0; i < nv; ++i)
+            if (views[i]->L - 2 >= li)
+            {
+                TaskState &s = state[i];
+                s.v = i;
+                s.li = li;
+                s.step = 0;
+                s.max_dz = (float)views[i]->D / 2.0f * (float)li / (float)views[i]->L;
+                s.max_dn = 1.0f * (float)li / (float)views[i]->L;
+                act.push_back(&s);
+            }
+        if (act.empty())
+            continue;
+        char rname[32];
+        std::snprintf(rname, sizeof(rname), "bp_level_%d", li);
+        NvtxRange level_range(rname);
+        // init_bp: priors and their data cost (partials in pc[0]), then costs,
+        // beliefs and seeds per node
+        {
+            StepDesc d = desc(act, 1, true);
+            for (int k = 0; k < d.nt; ++k)
+                d.t[k].pb = 0;
+            launch_cost(V, d, COST_INIT, st);
+            StepDesc dn = desc(act, 4, true);
+            for (int k = 0; k < dn.nt; ++k)
+                dn.t[k].pb = 0;
+            k_init_nodes<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+            note_launch();
+            HBP_LAUNCH_CHECK();
+        }
         const int iter_bp = 10 + 10 * li;
-        float max_dz = (float)D / 2.0f * (float)li / (float)L;
-        float max_dn = 1.0f * (float)li / (float)L;
         for (int i = 0; i < iter_bp; ++i)
         {
-            const int iter_random = (i <= iter_bp / 4 * 3) ? 4 : 5;
-            for (int it = 0;; ++it)
+            for (int it = 0; it <= 5; ++it)
             {
+                std::vector<TaskState *> ts;
+                int kind;
                 if (it <= 3)
                 {
-                    ransac_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, c, s_ransac);
-                    note_launch();
+                    kind = 0;
+                    ts = act;
                 }
-                else if (it <= 4)
+                else if (it == 4)
                 {
-                    select_child_kernel<<<blocks(h.N, 128), 128, 0, st>>>(d, h, s_child);
-                    note_launch();
-                    neighbor_kernel<<<blocks(h.N, 128), 128, 0, st>>>(h, s_nb, buf);
-                    note_launch();
-                    buf_to_candidates<<<blocks(h.N, 128), 128, 0, st>>>(h, buf);
-                    note_launch();
-                    set_candidate_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, h);
-                    note_launch();
-                }
-                else if (it <= iter_random && max_dz >= 0.01f)
-                {
-                    random_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, s_ransac, max_dz, max_dn);
-                    note_launch();
-                    max_dz /= 2.0f;
-                    max_dn /= 2.0f;
+                    kind = 1;
+                    ts = act;
                 }
                 else
-                    break;
+                {
+                    kind = 2;
+                    for (TaskState *s : act)
+                        if (i > iter_bp / 4 * 3 && s->max_dz >= 0.01f)
+                            ts.push_back(s);
+                    if (ts.empty())
+                        break;
+                }
+                const bool first = ts[0]->step == 0; // all tasks start a level together
+                const bool tp = prof && (prof_step++ % 16 == 0);
+                StepDesc dn = desc(ts, 0, first);
+                dn.mode = kind == 0 ? NODE_SELECT_RANSAC : kind == 2 ? NODE_SELECT_RANDOM : NODE_SELECT;
+                k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+                note_launch();
+                if (kind == 1)
+                {
+                    StepDesc dp = desc(ts, 3, first);
+                    k_child<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp);
+                    note_launch();
+                    k_neighbor<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp);
+                    note_launch();
+                    k_set_cand<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+                    note_launch();
+                }
+                StepDesc dc = desc(ts, 1, first);
+                timed(tp, [&] { launch_cost(V, dc, COST_STEP, st); });
+                StepDesc de = desc(ts, 2, first);
+                k_edges<<<blocks(de.pre[de.nt], 128), 128, 0, st>>>(V, de);
+                note_launch();
                 HBP_LAUNCH_CHECK();
-                bp_step(d);
+                if (tp)
+                {
+                    // compulsory bytes of the timed data-cost launch: every
+                    // pixel's packed id (4 B) and two volume bytes per candidate,
+                    // plus per chunk the node's 4 planes in and 4 partial sums out
+                    for (TaskState *s : ts)
+                    {
+                        const ViewPlan &vp = *views[s->v];
+                        prof->bytes += (double)vp.HW * (4 + 2 * P) + (double)vp.levelC[s->li] * (4 * 16 + 16);
+                    }
+                    prof->launches += 1;
+                }
+                for (TaskState *s : ts)
+                {
+                    s->step++;
+                    if (kind == 0 || kind == 2)
+                        s->rb ^= 1;
+                    if (kind == 2)
+                    {
+                        s->max_dz /= 2.0f;
+                        s->max_dn /= 2.0f;
+                    }
+                }
             }
         }
+        // final select of the level
+        StepDesc dn = desc(act, 0, false);
+        dn.mode = NODE_SELECT;
+        k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+        note_launch();
+        HBP_LAUNCH_CHECK();
     }
-    const LevelDev &d = lv[m];
-    map_kernel<<<blocks(d.N, 128), 128, 0, st>>>(d, c, disp, plane_out);
-    note_launch();
-    HBP_LAUNCH_CHECK();
+    // MAP at min_level for every view
+    {
+        NvtxRange map_range("bp_map");
+        std::vector<TaskState *> all;
+        for (int i = 0; i < nv; ++i)
+        {
+            state[i].v = i;
+            state[i].li = m;
+            all.push_back(&state[i]);
+        }
+        StepDesc d = desc(all, 0, false);
+        k_map<<<blocks((long)d.pre[d.nt] * 32, 128), 128, 0, st>>>(V, d);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+    }
     HBP_CUDA(cudaStreamSynchronize(st));
-    a.rewind(mark);
+    tmp.rewind(mark);
 }
 
 } // namespace hbp

@@ -83,8 +83,9 @@ def default_params(**kw) -> Params:
     return p
 
 
-def volume_pitch(W: int) -> int:
-    return lib().hbp_volume_pitch(W)
+def volume_pitch(D: int) -> int:
+    """Bytes per pixel of the pixel-major cost volume."""
+    return lib().hbp_volume_pitch(D)
 
 
 class Context:

@@ -70,11 +70,12 @@ void *hbp_ctx_stream(hbp_ctx *ctx);
 
 /* StereoCost::compute_stereo_cost("Census") (stereo_cost.cu:421-445) with the
  * grey conversion of the constructor (stereo_cost.cu:290-297): census of both
- * views, uint8 cost volume vol[d][y][x] (row pitch hbp_volume_pitch(W)) with
- * values min(popcount, 25), WTA disparity. With volR/wtaR non-NULL the
- * right-view volume and WTA of StereoCost::cost_to_right (stereo_cost.cu:
- * 488-516) are produced in the same pass. */
-int hbp_volume_pitch(int W);
+ * views, pixel-major uint8 cost volume vol[y][x][d] with hbp_volume_pitch(D)
+ * bytes per pixel (entries d >= D are 0) holding min(popcount, 25), and the
+ * WTA disparity. With volR/wtaR non-NULL the right-view volume and WTA of
+ * StereoCost::cost_to_right (stereo_cost.cu:488-516) are produced in the same
+ * pass. */
+int hbp_volume_pitch(int D);
 hbp_status hbp_cost_census_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H,
                              int D, uint32_t *censusL, uint32_t *censusR, uint8_t *vol,
                              float *wta, uint8_t *volR, float *wtaR, void *stream);
@@ -128,15 +129,24 @@ hbp_status hbp_run_pair(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, 
 
 /* A batch of same-size pairs whose images already sit in device memory
  * (arrays of npairs device pointers, held on the host); plane may be NULL or
- * hold NULL entries. Same path and outputs as hbp_run_pair per pair. */
+ * hold NULL entries. Same path and outputs as hbp_run_pair per pair. Pairs run
+ * concurrently on up to hbp_set_lanes() lanes (own stream and device slabs
+ * each, default 8 or $HBP_LANES), one host thread per lane; the call returns
+ * when every pair is done. */
 hbp_status hbp_run_batch_d(hbp_ctx *ctx, int npairs, const uint8_t *const *bgrL,
                            const uint8_t *const *bgrR, int W, int H, int D, const hbp_params *prm,
                            float *const *disp, float *const *plane);
+
+hbp_status hbp_set_lanes(hbp_ctx *ctx, int lanes);
 
 /* -------------------------------------------------------- measurement */
 
 /* Number of kernels the library has launched since it was loaded. */
 long hbp_launch_count(void);
+/* Host wall time (ms) of the last hbp_run_batch_d / hbp_run_pair call:
+ * [0] preparation (cost volume, pyramid, BP setup; concurrent lanes),
+ * [1] batched BP, [2] post stages, [3] whole call. */
+hbp_status hbp_last_phase_ms(hbp_ctx *ctx, double *out4);
 /* While enabled, launches of the data-cost kernel (the dominant kernel of the
  * path) are bracketed by CUDA events on the context stream: mode 1 times every
  * launch, mode 2 only those of the first pair of each hbp_run_batch_d call

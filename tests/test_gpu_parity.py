@@ -36,17 +36,18 @@ def dev(torch, a):
 
 def run_cost(E, ctx, torch, L, R, D, right=False):
     H, W = L.shape[:2]
-    Wp = E.volume_pitch(W)
+    Dp = E.volume_pitch(D)
     dL, dR = dev(torch, L), dev(torch, R)
     cL = torch.zeros(H * W, dtype=torch.int32, device="cuda")
     cR = torch.zeros_like(cL)
-    vol = torch.zeros(D * H * Wp, dtype=torch.uint8, device="cuda")
+    vol = torch.zeros(H * W * Dp, dtype=torch.uint8, device="cuda")
     wta = torch.zeros(H * W, dtype=torch.float32, device="cuda")
     volR = torch.zeros_like(vol) if right else None
     wtaR = torch.zeros_like(wta) if right else None
     ctx.cost_census_d(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR)
     torch.cuda.synchronize()
-    strip = lambda v: v.cpu().numpy().reshape(D, H, Wp)[:, :, :W].reshape(D, H * W)
+    # engine layout [y][x][Dp] -> oracle layout [d][y*W+x]
+    strip = lambda v: np.ascontiguousarray(v.cpu().numpy().reshape(H * W, Dp)[:, :D].T)
     out = dict(censusL=cL.cpu().numpy().view(np.uint32).reshape(H, W),
                censusR=cR.cpu().numpy().view(np.uint32).reshape(H, W),
                vol=strip(vol), wta=wta.cpu().numpy().reshape(H, W), vol_dev=vol, wta_dev=wta)
@@ -182,3 +183,22 @@ def test_run_pair_matches_oracle_pipeline(eng, golden_dir, name):
     disp = ctx.run_pair(L, R, D, E.default_params(post=1))
     ref = O.driver_median(O.pipeline(L, R, D)["disp"])
     assert np.array_equal(disp.view(np.uint32), ref.view(np.uint32)), float(np.mean(disp != ref))
+
+
+def test_batch_lanes_match_single_pair(eng, golden_dir):
+    """Pairs run concurrently on several lanes give the same disparity as one by one."""
+    import ctypes as C
+    E, ctx, torch = eng
+    from scenes import make_scene
+    scenes = [make_scene(160, 120, 48, 50 + i) for i in range(5)]
+    single = [ctx.run_pair(s.left, s.right, 48, E.default_params(post=1)) for s in scenes]
+    E._check(E.lib().hbp_set_lanes(ctx.h, 3))
+    dL = [dev(torch, s.left) for s in scenes]
+    dR = [dev(torch, s.right) for s in scenes]
+    out = [torch.zeros((120, 160), dtype=torch.float32, device="cuda") for _ in scenes]
+    arr = lambda ts: (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+    prm = E.default_params(post=1)
+    E._check(E.lib().hbp_run_batch_d(ctx.h, len(scenes), arr(dL), arr(dR), 160, 120, 48, C.byref(prm), arr(out), None))
+    torch.cuda.synchronize()
+    for a, b in zip(single, out):
+        assert np.array_equal(a, b.cpu().numpy())
