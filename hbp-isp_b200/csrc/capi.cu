@@ -590,6 +590,17 @@ hbp_status hbp_driver_median_d(hbp_ctx *c, float *disp, int W, int H, void *stre
     });
 }
 
+hbp_status hbp_driver_median_noalloc_d(float *disp, int W, int H, void *stream)
+{
+    if (!disp)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    if (W <= 0 || H <= 0)
+        return fail(HBP_ERR_INVALID_ARG, "W and H must be positive");
+    if ((long)W * H > HBP_NOALLOC_MAX_PIXELS)
+        return fail(HBP_ERR_INVALID_ARG, "W*H exceeds HBP_NOALLOC_MAX_PIXELS (2097152), the size of the static scratch");
+    return guarded([&] { launch_driver_median_noalloc(disp, W, H, static_cast<cudaStream_t>(stream)); });
+}
+
 namespace
 {
 // Every pair of a batch: preparation on the lanes (one host thread each),

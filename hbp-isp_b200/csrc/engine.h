@@ -178,5 +178,7 @@ void launch_weighted_median(const uint8_t *bgr, const uint8_t *fail, const float
                             float *plane_out, int W, int H, const float *wtab, Arena &tmp,
                             cudaStream_t st);
 void launch_driver_median(float *disp, float *tmp, int W, int H, cudaStream_t st);
+// same filter with the file-scope static scratch of noalloc.cu (allocates nothing)
+void launch_driver_median_noalloc(float *disp, int W, int H, cudaStream_t st);
 
 } // namespace hbp

@@ -88,6 +88,16 @@ def volume_pitch(D: int) -> int:
     return lib().hbp_volume_pitch(D)
 
 
+NOALLOC_MAX_PIXELS = 2097152  # HBP_NOALLOC_MAX_PIXELS of the header
+
+
+def driver_median_noalloc_d(disp, W: int, H: int, stream: int | None = None):
+    """hbp_driver_median_noalloc_d: in-place driver median of a device disparity
+    map on the current device, no context and no device allocation; enqueued
+    on ``stream`` (None = legacy default stream) and not synchronised."""
+    _check(lib().hbp_driver_median_noalloc_d(_p(disp), W, H, P(stream) if stream else None))
+
+
 class Context:
     """One device context (stream + device memory slab). Not thread safe."""
 

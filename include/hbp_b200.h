@@ -118,6 +118,29 @@ hbp_status hbp_weighted_median_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_
 /* medianFilter of the single-pair driver (main_stereo_hbp_isp.cu:120-192). */
 hbp_status hbp_driver_median_d(hbp_ctx *ctx, float *disp, int W, int H, void *stream);
 
+/* The same driver median with no context and no device allocation. This entry
+ * point has no counterpart in the reference: it serves callers that may not
+ * allocate device memory, e.g. a frame loop that reserved its whole device
+ * budget up front (cudaMalloc/cudaFree synchronise the device and stall the
+ * other streams) or a PyTorch process whose caching allocator already holds
+ * the free memory, where creating a context could fail.
+ *   - Scratch: a file-scope device array of HBP_NOALLOC_MAX_PIXELS floats
+ *     (8 MiB); W*H above that is rejected with HBP_ERR_INVALID_ARG before
+ *     anything is launched. No scratch contents need to start at zero: the
+ *     first pass writes every entry the second pass reads.
+ *   - Device: the calling thread's current CUDA device, which must own disp
+ *     and stream (NULL = the legacy default stream).
+ *   - Setup: the first call on each device looks up the scratch address
+ *     (cudaGetSymbolAddress, which loads the module holding it); make that
+ *     first call before any stream capture begins.
+ *   - Asynchronous: enqueues two kernels on stream and returns; disp is
+ *     updated in place when the stream reaches them.
+ *   - One scratch per device: calls whose executions may overlap (different
+ *     streams or host threads without ordering between them) race on it;
+ *     order them on one stream or with events. */
+#define HBP_NOALLOC_MAX_PIXELS 2097152L
+hbp_status hbp_driver_median_noalloc_d(float *disp, int W, int H, void *stream);
+
 /* ------------------------------------------------------------ whole pair */
 
 /* The single-pair path of main_stereo_hbp_isp.cu:33-76 (post = 1) or of
