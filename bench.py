@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--fp16", type=int, default=0, help="store BP messages as FP16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="after the timed region, one extra step with every BP kernel of every 8th "
+                         "BP step event-timed; per-kernel/per-level estimate printed to stderr")
     return ap.parse_args()
 
 
@@ -140,6 +143,34 @@ def cpu_baseline(scene, W, H, D):
     return {"value": 1.0 / dt, "unit": "pairs/s", "cores": cores, "kind": "port",
             "sample": f"1 pair {W}x{H} D{D} (seed {scene.seed}) through the CPU oracle, "
                       f"OpenMP on {cores} threads, {dt:.1f} s"}
+
+
+KINDS = ["node_select", "child_cand", "neighbor_cand", "set_cand", "data_cost", "edge_msgs",
+         "prior_cost", "init_nodes", "map"]
+
+
+def breakdown(E, ctx, step):
+    """One untimed step with the BP kernels event-timed (mode 3): estimated
+    device ms per step by kernel kind and by (kind, pyramid level)."""
+    import ctypes as C
+    n = 10 * 32
+    ms, timed, allc = (C.c_double * n)(), (C.c_long * n)(), (C.c_long * n)()
+    E._check(E.lib().hbp_profile_enable(ctx.h, 3))
+    step()
+    E._check(E.lib().hbp_profile_breakdown(ctx.h, ms, timed, allc))
+    E._check(E.lib().hbp_profile_enable(ctx.h, 0))
+    by_kind, by_level = {}, {}
+    for k, name in enumerate(KINDS):
+        for lv in range(32):
+            i = k * 32 + lv
+            if allc[i] == 0 or timed[i] == 0:
+                continue
+            est = ms[i] / timed[i] * allc[i]
+            by_kind[name] = by_kind.get(name, 0.0) + est
+            by_level.setdefault(str(lv), {})[name] = {"est_ms": round(est, 3), "launches": allc[i],
+                                                      "avg_us": round(1e3 * ms[i] / timed[i], 2)}
+    return {"breakdown_est_ms_per_step": {k: round(v, 3) for k, v in by_kind.items()},
+            "total_est_ms": round(sum(by_kind.values()), 3), "by_level": by_level}
 
 
 def run_reference(args, rank):
@@ -260,6 +291,9 @@ def main():
         t_max = float(t.item())
     total_pairs = NP * args.steps * world
     value = total_pairs / (t_max / 1e3)
+
+    if args.breakdown and rank == 0:
+        print(json.dumps(breakdown(E, ctx, step)), file=sys.stderr)
 
     # ------------------------------------------------------------ end to end
     e2e = None

@@ -220,11 +220,10 @@ void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint
     a.reset();
     L->tmp.reset();
     HBP_CUDA(cudaMemsetAsync(L->err_dev, 0, sizeof(int), st));
-    const int Dp = volume_pitch(D);
     const bool lr = p.post == 2;
     uint32_t *cL = a.alloc<uint32_t>(n), *cR = a.alloc<uint32_t>(n);
-    uint8_t *vol = a.alloc<uint8_t>((size_t)Dp * n);
-    uint8_t *volR = lr ? a.alloc<uint8_t>((size_t)Dp * n) : nullptr;
+    uint8_t *vol = a.alloc<uint8_t>(volume_bytes(W, H, D));
+    uint8_t *volR = lr ? a.alloc<uint8_t>(volume_bytes(W, H, D)) : nullptr;
     float *wta = a.alloc<float>(n), *wtaR = lr ? a.alloc<float>(n) : nullptr;
     sl->plane = plane ? plane : a.alloc<float>(3 * n);
     {
@@ -240,7 +239,7 @@ void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint
     L->tmp.reset();
     {
         NvtxRange r("bp_setup");
-        hbp_prepare(sl->pyr, vol, Dp, wta, D, q, disp, sl->plane, a, L->tmp, st, sl->plan);
+        hbp_prepare(sl->pyr, vol, wta, D, q, disp, sl->plane, a, L->tmp, st, sl->plan);
     }
     if (lr)
     {
@@ -250,7 +249,7 @@ void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint
         segment_image(dR, W, H, sl->pyrR, a, L->tmp, L->err_dev, st);
         check_device_error(L);
         L->tmp.reset();
-        hbp_prepare(sl->pyrR, volR, Dp, wtaR, D, q, sl->dispR, sl->planeR, a, L->tmp, st, sl->planR);
+        hbp_prepare(sl->pyrR, volR, wtaR, D, q, sl->dispR, sl->planeR, a, L->tmp, st, sl->planR);
     }
     HBP_CUDA(cudaStreamSynchronize(st));
 }
@@ -406,7 +405,10 @@ void hbp_ctx_destroy(hbp_ctx *c)
 
 void *hbp_ctx_stream(hbp_ctx *c) { return c ? (void *)c->st : nullptr; }
 
-int hbp_volume_pitch(int D) { return volume_pitch(D); }
+size_t hbp_volume_bytes(int W, int H, int D)
+{
+    return W > 0 && H > 0 && D > 0 ? volume_bytes(W, H, D) : 0;
+}
 
 hbp_status hbp_cost_census_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
                              uint32_t *censusL, uint32_t *censusR, uint8_t *vol, float *wta,
@@ -528,7 +530,7 @@ hbp_status hbp_infer_d(hbp_ctx *c, const uint8_t *vol, const float *wta, int D, 
         ensure_slot(sl, (long)c->pyr.W * c->pyr.H, D);
         sl->mem.reset();
         c->tmp.reset();
-        hbp_prepare(c->pyr, vol, volume_pitch(D), wta, D, q, disp, plane, sl->mem, c->tmp, st, sl->plan);
+        hbp_prepare(c->pyr, vol, wta, D, q, disp, plane, sl->mem, c->tmp, st, sl->plan);
         c->tmp.reset();
         std::vector<ViewPlan *> views{&sl->plan};
         hbp_run_views(views, q, c->tmp, st);
@@ -774,10 +776,11 @@ hbp_status hbp_profile_enable(hbp_ctx *c, int on)
 {
     if (!c)
         return fail(HBP_ERR_INVALID_ARG, "null context");
-    if (on < 0 || on > 2)
-        return fail(HBP_ERR_INVALID_ARG, "profile mode must be 0, 1 or 2");
+    if (on < 0 || on > 3)
+        return fail(HBP_ERR_INVALID_ARG, "profile mode must be 0, 1, 2 or 3");
     c->prof_mode = on;
     c->prof.on = on != 0;
+    c->prof.breakdown = on == 3;
     c->prof.reset();
     for (auto &l : c->lanes)
         l->prof.reset();
@@ -792,8 +795,14 @@ hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *byte
         *ms = c->prof.total_ms();
         *launches = c->prof.launches;
         *bytes = c->prof.bytes;
-
     });
+}
+
+hbp_status hbp_profile_breakdown(hbp_ctx *c, double *ms, long *timed, long *all)
+{
+    if (!c || !ms || !timed || !all)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] { c->prof.read_breakdown(ms, timed, all); });
 }
 
 } // extern "C"

@@ -7,11 +7,11 @@
 // HammingDistanceCostKernel (:148-207), cost_u1_to_f1_transpose (:209-228),
 // WTA_D_k (:248-280); right view: cost_to_right (:471-516).
 //
-// Layout: pixel-major vol[y][x][d] with Dp = round_up(D, 16) bytes per pixel
-// (entries d >= D are 0), so the data-cost kernel finds V[d] and V[d+1] of all
-// of a pixel's candidate planes in one 32-byte sector. Values are
-// min(popcount, 25) (exact in 8 bits; the reference's float volume holds the
-// same integers).
+// Layout: 8x4-pixel tiles, disparity-major inside a tile (vol_offset in
+// engine.h): one 32-byte sector holds a whole tile at one disparity, so the
+// data-cost kernel, whose warps walk compact superpixels, touches few sectors
+// per load. Values are min(popcount, 25) (exact in 8 bits; the reference's
+// float volume holds the same integers).
 #include "engine.h"
 
 namespace hbp
@@ -79,103 +79,100 @@ __global__ void __launch_bounds__(CT_W *CT_H)
     cR[(size_t)y * W + x] = b;
 }
 
-constexpr int HM_THREADS = 128; // one pixel per thread, 128 pixels per block
+constexpr int HM_TILES = 8;               // 8x4-pixel tiles per block (one warp each)
+constexpr int HM_THREADS = 32 * HM_TILES;  // 256
+constexpr int HM_COLS = VT_W * HM_TILES;   // 64 columns x VT_H rows per block
 
-// One block = 128 consecutive pixels of a row; thread = pixel. Shared memory
-// holds the left census of the segment plus D columns to the right (right
-// view) and the right census of the segment plus D columns to the left
-// (clamped at the image border, which reproduces the reference's use of
-// cR[row][0] for x-d < 0). Each thread writes its Dp cost bytes contiguously
-// in 16-byte words (pixel-major, like the reference's u8 volume
-// [px][D_align]).
+// Shared-memory row stride of the census staging: >= HM_COLS + D and = 8
+// (mod 32), so the four rows of a warp's tile fall in distinct banks.
+__host__ __device__ inline int hm_stride(int D) { return (HM_COLS + D + 31) / 32 * 32 + 8; }
+
+// One block = a strip of 64 columns x 4 rows (8 tiles); warp w = tile w, lane
+// = (y & 3) * 8 + (x & 7). Shared memory holds, per row, the left census of
+// the strip plus D columns to the right (right view) and the right census of
+// the strip plus D columns to the left, clamped at the image border (which
+// reproduces the reference's use of cR[row][0] for x-d < 0). For every d the
+// warp stores its tile's 32 cost bytes as one sector; pixels outside the image
+// get 0.
 __global__ void __launch_bounds__(HM_THREADS)
     hamming_wta_kernel(const uint32_t *__restrict__ cL, const uint32_t *__restrict__ cR, int W,
-                       int H, int D, int Dp, uint8_t *__restrict__ vol, float *__restrict__ wta,
+                       int H, int D, int TX, uint8_t *__restrict__ vol, float *__restrict__ wta,
                        uint8_t *__restrict__ volR, float *__restrict__ wtaR)
 {
     extern __shared__ uint32_t sm[];
-    const int y = blockIdx.y;
-    const int xs = blockIdx.x * HM_THREADS;
-    const int span = HM_THREADS + D;
-    uint32_t *sLc = sm;        // cL[xs + i], i in [0, span)  (clamped to W-1)
-    uint32_t *sRc = sm + span; // cR[xs - D + i], i in [0, span) (clamped to 0 / W-1)
-    const uint32_t *rowL = cL + (size_t)y * W, *rowR = cR + (size_t)y * W;
-    for (int i = threadIdx.x; i < span; i += HM_THREADS)
+    const int xs = blockIdx.x * HM_COLS, ys = blockIdx.y * VT_H;
+    const int S = hm_stride(D), span = HM_COLS + D;
+    uint32_t *sLc = sm;              // [VT_H][S]: cL[y][xs + i]
+    uint32_t *sRc = sm + VT_H * S;   // [VT_H][S]: cR[y][xs - D + i]
+    for (int r = 0; r < VT_H; ++r)
     {
-        int gl = min(xs + i, W - 1);
-        int gr = max(min(xs - D + i, W - 1), 0);
-        sLc[i] = rowL[gl];
-        sRc[i] = rowR[gr];
+        const int yy = min(ys + r, H - 1);
+        const uint32_t *rowL = cL + (size_t)yy * W, *rowR = cR + (size_t)yy * W;
+        for (int i = threadIdx.x; i < span; i += HM_THREADS)
+        {
+            sLc[r * S + i] = rowL[min(xs + i, W - 1)];
+            sRc[r * S + i] = rowR[max(min(xs - D + i, W - 1), 0)];
+        }
     }
     __syncthreads();
-    const int lx = threadIdx.x, x = xs + lx;
-    if (x >= W)
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = (xs >> 3) + w;
+    if (tx >= TX)
         return;
-    const size_t px = (size_t)y * W + x;
-    const uint32_t cl = sLc[lx];
-    uint4 *out = reinterpret_cast<uint4 *>(vol + px * Dp);
+    const int ly = lane >> 3, lc = w * VT_W + (lane & 7);
+    const int x = xs + lc, y = ys + ly;
+    const bool in = x < W && y < H;
+    const uint32_t *rL = sLc + ly * S, *rR = sRc + ly * S;
+    const size_t tile = (size_t)blockIdx.y * TX + tx;
+    uint8_t *out = vol + tile * D * VT_BYTES + lane;
+    const uint32_t cl = rL[lc];
     int best = 1 << 30, arg = 0;
-    for (int d0 = 0; d0 < Dp; d0 += 16)
+    for (int d = 0; d < D; ++d)
     {
-        uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
+        int c = 0;
+        if (in)
         {
-            int d = d0 + j;
-            int c = 0;
-            if (d < D)
+            // cR[max(x - d, 0)]: local index (lc - d) + D in rR
+            c = __popc(cl ^ rR[lc - d + D]);
+            c = c < 25 ? c : 25;
+            if (c < best)
             {
-                // cR[max(x - d, 0)]: local index (lx - d) + D in sRc
-                c = __popc(cl ^ sRc[lx - d + D]);
-                c = c < 25 ? c : 25;
-                if (c < best)
-                {
-                    best = c;
-                    arg = d;
-                }
+                best = c;
+                arg = d;
             }
-            w[j >> 2] |= (uint32_t)c << (8 * (j & 3));
         }
-        out[d0 >> 4] = make_uint4(w[0], w[1], w[2], w[3]);
+        out[(size_t)d * VT_BYTES] = (uint8_t)c;
     }
-    wta[px] = (float)arg;
+    if (in)
+        wta[(size_t)y * W + x] = (float)arg;
     if (!volR)
         return;
-    // Right view: VR[y][x][d] = V[y][min(x + d, W - 1)][d] (convert_vol_L2R_k
+    // Right view: VR(x, y, d) = V(min(x + d, W - 1), y, d) (convert_vol_L2R_k
     // followed by fill_out_of_view_k).
-    uint4 *outR = reinterpret_cast<uint4 *>(volR + px * Dp);
+    uint8_t *outR = volR + tile * D * VT_BYTES + lane;
     best = 1 << 30;
     arg = 0;
-    for (int d0 = 0; d0 < Dp; d0 += 16)
+    for (int d = 0; d < D; ++d)
     {
-        uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
+        int c = 0;
+        if (in)
         {
-            int d = d0 + j;
-            int c = 0;
-            if (d < D)
+            int xl = min(x + d, W - 1); // source column in the left view
+            int xr = max(xl - d, 0);    // its match in the right view
+            c = __popc(rL[xl - xs] ^ rR[xr - xs + D]);
+            c = c < 25 ? c : 25;
+            if (c < best)
             {
-                int xl = min(x + d, W - 1); // source column in the left view
-                int xr = max(xl - d, 0);    // its match in the right view
-                c = __popc(sLc[xl - xs] ^ sRc[xr - xs + D]);
-                c = c < 25 ? c : 25;
-                if (c < best)
-                {
-                    best = c;
-                    arg = d;
-                }
+                best = c;
+                arg = d;
             }
-            w[j >> 2] |= (uint32_t)c << (8 * (j & 3));
         }
-        outR[d0 >> 4] = make_uint4(w[0], w[1], w[2], w[3]);
+        outR[(size_t)d * VT_BYTES] = (uint8_t)c;
     }
-    wtaR[px] = (float)arg;
+    if (in)
+        wtaR[(size_t)y * W + x] = (float)arg;
 }
-
 } // namespace
-
-int volume_pitch(int D) { return (D + 15) / 16 * 16; }
 
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
@@ -185,10 +182,10 @@ void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, 
     census_pair_kernel<<<cg, cb, 0, st>>>(bgrL, bgrR, W, H, cL, cR);
     note_launch();
     HBP_LAUNCH_CHECK();
-    const int Dp = volume_pitch(D);
-    size_t smem = sizeof(uint32_t) * 2 * (HM_THREADS + D);
-    dim3 hg(ceil_div(W, HM_THREADS), H);
-    hamming_wta_kernel<<<hg, HM_THREADS, smem, st>>>(cL, cR, W, H, D, Dp, vol, wta, volR, wtaR);
+    const int TX = ceil_div(W, VT_W);
+    size_t smem = sizeof(uint32_t) * 2 * VT_H * hm_stride(D);
+    dim3 hg(ceil_div(W, HM_COLS), ceil_div(H, VT_H));
+    hamming_wta_kernel<<<hg, HM_THREADS, smem, st>>>(cL, cR, W, H, D, TX, vol, wta, volR, wtaR);
     note_launch();
     HBP_LAUNCH_CHECK();
 }

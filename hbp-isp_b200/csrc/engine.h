@@ -45,7 +45,22 @@ struct Scratch
 
 // ---------------------------------------------------------------------------
 // cost.cu
-int volume_pitch(int D); // bytes per pixel of the pixel-major volume
+// Cost volume layout: 8x4-pixel tiles in raster order, disparity-major inside
+// a tile; byte (x, y, d) sits at vol_offset(x, y, d). Tiles that overhang the
+// image hold 0 for the missing pixels.
+constexpr int VT_W = 8, VT_H = 4, VT_BYTES = VT_W * VT_H;
+__host__ __device__ __forceinline__ size_t vol_tile_base(int x, int y, int TX, int D)
+{
+    return ((size_t)(y >> 2) * TX + (x >> 3)) * (size_t)D * VT_BYTES + ((y & 3) << 3) + (x & 7);
+}
+__host__ __device__ __forceinline__ size_t vol_offset(int x, int y, int d, int TX, int D)
+{
+    return vol_tile_base(x, y, TX, D) + (size_t)d * VT_BYTES;
+}
+inline size_t volume_bytes(int W, int H, int D)
+{
+    return (size_t)((W + VT_W - 1) / VT_W) * ((H + VT_H - 1) / VT_H) * (size_t)D * VT_BYTES;
+}
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
                  cudaStream_t st);
@@ -105,11 +120,49 @@ struct KernelProf
     size_t used = 0;
     double bytes = 0; // algorithmic bytes of the timed launches
     long launches = 0;
+    // breakdown mode: every BP kernel of every 8th step timed, per (kind, level)
+    static constexpr int KINDS = 10, LEVELS = 32;
+    bool breakdown = false;
+    std::vector<cudaEvent_t> evb;
+    size_t usedb = 0;
+    std::vector<int> tagb;           // kind * LEVELS + level of each timed pair
+    long count[KINDS * LEVELS] = {}; // every launch, timed or not
     void reset()
     {
         used = 0;
         bytes = 0;
         launches = 0;
+        usedb = 0;
+        tagb.clear();
+        for (long &x : count)
+            x = 0;
+    }
+    void markb(cudaStream_t st)
+    {
+        if (usedb == evb.size())
+        {
+            cudaEvent_t e;
+            HBP_CUDA(cudaEventCreate(&e));
+            evb.push_back(e);
+        }
+        HBP_CUDA(cudaEventRecord(evb[usedb++], st));
+    }
+    void read_breakdown(double *ms, long *timed, long *all)
+    {
+        for (int i = 0; i < KINDS * LEVELS; ++i)
+        {
+            ms[i] = 0;
+            timed[i] = 0;
+            all[i] = count[i];
+        }
+        for (size_t i = 0; i + 1 < usedb; i += 2)
+        {
+            float t = 0;
+            HBP_CUDA(cudaEventSynchronize(evb[i + 1]));
+            HBP_CUDA(cudaEventElapsedTime(&t, evb[i], evb[i + 1]));
+            ms[tagb[i / 2]] += t;
+            timed[tagb[i / 2]] += 1;
+        }
     }
     void mark(cudaStream_t st)
     {
@@ -161,7 +214,7 @@ struct ViewPlan
 
 // Level setup of one view (persistent data in `persist`, temporaries in `tmp`);
 // BP writes disparity (HW floats) and planes (HW x 3, may be null) there.
-void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wta, int D,
+void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D,
                  const HbpParams &prm, float *disp, float *plane, Arena &persist, Arena &tmp,
                  cudaStream_t st, ViewPlan &vp);
 // HBP_ISP::run_ms for up to 32 prepared views at once (same min_level).

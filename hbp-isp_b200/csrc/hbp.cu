@@ -11,12 +11,13 @@
 //
 // Engine layout (node-major / edge-major, so the neighbour gathers of the BP
 // kernels read contiguous slots): plane[n][12] float4, cost/belief[n][12],
-// msg/msg_t[e][12]. Pixels of a node are listed in raster order (packed y<<16|x)
-// and cut into chunks of 256 for the data cost.
+// msg/msg_t[e][12]. Each level lists its pixels sorted by node, raster order
+// inside a node (packed y<<16|x); the data cost walks that list in windows of
+// 256 positions, and a node's chunks are the windows it overlaps.
 //
 // Reduction orders (the reference's float atomics / reduce_by_key have none):
-// chunk sums over 32 slots x 8 deep combined by an xor butterfly, chunks of a
-// node added in order; beliefs = cost + out-edge messages in edge order.
+// plane costs by the segmented-scan order described at k_cost; beliefs =
+// cost + out-edge messages in edge order.
 // Everything else follows the reference operation for operation; this file is
 // compiled without multiply-add contraction so that each a*b+c rounds twice
 // like the CPU oracle.
@@ -37,8 +38,8 @@ struct LevelDev
     const int *clus;         // N -> parent
     const uint32_t *pix;     // HW packed y<<16|x, sorted by (node, pixel)
     const int *pix_off;      // N + 1
-    const int *chunk_off;    // N + 1
-    const int *chunk_node;   // nchunks
+    const int *chunk_off;    // N + 1: first data-cost chunk of each node
+    const int *pnode;        // HW: node of each list position
     const int2 *bd;          // E
     const int *bdl;          // E
     const int *nb_off;       // N + 1
@@ -55,9 +56,9 @@ struct LevelDev
 
 struct Common
 {
-    int W, H, D, Dp;
+    int W, H, D, TX; // TX: volume tiles per row
     float lambda, tau, tau_smooth;
-    const uint8_t *vol; // [H][W][Dp]
+    const uint8_t *vol; // tiled, vol_offset()
     const float *wta;   // HW
 };
 
@@ -74,9 +75,9 @@ __device__ __forceinline__ float pixel_cost(const Common &c, int x, int y, float
         cost = c.tau;
     else
     {
-        const uint8_t *pv = c.vol + ((size_t)y * c.W + x) * c.Dp + d;
+        const uint8_t *pv = c.vol + vol_offset(x, y, d, c.TX, c.D);
         float v0 = (float)pv[0];
-        float v1 = (float)pv[1];
+        float v1 = (float)pv[VT_BYTES];
         cost = ((float)(d + 1) - d_f) * v0 + (d_f - (float)d) * v1;
     }
     return c.lambda * cost;
@@ -115,21 +116,15 @@ __global__ void count_keys(const int *k, int n, int *count)
         atomicAdd(&count[k[i]], 1);
 }
 
+// A node's data-cost chunks are the 256-position windows of the level's pixel
+// list that it overlaps.
 __global__ void chunk_counts(const int *pix_off, int N, int *nch)
 {
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n < N)
-        nch[n] = (pix_off[n + 1] - pix_off[n] + PC_CHUNK - 1) / PC_CHUNK;
+        nch[n] = ((pix_off[n + 1] - 1) / PC_CHUNK) - (pix_off[n] / PC_CHUNK) + 1;
     if (n == N)
         nch[N] = 0;
-}
-
-__global__ void chunk_fill(const int *chunk_off, int N, int *chunk_node)
-{
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < N)
-        for (int c = chunk_off[n]; c < chunk_off[n + 1]; ++c)
-            chunk_node[c] = n;
 }
 
 // reverse_bd_id_k (hbp_isp.cu:154-175): first edge t -> s in t's range.
@@ -258,7 +253,7 @@ enum NodeMode
 
 struct StepDesc
 {
-    int nt, gs, mode;
+    int nt, mode;
     int pre[MAXV + 1];
     Task t[MAXV];
 };
@@ -526,71 +521,6 @@ __global__ void __launch_bounds__(128) k_set_cand(const ViewDev *__restrict__ V,
         l.plane[(size_t)n * K + 2 * P + p] = v.b.buf[(size_t)pn * P + p];
 }
 
-// Data cost of 4 planes over one chunk with a group of GS lanes. The value is
-// the engine's 32-slot reduction: slot j accumulates the chunk's pixels j,
-// j+32, ... sequentially; the 32 slots are combined by an xor butterfly with
-// offsets 16..1. Lane r of the group holds slots r + GS*u; butterfly levels
-// with offset >= GS pair slots inside the lane, the others pair lanes by
-// shuffles, so every group size gives the same sums.
-template <int GS>
-__device__ __forceinline__ float4 group_cost(const LevelDev &l, const Common &c, int n, int ch, const float4 pl[4],
-                                             int r, bool valid)
-{
-    constexpr int SL = 32 / GS;
-    float acc[SL][4];
-#pragma unroll
-    for (int u = 0; u < SL; ++u)
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            acc[u][k] = 0.f;
-    if (valid)
-    {
-        const int start = l.pix_off[n] + (ch - l.chunk_off[n]) * PC_CHUNK;
-        const int end = min(start + PC_CHUNK, l.pix_off[n + 1]);
-#pragma unroll
-        for (int u = 0; u < SL; ++u)
-        {
-            const int j = r + GS * u;
-#pragma unroll
-            for (int dd = 0; dd < PC_CHUNK / 32; ++dd)
-            {
-                int idx = start + j + 32 * dd;
-                if (idx < end)
-                {
-                    uint32_t xy = l.pix[idx];
-                    int x = px_x(xy), y = px_y(xy);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        acc[u][k] = acc[u][k] + pixel_cost(c, x, y, pl[k]);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int off = 16; off >= GS; off >>= 1)
-    {
-        const int ku = off / GS;
-        float nw[SL][4];
-#pragma unroll
-        for (int u = 0; u < SL; ++u)
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                nw[u][k] = acc[u][k] + acc[u ^ ku][k];
-#pragma unroll
-        for (int u = 0; u < SL; ++u)
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                acc[u][k] = nw[u][k];
-    }
-    float v[4] = {acc[0][0], acc[0][1], acc[0][2], acc[0][3]};
-#pragma unroll
-    for (int off = GS / 2; off >= 1; off >>= 1)
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            v[k] = v[k] + __shfl_xor_sync(0xffffffffu, v[k], off);
-    return make_float4(v[0], v[1], v[2], v[3]);
-}
-
 // COST_INIT: priors of the parent's best slots (init_bp + copy_prior_plane,
 // hbp_isp.cu:56-73, :930-950); COST_STEP: candidates in slots 8-11.
 enum CostMode
@@ -599,49 +529,128 @@ enum CostMode
     COST_STEP = 1
 };
 
-template <int GS>
+// Data cost of 4 planes (read_plane_cost for every pixel, hbp_isp.cu:205-227,
+// and the per-node sum of compute_plane_cost, :1159-1174). One warp = one
+// 256-position window of the level's pixel list (sorted by node, raster order
+// inside a node), walked as 8 sub-windows of 32 positions, one per lane. The
+// node sum is taken in a fixed order (the reference's float atomics have
+// none; the CPU oracle restates it):
+//   S1 inside each 32-position sub-window the pixels of one node form a
+//      segment, summed by a segmented Hillis-Steele scan: for off = 1, 2, 4,
+//      8, 16, x[r] = x[r - off] + x[r] where r - off is still in the segment;
+//   S2 inside the 256-window the node's S1 pieces are added in order (a carry
+//      from one sub-window to the next);
+//   S3 the node's 256-window sums (its chunks, pc[]) are added in chunk order
+//      by the consumers (k_init_nodes, select_thread).
+__device__ __forceinline__ void emit_chunk(const LevelDev &l, float4 *pc, int n, int win, float4 v)
+{
+    pc[l.chunk_off[n] + win - l.pix_off[n] / PC_CHUNK] = v;
+}
+
 __global__ void __launch_bounds__(256) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
 {
+    const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    const int item = (blockIdx.x * blockDim.x + threadIdx.x) / GS;
-    const int r = lane % GS;
-    const bool valid = item < d.pre[d.nt];
-    int ti = valid ? find_task(d, item) : 0;
+    if (item >= d.pre[d.nt]) // warp-uniform
+        return;
+    const int ti = find_task(d, item);
     const Task &t = d.t[ti];
     const ViewDev &v = *t.vd;
     const LevelDev &l = *t.lvl;
-    int ch = valid ? item - d.pre[ti] : 0;
-    int n = valid ? l.chunk_node[ch] : 0;
-    float4 pl[4];
-    if (valid)
+    const Common c = v.c;
+    const int HW = c.W * c.H, N = l.N;
+    const int win = item - d.pre[ti];
+    float4 *pc = v.b.pc[t.pb];
+    const unsigned upto = 0xffffffffu >> (31 - lane); // lanes 0..lane
+    int carry_n = -1;
+    float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
+    int qn = win * PC_CHUNK + lane;
+    int n_nx = qn < HW ? l.pnode[qn] : N;
+    uint32_t xy_nx = qn < HW ? l.pix[qn] : 0u;
+    for (int k = 0; k < PC_CHUNK / 32; ++k)
     {
-        if (mode == COST_INIT)
+        const int q0 = win * PC_CHUNK + 32 * k;
+        if (q0 >= HW) // warp-uniform
+            break;
+        const int q = q0 + lane;
+        const int n = n_nx;
+        const uint32_t xy = xy_nx;
+        if (k + 1 < PC_CHUNK / 32)
         {
-            const LevelDev &h = *t.lvh;
-            int pn = l.clus[n];
+            qn = q + 32;
+            n_nx = qn < HW ? l.pnode[qn] : N;
+            xy_nx = qn < HW ? l.pix[qn] : 0u;
+        }
+        // segments: heads where the node changes (positions past HW form node N)
+        const int prev = __shfl_up_sync(0xffffffffu, n, 1);
+        const bool head = lane == 0 || prev != n;
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        const int seg = 31 - __clz(heads & upto);
+        const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+        // the node carried from the previous sub-window ends there unless it
+        // goes on at lane 0
+        const int n_first = __shfl_sync(0xffffffffu, n, 0);
+        if (lane == 0 && carry_n >= 0 && carry_n < N && carry_n != n_first)
+            emit_chunk(l, pc, carry_n, win, carry);
+        float cc[4] = {0.f, 0.f, 0.f, 0.f};
+        if (n < N)
+        {
+            float4 pl[4];
+            if (mode == COST_INIT)
+            {
+                const LevelDev &h = *t.lvh;
+                const int pn = l.clus[n];
 #pragma unroll
-            for (int p = 0; p < P; ++p)
-                pl[p] = h.plane[(size_t)pn * K + p];
-        }
-        else
-        {
+                for (int p = 0; p < P; ++p)
+                    pl[p] = h.plane[(size_t)pn * K + p];
+                if (head && q == l.pix_off[n])
+                {
+                    for (int kk = 0; kk < K; ++kk)
+                        l.plane[(size_t)n * K + kk] = pl[kk % P];
+                    v.b.s_nb[n] = (uint32_t)l.nb_off[n];
+                    v.b.s_ransac[t.rb][n] = (uint32_t)q;
+                }
+            }
+            else
+            {
 #pragma unroll
-            for (int p = 0; p < P; ++p)
-                pl[p] = l.plane[(size_t)n * K + 2 * P + p];
+                for (int p = 0; p < P; ++p)
+                    pl[p] = l.plane[(size_t)n * K + 2 * P + p];
+            }
+            const int x = px_x(xy), y = px_y(xy);
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+                cc[p] = pixel_cost(c, x, y, pl[p]);
         }
-    }
-    float4 cc = group_cost<GS>(l, v.c, n, ch, pl, r, valid);
-    if (valid && r == 0)
-    {
-        v.b.pc[t.pb][ch] = cc;
-        if (mode == COST_INIT && ch == l.chunk_off[n])
+        // S1
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+            {
+                const float u = __shfl_up_sync(0xffffffffu, cc[p], off);
+                if (lane - off >= seg)
+                    cc[p] = u + cc[p];
+            }
+        // S2
+        float4 val = make_float4(cc[0], cc[1], cc[2], cc[3]);
+        if (seg == 0 && n == carry_n)
         {
-            for (int k = 0; k < K; ++k)
-                l.plane[(size_t)n * K + k] = pl[k % P];
-            v.b.s_nb[n] = (uint32_t)l.nb_off[n];
-            v.b.s_ransac[t.rb][n] = (uint32_t)l.pix_off[n];
+            val.x = carry.x + val.x;
+            val.y = carry.y + val.y;
+            val.z = carry.z + val.z;
+            val.w = carry.w + val.w;
         }
+        if (tail && lane != 31 && n < N)
+            emit_chunk(l, pc, n, win, val);
+        carry.x = __shfl_sync(0xffffffffu, val.x, 31);
+        carry.y = __shfl_sync(0xffffffffu, val.y, 31);
+        carry.z = __shfl_sync(0xffffffffu, val.z, 31);
+        carry.w = __shfl_sync(0xffffffffu, val.w, 31);
+        carry_n = __shfl_sync(0xffffffffu, n, 31);
     }
+    if (lane == 0 && carry_n >= 0 && carry_n < N)
+        emit_chunk(l, pc, carry_n, win, carry);
 }
 
 // init_bp, continued: costs of the prior slots, belief = cost, child seeds.
@@ -743,17 +752,14 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
         pt[p] = l.plane[(size_t)st.y * K + p];
     // Each group's minimum over t's labels p of mp[p] + c0 * phi: c0 * phi is
     // >= 0 and float addition is monotone, so a label whose mp[p] is not
-    // below the running minimum cannot lower it. Labels are visited in
-    // increasing mp (NaN last) and the scan stops at the first such label;
-    // the minimum, hence the message, is the reference's.
-    int ordr[2 * P];
+    // below the running minimum cannot lower it. The labels of each group are
+    // sorted by mp (NaN last; the planes move with them) and the scan stops
+    // at the first such label; the minimum, hence the message, is the
+    // reference's.
     float key[2 * P];
 #pragma unroll
     for (int p = 0; p < 2 * P; ++p)
-    {
-        ordr[p] = p;
         key[p] = mp[p] == mp[p] ? mp[p] : INFINITY;
-    }
 #pragma unroll
     for (int g = 0; g < 2; ++g)
     {
@@ -764,9 +770,12 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
                 float tk = key[b + i];
                 key[b + i] = key[b + j];
                 key[b + j] = tk;
-                int to = ordr[b + i];
-                ordr[b + i] = ordr[b + j];
-                ordr[b + j] = to;
+                float tm = mp[b + i];
+                mp[b + i] = mp[b + j];
+                mp[b + j] = tm;
+                float4 tp = pt[b + i];
+                pt[b + i] = pt[b + j];
+                pt[b + j] = tp;
             }
         };
         cswap(0, 1);
@@ -775,12 +784,24 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
         cswap(1, 3);
         cswap(1, 2);
     }
-    float out[K];
+    // Lower bound of q = (phi / 3) / dist_pos from one multiply by rounded
+    // reciprocals: qa is within 4 ulp of q, so qa * (1 - 2^-20) <= q (tiny
+    // or NaN qa -> bound 0). Rounding is monotone, so with the bound qlb:
+    // qlb >= tau_smooth means min(q, tau_smooth) == tau_smooth exactly, and
+    // mp + c0 * qlb >= the running minimum means the label cannot lower it.
+    // Only the remaining labels need the exact divisions. Every label's phi
+    // is evaluated (uniform across the warp); a label skipped this way or
+    // with mp >= the minimum leaves the minimum unchanged, as does a NaN.
+    const float tau = c.tau_smooth;
+    const float inv_dp = 1.0f / dist_pos;
+    const float inv3 = 1.0f / 3.0f;
+    const float ct = c0 * tau;
+    __shared__ float s_out[K][128];
     float sum = 0.f;
-#pragma unroll
+#pragma unroll 1
     for (int y = 0; y < K; ++y)
     {
-        float4 ps = l.plane[(size_t)st.x * K + y];
+        const float4 ps = l.plane[(size_t)st.x * K + y];
         float acc = 0.f;
 #pragma unroll
         for (int g = 0; g < 2; ++g)
@@ -790,34 +811,33 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
             for (int k = 0; k < P; ++k)
             {
                 const int q = g * P + k;
-                if (k > 0 && key[q] >= mn)
-                    break;
-                const int p = ordr[q];
-                float4 tp = pt[0];
-#pragma unroll
-                for (int j = 1; j < 2 * P; ++j)
-                    if (j == p)
-                        tp = pt[j];
-                float mpp = mp[0];
-#pragma unroll
-                for (int j = 1; j < 2 * P; ++j)
-                    if (j == p)
-                        mpp = mp[j];
+                const float4 tp = pt[q];
                 float dx = ps.x - tp.x, dy = ps.y - tp.y, dz = ps.z - tp.z;
                 float phi = fabsf(dx * X[0] + dy * Y[0] + dz);
 #pragma unroll
                 for (int i = 1; i < 6; ++i)
                     phi = phi + fabsf(dx * X[i] + dy * Y[i] + dz);
-                phi = fminf(phi / 3.0f / dist_pos, c.tau_smooth);
-                float m = mpp + c0 * phi;
+                const float qa = phi * inv3 * inv_dp;
+                const float qlb = qa >= 1e-30f ? qa * 0.99999905f : 0.0f; // 1 - 2^-20
+                float m;
+                if (qlb >= tau)
+                    m = mp[q] + ct;
+                else if (k == 0 || mp[q] + c0 * qlb < mn)
+                    m = mp[q] + c0 * fminf(phi / 3.0f / dist_pos, tau);
+                else
+                    m = mn;
                 if (m < mn)
                     mn = m;
             }
             acc = acc + mn;
         }
-        out[y] = acc;
+        s_out[y][threadIdx.x] = acc;
         sum = sum + acc;
     }
+    float out[K];
+#pragma unroll
+    for (int y = 0; y < K; ++y)
+        out[y] = s_out[y][threadIdx.x];
     float mean = sum / (float)K;
     float4 *o = reinterpret_cast<float4 *>(v.b.msgt[t.mb] + (size_t)e * K);
     o[0] = make_float4(out[0] - mean, out[1] - mean, out[2] - mean, out[3] - mean);
@@ -893,7 +913,7 @@ ViewPlan::~ViewPlan() { delete impl; }
 // run_ms: setup_D4, reverse_bd_id, compute_dist_color_pos, sort_clus;
 // hbp_isp.cu:871-891, :952-1019), the BP buffers, and the view descriptor.
 // Persistent data go to `persist`, sort/scan temporaries to `tmp`.
-void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wta, int D,
+void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D,
                  const HbpParams &prm, float *disp, float *plane_out, Arena &persist, Arena &tmp,
                  cudaStream_t st, ViewPlan &vp)
 {
@@ -904,7 +924,7 @@ void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wt
     if ((int)pyr.N.size() != L || (int)pyr.E.size() != L || (int)pyr.node_off.size() != L ||
         (int)pyr.edge_off.size() != L || (int)pyr.child_base.size() != L || (int)pyr.nb_base.size() != L)
         throw StatusError{HBP_ERR_INTERNAL, "pyramid bookkeeping inconsistent"};
-    Common c{W, H, D, Dp, prm.alpha, CENSUS_TAU, prm.tau_smooth, vol, wta};
+    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, CENSUS_TAU, prm.tau_smooth, vol, wta};
     std::vector<LevelDev> &lv = vp.impl->lv;
     lv.assign(L, LevelDev{});
     vp.L = L;
@@ -959,9 +979,8 @@ void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wt
             exclusive_scan(cnt, chunk_off, N + 1, nch_total, tmp, st);
             d.nchunks = read_dev_int(nch_total, st);
             vp.levelC[l] = d.nchunks;
-            int *chunk_node = persist.alloc<int>(d.nchunks);
-            chunk_fill<<<blocks(N, 256), 256, 0, st>>>(chunk_off, N, chunk_node);
-            note_launch();
+            int *pnode = persist.alloc<int>(HW); // the sorted keys
+            HBP_CUDA(cudaMemcpyAsync(pnode, kt, sizeof(int) * HW, cudaMemcpyDeviceToDevice, st));
             HBP_LAUNCH_CHECK();
             int *rev = persist.alloc<int>(E);
             reverse_ids<<<blocks(E, 256), 256, 0, st>>>(d.bd, d.nb_off, E, rev);
@@ -976,7 +995,7 @@ void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, int Dp, const float *wt
             d.pix = pix;
             d.pix_off = pix_off;
             d.chunk_off = chunk_off;
-            d.chunk_node = chunk_node;
+            d.pnode = pnode;
             d.rev = rev;
             d.dc = dc;
             d.mx = mx;
@@ -1032,28 +1051,9 @@ struct TaskState
     float max_dz = 0, max_dn = 0;
 };
 
-int pick_group(double avg_chunk_px)
-{
-    if (avg_chunk_px > 96)
-        return 32;
-    if (avg_chunk_px > 48)
-        return 16;
-    if (avg_chunk_px > 16)
-        return 8;
-    return 4;
-}
-
 void launch_cost(const ViewDev *V, const StepDesc &d, int mode, cudaStream_t st)
 {
-    long threads = (long)d.pre[d.nt] * d.gs;
-    int nb = blocks(threads, 256);
-    switch (d.gs)
-    {
-    case 4: k_cost<4><<<nb, 256, 0, st>>>(V, d, mode); break;
-    case 8: k_cost<8><<<nb, 256, 0, st>>>(V, d, mode); break;
-    case 16: k_cost<16><<<nb, 256, 0, st>>>(V, d, mode); break;
-    default: k_cost<32><<<nb, 256, 0, st>>>(V, d, mode); break;
-    }
+    k_cost<<<blocks((long)d.pre[d.nt] * 32, 256), 256, 0, st>>>(V, d, mode);
     note_launch();
 }
 } // namespace
@@ -1087,16 +1087,16 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
     long prof_step = 0;
 
     auto desc = [&](const std::vector<TaskState *> &ts, int what, bool first) {
-        // what: 0 nodes, 1 chunks, 2 edges, 3 parents, 4 max(nodes, parents)
+        // what: 0 nodes, 1 256-windows of the pixel list, 2 edges, 3 parents,
+        // 4 max(nodes, parents)
         StepDesc d{};
         d.nt = (int)ts.size();
         d.pre[0] = 0;
-        double px = 0, chs = 0;
         for (int k = 0; k < d.nt; ++k)
         {
             const TaskState &s = *ts[k];
             const ViewPlan &vp = *views[s.v];
-            int n = vp.levelN[s.li], e = vp.levelE[s.li], ch = vp.levelC[s.li];
+            int n = vp.levelN[s.li], e = vp.levelE[s.li], ch = (vp.HW + PC_CHUNK - 1) / PC_CHUNK;
             int nh = s.li + 1 < vp.L ? vp.levelN[s.li + 1] : 1;
             int cnt = what == 0 ? n : what == 1 ? ch : what == 2 ? e : what == 3 ? nh : std::max(n, nh);
             d.pre[k + 1] = d.pre[k] + cnt;
@@ -1112,10 +1112,7 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
             t.mb = s.step & 1;
             t.max_dz = s.max_dz;
             t.max_dn = s.max_dn;
-            px += vp.HW;
-            chs += ch;
         }
-        d.gs = pick_group(chs > 0 ? px / chs : 256);
         return d;
     };
     auto timed = [&](bool on, auto &&f) {
@@ -1124,6 +1121,29 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
         f();
         if (on)
             prof->mark(st);
+    };
+    // breakdown profiling: kinds 0 node, 1 child, 2 neighbor, 3 set_cand,
+    // 4 cost step, 5 edges, 6 cost init, 7 init_nodes, 8 map
+    KernelProf *bprof = prof && prof->breakdown ? prof : nullptr;
+    long substep = 0;
+    bool sample = false;
+    auto run = [&](int kind, int li, auto &&f) {
+        if (!bprof)
+        {
+            f();
+            return;
+        }
+        const int tag = kind * KernelProf::LEVELS + std::min(li, KernelProf::LEVELS - 1);
+        bprof->count[tag]++;
+        if (sample)
+        {
+            bprof->markb(st);
+            f();
+            bprof->markb(st);
+            bprof->tagb.push_back(tag);
+        }
+        else
+            f();
     };
 
     std::vector<TaskState> state(nv);
@@ -1149,14 +1169,15 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
         // init_bp: priors and their data cost (partials in pc[0]), then costs,
         // beliefs and seeds per node
         {
+            sample = true;
             StepDesc d = desc(act, 1, true);
             for (int k = 0; k < d.nt; ++k)
                 d.t[k].pb = 0;
-            launch_cost(V, d, COST_INIT, st);
+            run(6, li, [&] { launch_cost(V, d, COST_INIT, st); });
             StepDesc dn = desc(act, 4, true);
             for (int k = 0; k < dn.nt; ++k)
                 dn.t[k].pb = 0;
-            k_init_nodes<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+            run(7, li, [&] { k_init_nodes<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
             note_launch();
             HBP_LAUNCH_CHECK();
         }
@@ -1188,24 +1209,25 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
                 }
                 const bool first = ts[0]->step == 0; // all tasks start a level together
                 const bool tp = prof && (prof_step++ % 16 == 0);
+                sample = substep++ % 8 == 0;
                 StepDesc dn = desc(ts, 0, first);
                 dn.mode = kind == 0 ? NODE_SELECT_RANSAC : kind == 2 ? NODE_SELECT_RANDOM : NODE_SELECT;
-                k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+                run(0, li, [&] { k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
                 note_launch();
                 if (kind == 1)
                 {
                     StepDesc dp = desc(ts, 3, first);
-                    k_child<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp);
+                    run(1, li, [&] { k_child<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp); });
                     note_launch();
-                    k_neighbor<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp);
+                    run(2, li, [&] { k_neighbor<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp); });
                     note_launch();
-                    k_set_cand<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+                    run(3, li, [&] { k_set_cand<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
                     note_launch();
                 }
                 StepDesc dc = desc(ts, 1, first);
-                timed(tp, [&] { launch_cost(V, dc, COST_STEP, st); });
+                run(4, li, [&] { timed(tp, [&] { launch_cost(V, dc, COST_STEP, st); }); });
                 StepDesc de = desc(ts, 2, first);
-                k_edges<<<blocks(de.pre[de.nt], 128), 128, 0, st>>>(V, de);
+                run(5, li, [&] { k_edges<<<blocks(de.pre[de.nt], 128), 128, 0, st>>>(V, de); });
                 note_launch();
                 HBP_LAUNCH_CHECK();
                 if (tp)
@@ -1236,7 +1258,8 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
         // final select of the level
         StepDesc dn = desc(act, 0, false);
         dn.mode = NODE_SELECT;
-        k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn);
+        sample = true;
+        run(0, li, [&] { k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
         note_launch();
         HBP_LAUNCH_CHECK();
     }
@@ -1251,7 +1274,8 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
             all.push_back(&state[i]);
         }
         StepDesc d = desc(all, 0, false);
-        k_map<<<blocks((long)d.pre[d.nt] * 32, 128), 128, 0, st>>>(V, d);
+        sample = true;
+        run(8, m, [&] { k_map<<<blocks((long)d.pre[d.nt] * 32, 128), 128, 0, st>>>(V, d); });
         note_launch();
         HBP_LAUNCH_CHECK();
     }

@@ -83,9 +83,19 @@ def default_params(**kw) -> Params:
     return p
 
 
-def volume_pitch(D: int) -> int:
-    """Bytes per pixel of the pixel-major cost volume."""
-    return lib().hbp_volume_pitch(D)
+def volume_bytes(W: int, H: int, D: int) -> int:
+    """Size of the tiled cost volume (see hbp_volume_bytes in the header)."""
+    f = lib().hbp_volume_bytes
+    f.restype = C.c_size_t
+    return f(W, H, D)
+
+
+def volume_to_dhw(buf: np.ndarray, W: int, H: int, D: int) -> np.ndarray:
+    """Tiled volume bytes -> [D][H*W] (the reference's disparity-major order)."""
+    TX, TY = (W + 7) // 8, (H + 3) // 4
+    v = np.asarray(buf, np.uint8)[: TX * TY * D * 32].reshape(TY, TX, D, 4, 8)
+    v = v.transpose(2, 0, 3, 1, 4).reshape(D, TY * 4, TX * 8)[:, :H, :W]
+    return np.ascontiguousarray(v.reshape(D, H * W))
 
 
 NOALLOC_MAX_PIXELS = 2097152  # HBP_NOALLOC_MAX_PIXELS of the header

@@ -70,12 +70,16 @@ void *hbp_ctx_stream(hbp_ctx *ctx);
 
 /* StereoCost::compute_stereo_cost("Census") (stereo_cost.cu:421-445) with the
  * grey conversion of the constructor (stereo_cost.cu:290-297): census of both
- * views, pixel-major uint8 cost volume vol[y][x][d] with hbp_volume_pitch(D)
- * bytes per pixel (entries d >= D are 0) holding min(popcount, 25), and the
- * WTA disparity. With volR/wtaR non-NULL the right-view volume and WTA of
+ * views, the uint8 cost volume holding min(popcount, 25), and the WTA
+ * disparity. With volR/wtaR non-NULL the right-view volume and WTA of
  * StereoCost::cost_to_right (stereo_cost.cu:488-516) are produced in the same
- * pass. */
-int hbp_volume_pitch(int D);
+ * pass.
+ * Volume layout (hbp_volume_bytes(W, H, D) bytes): 8 x 4-pixel tiles in
+ * raster order, TX = ceil(W/8) tiles per row; inside a tile disparity-major
+ * with 32 bytes per disparity. Cost(x, y, d) is at byte
+ *   ((y/4 * TX + x/8) * D + d) * 32 + (y%4) * 8 + x%8;
+ * overhanging tile entries are 0. */
+size_t hbp_volume_bytes(int W, int H, int D);
 hbp_status hbp_cost_census_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H,
                              int D, uint32_t *censusL, uint32_t *censusR, uint8_t *vol,
                              float *wta, uint8_t *volR, float *wtaR, void *stream);
@@ -177,6 +181,12 @@ hbp_status hbp_last_phase_ms(hbp_ctx *ctx, double *out4);
  * algorithmic bytes of the timed launches. Enabling resets the totals. */
 hbp_status hbp_profile_enable(hbp_ctx *ctx, int on);
 hbp_status hbp_profile_read(hbp_ctx *ctx, double *ms, long *launches, double *bytes);
+/* Mode 3 additionally times every BP kernel of every 8th BP step. Breakdown
+ * fills three arrays of 10 x 32 entries indexed [kind][level] (kinds: 0 node
+ * select, 1 child candidates, 2 neighbour candidates, 3 set candidates,
+ * 4 data cost, 5 edge messages, 6 prior data cost, 7 init nodes, 8 MAP):
+ * summed device ms and count of the timed launches, and count of all launches. */
+hbp_status hbp_profile_breakdown(hbp_ctx *ctx, double *ms, long *timed, long *all);
 
 #ifdef __cplusplus
 }

@@ -59,20 +59,23 @@ inline float fmax_cuda(float a, float b) { return std::fmax(a, b); }
 // v[0..n) are laid out round-robin over 32 slots (slot j accumulates v[j],
 // v[j+32], ... sequentially from 0), then the slots are combined by an xor
 // butterfly with offsets 16, 8, 4, 2, 1 (slot i += slot i^off).
+// Last element of the Hillis-Steele inclusive scan of x[0..m) (m <= 32):
+// for off = 1, 2, 4, 8, 16: x[r] = x[r - off] + x[r] for r >= off.
 template <typename R>
-inline R butterfly32(const R *slots)
+inline R scan_last(const R *x0, int m)
 {
     R a[32];
-    for (int i = 0; i < 32; ++i)
-        a[i] = slots[i];
-    for (int off = 16; off >= 1; off >>= 1)
+    for (int i = 0; i < m; ++i)
+        a[i] = x0[i];
+    for (int off = 1; off < 32; off <<= 1)
     {
         R b[32];
-        for (int i = 0; i < 32; ++i)
-            b[i] = a[i] + a[i ^ off];
-        std::memcpy(a, b, sizeof(a));
+        for (int r = 0; r < m; ++r)
+            b[r] = r >= off ? a[r - off] + a[r] : a[r];
+        std::memcpy(a, b, sizeof(R) * m);
     }
-    return a[0];
+    return a[m - 1];
 }
+
 
 } // namespace orc

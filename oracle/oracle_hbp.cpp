@@ -8,10 +8,13 @@
 //
 // Reduction orders fixed by the engine (the reference uses float atomics and
 // Thrust reduce_by_key, whose order is unspecified):
-//   plane cost of node n, candidate k: the node's pixels in raster order are
-//   cut into chunks of 256; inside a chunk pixel j+32*s goes to slot j
-//   (slots accumulate sequentially from 0), the 32 slots are combined by the
-//   xor butterfly of orc::butterfly32; chunk sums are added in chunk order.
+//   plane cost of node n, candidate k, over the level's pixel list (sorted by
+//   node, raster order inside a node; list positions are absolute):
+//   S1 the node's positions inside one 32-position window are summed by a
+//      Hillis-Steele inclusive scan (off = 1..16: x[r] = x[r-off] + x[r] for
+//      r >= off), taking its last element;
+//   S2 the S1 pieces inside one 256-position window are added in order;
+//   S3 the 256-window sums are added in order.
 //   belief[k][s] = cost[k][s] + msg_t of s's out-edges in edge order.
 //   dc colour term: (|dL| + |da|) + |db|; position term: dx*dx + dy*dy.
 #include <algorithm>
@@ -102,19 +105,22 @@ struct Engine
             for (int p = 0; p < P; ++p)
             {
                 const P4<R> pl = l.plane[(size_t)(s_c + p) * l.N + n];
+                const int e = b + m;
                 R total = 0;
-                for (int c0 = 0; c0 < m; c0 += CHUNK)
+                for (int w256 = b / CHUNK; w256 <= (e - 1) / CHUNK; ++w256)
                 {
-                    R slots[32];
-                    for (int j = 0; j < 32; ++j)
+                    const int lo = std::max(b, w256 * CHUNK), hi = std::min(e, (w256 + 1) * CHUNK);
+                    R acc = 0;
+                    for (int w32 = lo / 32; w32 <= (hi - 1) / 32; ++w32)
                     {
-                        R acc = 0;
-                        for (int k = c0 + j; k < std::min(m, c0 + CHUNK); k += 32)
-                            acc += pixel_cost(l.pix[b + k], pl);
-                        slots[j] = acc;
+                        const int l2 = std::max(lo, w32 * 32), h2 = std::min(hi, (w32 + 1) * 32);
+                        R x[32];
+                        for (int q = l2; q < h2; ++q)
+                            x[q - l2] = pixel_cost(l.pix[q], pl);
+                        const R piece = scan_last(x, h2 - l2);
+                        acc = w32 == lo / 32 ? piece : acc + piece;
                     }
-                    R cs = butterfly32(slots);
-                    total = c0 == 0 ? cs : total + cs;
+                    total = w256 == b / CHUNK ? acc : total + acc;
                 }
                 l.cost[(size_t)(s_c + p) * l.N + n] = total;
             }

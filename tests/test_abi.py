@@ -26,7 +26,8 @@ def test_host_only_entry_points(lib):
     p = E.default_params()
     assert abs(p.alpha - 1000.1) < 1e-3 and abs(p.tau_smooth - 0.6) < 1e-6 and p.min_level == 2
     assert L.hbp_status_string(0) == b"ok" and L.hbp_status_string(5) == b"CUDA error"
-    assert E.volume_pitch(128) == 128 and E.volume_pitch(60) == 64
+    assert E.volume_bytes(720, 496, 128) == 720 * 496 * 128
+    assert E.volume_bytes(17, 5, 3) == 3 * 2 * 3 * 32  # overhanging tiles are stored whole
     h = C.c_void_p()
     assert L.hbp_ctx_create(0, -5, 0, C.byref(h)) != 0  # bad arguments rejected
     ph = (C.c_double * 4)()

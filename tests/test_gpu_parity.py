@@ -36,18 +36,23 @@ def dev(torch, a):
 
 def run_cost(E, ctx, torch, L, R, D, right=False):
     H, W = L.shape[:2]
-    Dp = E.volume_pitch(D)
     dL, dR = dev(torch, L), dev(torch, R)
     cL = torch.zeros(H * W, dtype=torch.int32, device="cuda")
     cR = torch.zeros_like(cL)
-    vol = torch.zeros(H * W * Dp, dtype=torch.uint8, device="cuda")
+    # filled with 0xAB: every byte, overhanging tile entries included, must be written
+    vol = torch.full((E.volume_bytes(W, H, D),), 0xAB, dtype=torch.uint8, device="cuda")
     wta = torch.zeros(H * W, dtype=torch.float32, device="cuda")
-    volR = torch.zeros_like(vol) if right else None
+    volR = torch.full_like(vol, 0xAB) if right else None
     wtaR = torch.zeros_like(wta) if right else None
     ctx.cost_census_d(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR)
     torch.cuda.synchronize()
-    # engine layout [y][x][Dp] -> oracle layout [d][y*W+x]
-    strip = lambda v: np.ascontiguousarray(v.cpu().numpy().reshape(H * W, Dp)[:, :D].T)
+
+    def strip(v):  # engine's tiled layout -> oracle layout [d][y*W+x]
+        b = v.cpu().numpy()
+        full = E.volume_to_dhw(b, W, H, D)
+        assert int(b.astype(np.int64).sum()) == int(full.astype(np.int64).sum()), "overhang not zero"
+        return full
+
     out = dict(censusL=cL.cpu().numpy().view(np.uint32).reshape(H, W),
                censusR=cR.cpu().numpy().view(np.uint32).reshape(H, W),
                vol=strip(vol), wta=wta.cpu().numpy().reshape(H, W), vol_dev=vol, wta_dev=wta)
