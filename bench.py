@@ -145,6 +145,28 @@ def cpu_baseline(scene, W, H, D):
                       f"OpenMP on {cores} threads, {dt:.1f} s"}
 
 
+# DRAM bytes (read + write) per list position of one k_cost launch, from the
+# committed ncu capture of a 4-view 720x496 D128 launch: 21,599,232 B over
+# 4 x 357,120 positions.
+KCOST_DRAM_BYTES_PER_PIXEL = 21599232 / (4 * 357120)
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's duration (every rank gets it); x itself without a
+    process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(pairs_per_rank: int, steps: int, world: int, seconds: float) -> float:
+    """pairs/s of the whole job: every rank's pairs over the slowest rank's time."""
+    return pairs_per_rank * steps * world / seconds
+
+
 KINDS = ["node_select", "child_cand", "neighbor_cand", "set_cand", "data_cost", "edge_msgs",
          "prior_cost", "init_nodes", "map"]
 
@@ -284,13 +306,8 @@ def main():
     pms, plaunch, pbytes = C.c_double(), C.c_long(), C.c_double()
     E._check(E.lib().hbp_profile_read(ctx.h, C.byref(pms), C.byref(plaunch), C.byref(pbytes)))
     E._check(E.lib().hbp_profile_enable(ctx.h, 0))
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    total_pairs = NP * args.steps * world
-    value = total_pairs / (t_max / 1e3)
+    t_max = max_over_ranks(ms, dist, "cuda")
+    value = whole_job_rate(NP, args.steps, world, t_max / 1e3)
 
     if args.breakdown and rank == 0:
         print(json.dumps(breakdown(E, ctx, step)), file=sys.stderr)
@@ -315,11 +332,8 @@ def main():
                 lat.append((time.perf_counter() - a) * 1e3)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": NP * args.steps * world / el, "unit": "pairs/s",
+        el = max_over_ranks(el, dist, "cuda")
+        e2e = {"value": whole_job_rate(NP, args.steps, world, el), "unit": "pairs/s",
                "h2d_bytes_per_step": NP * 2 * 3 * W * H, "d2h_bytes_per_step": NP * 4 * W * H}
 
     cpu = None
@@ -353,7 +367,11 @@ def main():
             "roofline": {"kernel": "plane_cost_kernel (data cost of 4 candidate planes per pixel)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": None, "launches_timed": plaunch.value,
+                         "traffic": KCOST_DRAM_BYTES_PER_PIXEL * NP * W * H,
+                         "traffic_source": "ncu dram__bytes_read+write of one k_cost launch over 4 views "
+                                           "(profiles/k_cost_level5_4x720x496_d128.md), per list position, "
+                                           "times the positions of one 16-view launch",
+                         "launches_timed": plaunch.value,
                          "avg_launch_us": 1e3 * pms.value / max(1, plaunch.value)},
             "cpu_baseline": cpu,
             "clocks": clk,

@@ -26,6 +26,8 @@
 #include <cstdio>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "engine.h"
 
 namespace hbp
@@ -217,7 +219,8 @@ __device__ __forceinline__ float4 fit_plane(float Ax, float Ay, float Az, float 
 //                the kept slots of e's target).
 struct ViewBufs
 {
-    float *msgt[2]; // [E][K] ping-pong
+    void *msgt[2]; // [E][K] ping-pong: float, or __half when fp16
+    int fp16;      // messages stored as FP16 (FP32 arithmetic)
     float4 *pc[2];  // chunk partial costs ping-pong
     uint32_t *s_child, *s_nb, *s_ransac[2];
     float4 *buf; // [Nmax][P] spatial candidates
@@ -270,7 +273,64 @@ __device__ __forceinline__ int find_task(const StepDesc &d, int item)
 // hbp_isp.cu:405-417, :432-472): belief = cost + out-edge messages in edge
 // order; a slot's rank counts the slots that beat it (a later slot loses
 // ties); slots ranked < P move to the front in slot order, in place.
-__device__ __forceinline__ void select_thread(const LevelDev &l, int n, const float4 *pc, const float *msgt)
+// msg_t[e][0..11] of buffer `buf` as floats. FP16 storage holds each value
+// rounded to nearest; the arithmetic on messages is FP32 either way.
+__device__ __forceinline__ void load_msg(const ViewBufs &b, int buf, size_t e, float v[K])
+{
+    if (b.fp16)
+    {
+        const uint2 *h = reinterpret_cast<const uint2 *>(static_cast<const __half *>(b.msgt[buf]) + e * K);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+        {
+            const uint2 w = h[i];
+            const float2 lo = __half22float2(*reinterpret_cast<const __half2 *>(&w.x));
+            const float2 hi = __half22float2(*reinterpret_cast<const __half2 *>(&w.y));
+            v[4 * i] = lo.x;
+            v[4 * i + 1] = lo.y;
+            v[4 * i + 2] = hi.x;
+            v[4 * i + 3] = hi.y;
+        }
+    }
+    else
+    {
+        const float4 *m4 = reinterpret_cast<const float4 *>(static_cast<const float *>(b.msgt[buf]) + e * K);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+        {
+            const float4 m = m4[i];
+            v[4 * i] = m.x;
+            v[4 * i + 1] = m.y;
+            v[4 * i + 2] = m.z;
+            v[4 * i + 3] = m.w;
+        }
+    }
+}
+
+__device__ __forceinline__ void store_msg(const ViewBufs &b, int buf, size_t e, const float v[K])
+{
+    if (b.fp16)
+    {
+        uint2 *h = reinterpret_cast<uint2 *>(static_cast<__half *>(b.msgt[buf]) + e * K);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+        {
+            __half2 lo = __floats2half2_rn(v[4 * i], v[4 * i + 1]);
+            __half2 hi = __floats2half2_rn(v[4 * i + 2], v[4 * i + 3]);
+            h[i] = make_uint2(*reinterpret_cast<uint32_t *>(&lo), *reinterpret_cast<uint32_t *>(&hi));
+        }
+    }
+    else
+    {
+        float4 *o = reinterpret_cast<float4 *>(static_cast<float *>(b.msgt[buf]) + e * K);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    }
+}
+
+__device__ __forceinline__ void select_thread(const LevelDev &l, int n, const float4 *pc, const ViewBufs &vb,
+                                              int mbuf)
 {
     float cs[K], b[K];
     float *cst = l.cost + (size_t)n * K;
@@ -298,20 +358,11 @@ __device__ __forceinline__ void select_thread(const LevelDev &l, int n, const fl
         b[k] = cs[k];
     for (int e = l.nb_off[n]; e < l.nb_off[n + 1]; ++e)
     {
-        const float4 *m4 = reinterpret_cast<const float4 *>(msgt + (size_t)e * K);
-        float4 m0 = m4[0], m1 = m4[1], m2 = m4[2];
-        b[0] = b[0] + m0.x;
-        b[1] = b[1] + m0.y;
-        b[2] = b[2] + m0.z;
-        b[3] = b[3] + m0.w;
-        b[4] = b[4] + m1.x;
-        b[5] = b[5] + m1.y;
-        b[6] = b[6] + m1.z;
-        b[7] = b[7] + m1.w;
-        b[8] = b[8] + m2.x;
-        b[9] = b[9] + m2.y;
-        b[10] = b[10] + m2.z;
-        b[11] = b[11] + m2.w;
+        float m[K];
+        load_msg(vb, mbuf, (size_t)e, m);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            b[k] = b[k] + m[k];
     }
     int ord[K];
 #pragma unroll
@@ -444,7 +495,7 @@ __global__ void __launch_bounds__(128) k_node(const ViewDev *__restrict__ V, Ste
     const LevelDev &l = *t.lvl;
     const int n = item - d.pre[find_task(d, item)];
     if (!t.first)
-        select_thread(l, n, v.b.pc[t.pb ^ 1], v.b.msgt[t.mb ^ 1]);
+        select_thread(l, n, v.b.pc[t.pb ^ 1], v.b, t.mb ^ 1);
     if (d.mode == NODE_SELECT_RANSAC)
         ransac_thread(l, v.c, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n]);
     else if (d.mode == NODE_SELECT_RANDOM)
@@ -729,11 +780,8 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
     {
         unsigned long long kl = l.keep[st.y];
         int cnt = (int)(kl & 15ull);
-        const float *src = v.b.msgt[t.mb ^ 1] + (size_t)l.rev[e] * K;
         float vv[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            vv[k] = src[k];
+        load_msg(v.b, t.mb ^ 1, (size_t)l.rev[e], vv);
 #pragma unroll
         for (int p = 0; p < 2 * P; ++p)
         {
@@ -838,11 +886,25 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
 #pragma unroll
     for (int y = 0; y < K; ++y)
         out[y] = s_out[y][threadIdx.x];
-    float mean = sum / (float)K;
-    float4 *o = reinterpret_cast<float4 *>(v.b.msgt[t.mb] + (size_t)e * K);
-    o[0] = make_float4(out[0] - mean, out[1] - mean, out[2] - mean, out[3] - mean);
-    o[1] = make_float4(out[4] - mean, out[5] - mean, out[6] - mean, out[7] - mean);
-    o[2] = make_float4(out[8] - mean, out[9] - mean, out[10] - mean, out[11] - mean);
+    // normalise: the reference subtracts the mean (normalize_msg_k); FP16
+    // storage subtracts the message's minimum instead, so the stored values
+    // start at 0 and keep FP16's relative precision (the beliefs of a node
+    // shift by a per-message constant, which leaves their order unchanged)
+    float norm;
+    if (v.b.fp16)
+    {
+        norm = out[0];
+#pragma unroll
+        for (int k = 1; k < K; ++k)
+            if (out[k] < norm)
+                norm = out[k];
+    }
+    else
+        norm = sum / (float)K;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        out[k] = out[k] - norm;
+    store_msg(v.b, t.mb, (size_t)e, out);
 }
 
 // map_msg (hbp_isp.cu:783-841), one warp per node of the finest level
@@ -1024,13 +1086,15 @@ void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D
     }
     ViewDev &vd = vp.impl->vd;
     vd.c = c;
+    vd.b.fp16 = prm.msg_fp16 ? 1 : 0;
     vd.L = L;
     LevelDev *lv_dev = persist.alloc<LevelDev>(L);
     HBP_CUDA(cudaMemcpyAsync(lv_dev, lv.data(), sizeof(LevelDev) * L, cudaMemcpyHostToDevice, st));
     vd.lv = lv_dev;
     for (int k = 0; k < 2; ++k)
     {
-        vd.b.msgt[k] = persist.alloc<float>((size_t)Emax * K);
+        vd.b.msgt[k] = prm.msg_fp16 ? (void *)persist.alloc<__half>((size_t)Emax * K)
+                                    : (void *)persist.alloc<float>((size_t)Emax * K);
         vd.b.pc[k] = persist.alloc<float4>(CHmax);
         vd.b.s_ransac[k] = persist.alloc<uint32_t>(Nmax);
     }

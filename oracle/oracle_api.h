@@ -23,9 +23,10 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
                 float *mean, int *bd, int *bdl);
 
 // belief propagation (oracle_hbp.cpp)
+void orc_round_fp16(const float *in, float *out, long n);
 int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
             const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
-            float alpha, float tau_smooth, int min_level, int fp64, long max_steps, float *disp,
+            float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
             float *plane, float *state_belief, float *state_plane);
 
 // post-processing (oracle_post.cpp)

@@ -71,6 +71,7 @@ struct Engine
     std::vector<P4<R>> plane_buf;
     long steps = 0, max_steps = -1;
     bool stopped = false;
+    bool fp16_msg = false; // messages stored as FP16 (float mode only)
 
     R pixel_cost(int px, const P4<R> &pl) const
     {
@@ -314,12 +315,25 @@ struct Engine
                 acc += mn;
                 out[y] = acc;
             }
-            R mean = 0;
-            for (int k = 0; k < K; ++k)
-                mean += out[k];
-            mean /= (R)K;
-            for (int k = 0; k < K; ++k)
-                msg_t[(size_t)k * E + e] = out[k] - mean;
+            if (fp16_msg)
+            {
+                // FP16 storage: minus the message's minimum, rounded to FP16
+                R mn = out[0];
+                for (int k = 1; k < K; ++k)
+                    if (out[k] < mn)
+                        mn = out[k];
+                for (int k = 0; k < K; ++k)
+                    msg_t[(size_t)k * E + e] = (R)(float)(_Float16)(float)(out[k] - mn);
+            }
+            else
+            {
+                R mean = 0;
+                for (int k = 0; k < K; ++k)
+                    mean += out[k];
+                mean /= (R)K;
+                for (int k = 0; k < K; ++k)
+                    msg_t[(size_t)k * E + e] = out[k] - mean;
+            }
         }
         // aggregate_belief: belief = cost + out-edge messages in edge order
         for (int n = 0; n < N; ++n)
@@ -533,7 +547,7 @@ template <typename R>
 int run(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
         const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
         float tau_smooth, int min_level, long max_steps, float *disp, float *plane_out,
-        float *state_belief, float *state_plane)
+        float *state_belief, float *state_plane, bool fp16_msg = false)
 {
     if (L < 1 || min_level < 0 || min_level > L - 1)
         return -1;
@@ -548,6 +562,7 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
     eng.vol = vol;
     eng.wta = wta;
     eng.max_steps = max_steps;
+    eng.fp16_msg = fp16_msg;
     eng.setup(level_sizes, clus, mean, bd, bdl);
     // top level: messages and beliefs zero, planes zero (never written by the
     // reference, hbp_isp.cu:1333-1337)
@@ -612,19 +627,32 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
 
 extern "C" {
 
+// Each value rounded to FP16 (nearest, ties to even) and back, as the FP16
+// message store does; exposed so the tests can pin it against numpy.
+void orc_round_fp16(const float *in, float *out, long n)
+{
+    for (long i = 0; i < n; ++i)
+        out[i] = (float)(_Float16)in[i];
+}
+
 // HBP_ISP(ISPData, StereoData, alpha, tau_smooth).run_ms(min_level)
 // (hbp_isp.hpp:288-386, hbp_isp.cu:1313-1346) on a segmentation pyramid in
 // the ISP layout of orc_segment, the u8 disparity-major cost volume and the
-// WTA disparity. fp64 != 0 selects the FP64 oracle. max_steps >= 0 stops after
+// WTA disparity. mode 0: float, the engine's arithmetic; 1: the FP64 oracle;
+// 2: float with messages stored as FP16 after subtracting each message's
+// minimum (the engine's msg_fp16 path). max_steps >= 0 stops after
 // that many candidate/BP steps and reports the current level's beliefs and
 // planes (K x N, plane as 4 floats) in state_*; otherwise those are filled
 // for min_level. Returns the number of BP steps run, or < 0 on bad input.
 int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
             const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
-            float alpha, float tau_smooth, int min_level, int fp64, long max_steps, float *disp,
+            float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
             float *plane, float *state_belief, float *state_plane)
 {
-    if (fp64)
+    if (mode == 2)
+        return run<float>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth,
+                          min_level, max_steps, disp, plane, state_belief, state_plane, true);
+    if (mode == 1)
         return run<double>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha,
                            tau_smooth, min_level, max_steps, disp, plane, state_belief,
                            state_plane);

@@ -125,9 +125,19 @@ def segment(lab4: np.ndarray) -> dict:
     return dict(level_sizes=sizes, clus=clus[:tc], mean=mean[: 6 * tc], bd=bd[: 2 * tb].reshape(tb, 2), bdl=bdl[:tb])
 
 
+def round_fp16(x: np.ndarray) -> np.ndarray:
+    """The oracle's FP16 store: nearest FP16 value, back to float32."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_round_fp16(_p(x), _p(out), C.c_long(x.size))
+    return out
+
+
 def hbp(seg: dict, vol, wta, W, H, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False,
-        max_steps=-1):
-    """Returns (disparity HxW, plane HxWx3, steps, belief KxN, plane KxNx4)."""
+        max_steps=-1, fp16_msg=False):
+    """Returns (disparity HxW, plane HxWx3, steps, belief KxN, plane KxNx4).
+    fp64 selects the FP64 oracle; fp16_msg the float path with FP16 message
+    storage (min-normalised), as the engine's msg_fp16."""
     sizes = np.ascontiguousarray(seg["level_sizes"], np.int32)
     L = sizes.shape[0]
     disp = np.zeros((H, W), np.float32)
@@ -140,7 +150,7 @@ def hbp(seg: dict, vol, wta, W, H, D, alpha=1000.1, tau_smooth=0.6, min_level=2,
                           _p(np.ascontiguousarray(seg["bd"], np.int32)),
                           _p(np.ascontiguousarray(seg["bdl"], np.int32)),
                           _p(np.ascontiguousarray(vol, np.uint8)), _p(np.ascontiguousarray(wta, np.float32)),
-                          W, H, D, alpha, tau_smooth, min_level, int(fp64), int(max_steps), _p(disp),
+                          W, H, D, alpha, tau_smooth, min_level, 2 if fp16_msg else int(fp64), int(max_steps), _p(disp),
                           _p(plane), _p(sb), _p(sp))
     if steps < 0:
         raise ValueError("oracle hbp rejected its input")
@@ -186,7 +196,8 @@ def cost_stage(L, R, D):
     return dict(greyL=gL, greyR=gR, censusL=cL, censusR=cR, vol=vol, wta=wta)
 
 
-def pipeline(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False, right_view=False):
+def pipeline(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False, right_view=False,
+             fp16_msg=False):
     """The single-pair path of main_stereo_hbp_isp.cu:33-72 (without the driver
     median); right_view selects the right-view path of main_bench_middv3.cu:189-203."""
     H, W = L.shape[:2]
@@ -195,5 +206,6 @@ def pipeline(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False, rig
     if right_view:
         vol, wta = cost_to_right(vol, W, H, D)
     seg = segment(lab(R if right_view else L))
-    disp, plane, steps, _, _ = hbp(seg, vol, wta, W, H, D, alpha, tau_smooth, min_level, fp64)
+    disp, plane, steps, _, _ = hbp(seg, vol, wta, W, H, D, alpha, tau_smooth, min_level, fp64,
+                                   fp16_msg=fp16_msg)
     return dict(disp=disp, plane=plane, steps=steps, seg=seg, wta=wta, vol=vol)

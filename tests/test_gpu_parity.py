@@ -207,3 +207,31 @@ def test_batch_lanes_match_single_pair(eng, golden_dir):
     torch.cuda.synchronize()
     for a, b in zip(single, out):
         assert np.array_equal(a, b.cpu().numpy())
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_fp16_messages_match_oracle(eng, golden_dir, name):
+    """FP16 message storage (min-normalised, FP32 arithmetic) equals the
+    oracle's FP16-store mode bit for bit."""
+    import pyoracle as O
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    L, R, D = z["left"], z["right"], int(z["D"])
+    disp = ctx.run_pair(L, R, D, E.default_params(post=1, msg_fp16=1))
+    ref = O.driver_median(O.pipeline(L, R, D, fp16_msg=True)["disp"])
+    assert np.array_equal(disp.view(np.uint32), ref.view(np.uint32)), float(np.mean(disp != ref))
+
+
+def test_fp16_messages_agree_with_fp32(eng):
+    """FP16 messages against the FP32 path on the single-pair workload
+    (450x375, D 64): at least 99.9% of pixels identical, and bad-2.0 against
+    the generator's ground truth within 0.1 percentage point."""
+    E, ctx, torch = eng
+    from scenes import make_scene
+    for seed in (1000, 1001):
+        s = make_scene(450, 375, 64, seed)
+        d32 = ctx.run_pair(s.left, s.right, 64, E.default_params(post=1))
+        d16 = ctx.run_pair(s.left, s.right, 64, E.default_params(post=1, msg_fp16=1))
+        assert np.mean(d16 == d32) >= 0.999
+        bad = lambda d: 100.0 * float(np.mean(np.abs(d - s.gt)[s.nonocc] > 2.0))
+        assert abs(bad(d16) - bad(d32)) <= 0.1

@@ -104,3 +104,19 @@ def test_hbp_agrees_with_reference(golden_dir, name):
     assert np.mean(np.abs(res["disp"] - z["disp"]) < 1.0) >= 0.99
     resR = O.pipeline(L, R, D, right_view=True)
     assert np.mean(np.abs(resR["disp"] - z["disp_right"]) < 1.0) >= 0.99
+
+
+def test_fp16_message_rounding_matches_ieee():
+    """The oracle's FP16 message store rounds like IEEE binary16 (numpy):
+    normal, subnormal, tie, overflow and special values."""
+    import pyoracle as O
+    rng = np.random.default_rng(5)
+    x = np.concatenate([
+        rng.normal(0, 1, 20000).astype(np.float32) * np.float32(10) ** rng.integers(-8, 6, 20000),
+        np.array([65504, 65519.99, 65520, 1e6, -65520, 2 ** -24, 2 ** -25, 3 * 2 ** -26, 1e-9,
+                  0.0, -0.0, np.inf, -np.inf, 1 + 2 ** -11, 1 + 3 * 2 ** -11], np.float32)])
+    with np.errstate(over="ignore"):
+        want = x.astype(np.float16).astype(np.float32)
+    got = O.round_fp16(x)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert np.isnan(O.round_fp16(np.array([np.nan], np.float32)))[0]
