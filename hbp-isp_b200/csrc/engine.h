@@ -217,9 +217,34 @@ struct ViewPlan
 void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D,
                  const HbpParams &prm, float *disp, float *plane, Arena &persist, Arena &tmp,
                  cudaStream_t st, ViewPlan &vp);
-// HBP_ISP::run_ms for up to 32 prepared views at once (same min_level).
+// HBP_ISP::run_ms for prepared views, run together to completion.
 void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &tmp,
                    cudaStream_t st);
+
+// Continuous BP over prepared views (HBP_ISP::run_ms per view). Each tick
+// advances every active view by one action (level setup, one candidate/BP
+// step, the level's final select, or MAP), with one launch per kernel kind
+// serving all views (32 per launch descriptor). Views join with add() before
+// any tick and leave after their MAP; a view's results do not depend on the
+// others in flight. Launches go to `st`; the caller orders the views'
+// preparation before their first tick (e.g. with an event).
+class BpScheduler
+{
+  public:
+    BpScheduler(const HbpParams &prm, cudaStream_t st);
+    ~BpScheduler();
+    BpScheduler(const BpScheduler &) = delete;
+    BpScheduler &operator=(const BpScheduler &) = delete;
+    void add(ViewPlan *vp, void *user);
+    // One tick; appends the user tags of views whose MAP it launched.
+    void tick(std::vector<void *> &finished);
+    int active() const;
+
+  private:
+    struct View;
+    struct Impl;
+    Impl *impl;
+};
 
 // ---------------------------------------------------------------------------
 // post.cu

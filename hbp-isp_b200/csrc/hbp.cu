@@ -235,17 +235,7 @@ struct ViewDev
     int L;
 };
 
-constexpr int MAXV = 32;
-
-struct Task
-{
-    const ViewDev *vd;             // the view's record in device memory
-    const LevelDev *lvl, *lvh;     // its level li and li+1 records
-    int v, li;
-    int first;        // first BP step of the level: no select, zero messages
-    int rb, pb, mb;   // seed buffer read / cost partials written / messages written
-    float max_dz, max_dn;
-};
+constexpr int MAXV = 32; // tasks per launch descriptor
 
 enum NodeMode
 {
@@ -254,9 +244,21 @@ enum NodeMode
     NODE_SELECT_RANDOM = 2
 };
 
+
+struct Task
+{
+    const ViewDev *vd;             // the view's record in device memory
+    const LevelDev *lvl, *lvh;     // its level li and li+1 records
+    int v, li;
+    int first;        // first BP step of the level: no select, zero messages
+    int rb, pb, mb;   // seed buffer read / cost partials written / messages written
+    int mode;         // node phase: NodeMode
+    float max_dz, max_dn;
+};
+
 struct StepDesc
 {
-    int nt, mode;
+    int nt;
     int pre[MAXV + 1];
     Task t[MAXV];
 };
@@ -496,9 +498,9 @@ __global__ void __launch_bounds__(128) k_node(const ViewDev *__restrict__ V, Ste
     const int n = item - d.pre[find_task(d, item)];
     if (!t.first)
         select_thread(l, n, v.b.pc[t.pb ^ 1], v.b, t.mb ^ 1);
-    if (d.mode == NODE_SELECT_RANSAC)
+    if (t.mode == NODE_SELECT_RANSAC)
         ransac_thread(l, v.c, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n]);
-    else if (d.mode == NODE_SELECT_RANDOM)
+    else if (t.mode == NODE_SELECT_RANDOM)
         random_thread(l, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n], t.max_dz, t.max_dn);
 }
 
@@ -964,7 +966,8 @@ int read_dev_int(const int *p, cudaStream_t st)
 // host side
 struct ViewPlan::Impl
 {
-    ViewDev vd;
+    ViewDev vd;              // host copy
+    ViewDev *vd_dev = nullptr; // the same record in device memory
     std::vector<LevelDev> lv;
 };
 
@@ -1103,94 +1106,174 @@ void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D
     vd.b.buf = persist.alloc<float4>((size_t)Nmax * P);
     vd.disp = disp;
     vd.plane_out = plane_out;
-    HBP_CUDA(cudaStreamSynchronize(st)); // lv (host) feeds the copy above
+    vp.impl->vd_dev = persist.alloc<ViewDev>(1);
+    HBP_CUDA(cudaMemcpyAsync(vp.impl->vd_dev, &vd, sizeof(ViewDev), cudaMemcpyHostToDevice, st));
+    HBP_CUDA(cudaStreamSynchronize(st)); // lv and vd (host) feed the copies above
     tmp.rewind(tm);
 }
 
 namespace
 {
-struct TaskState
-{
-    int v, li, step = 0, rb = 0;
-    float max_dz = 0, max_dn = 0;
-};
-
 void launch_cost(const ViewDev *V, const StepDesc &d, int mode, cudaStream_t st)
 {
     k_cost<<<blocks((long)d.pre[d.nt] * 32, 256), 256, 0, st>>>(V, d, mode);
     note_launch();
 }
+
+enum Phase
+{
+    PH_INIT,  // level setup: priors, their costs, beliefs, seeds (init_bp)
+    PH_STEP,  // one candidate step + data cost + BP sweep
+    PH_FINAL, // the level's last select
+    PH_MAP,   // map_msg at min_level
+    PH_DONE
+};
+
+// what a launch counts per task
+enum Count
+{
+    CNT_NODES,
+    CNT_WINDOWS, // 256-position windows of the pixel list
+    CNT_EDGES,
+    CNT_PARENTS,
+    CNT_NODES_OR_PARENTS
+};
 } // namespace
 
-// HBP_ISP::run_ms for every view of the batch (hbp_isp.cu:1313-1346): levels
-// coarse to fine in lockstep, views whose pyramid is shallower join when
-// their top level is reached; random-adjust steps run for the views whose
-// max_dz is still above the end threshold.
-void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &tmp,
-                   cudaStream_t st)
+// One view's place in HBP_ISP::run_ms (hbp_isp.cu:1313-1346): level li, outer
+// iteration i, candidate step it (0-3 RANSAC, 4 spatial, 5 random adjust).
+struct BpScheduler::View
 {
-    const int nv = (int)views.size();
-    if (nv == 0)
-        return;
-    if (nv > MAXV)
-        throw StatusError{HBP_ERR_INVALID_ARG, "too many views in one BP batch"};
-    const int m = prm.min_level;
-    size_t mark = tmp.mark();
-    std::vector<ViewDev> vh(nv);
-    int maxL = 0;
-    for (int i = 0; i < nv; ++i)
-    {
-        vh[i] = views[i]->impl->vd;
-        maxL = std::max(maxL, views[i]->L);
-        if (views[i]->min_level != m)
-            throw StatusError{HBP_ERR_INVALID_ARG, "views of one batch share min_level"};
-    }
-    ViewDev *V = tmp.alloc<ViewDev>(nv);
-    HBP_CUDA(cudaMemcpyAsync(V, vh.data(), sizeof(ViewDev) * nv, cudaMemcpyHostToDevice, st));
-    KernelProf *prof = prm.prof && prm.prof->on ? prm.prof : nullptr;
-    long prof_step = 0;
+    ViewPlan *vp;
+    void *user;
+    int phase = PH_INIT, li = 0, i = 0, it = 0, step = 0, rb = 0;
+    float max_dz = 0, max_dn = 0;
 
-    auto desc = [&](const std::vector<TaskState *> &ts, int what, bool first) {
-        // what: 0 nodes, 1 256-windows of the pixel list, 2 edges, 3 parents,
-        // 4 max(nodes, parents)
-        StepDesc d{};
-        d.nt = (int)ts.size();
-        d.pre[0] = 0;
-        for (int k = 0; k < d.nt; ++k)
+    int iter_bp() const { return 10 + 10 * li; }
+    void enter_level(int level)
+    {
+        li = level;
+        phase = PH_INIT;
+        step = 0;
+        i = 0;
+        it = 0;
+        max_dz = (float)vp->D / 2.0f * (float)li / (float)vp->L;
+        max_dn = 1.0f * (float)li / (float)vp->L;
+    }
+    // skip random-adjust steps that do not apply; end the level after its
+    // last iteration
+    void settle()
+    {
+        while (phase == PH_STEP)
         {
-            const TaskState &s = *ts[k];
-            const ViewPlan &vp = *views[s.v];
-            int n = vp.levelN[s.li], e = vp.levelE[s.li], ch = (vp.HW + PC_CHUNK - 1) / PC_CHUNK;
-            int nh = s.li + 1 < vp.L ? vp.levelN[s.li + 1] : 1;
-            int cnt = what == 0 ? n : what == 1 ? ch : what == 2 ? e : what == 3 ? nh : std::max(n, nh);
-            d.pre[k + 1] = d.pre[k] + cnt;
-            Task &t = d.t[k];
-            t.vd = V + s.v;
-            t.lvl = vh[s.v].lv + s.li;
-            t.lvh = s.li + 1 < vp.L ? vh[s.v].lv + s.li + 1 : t.lvl;
-            t.v = s.v;
-            t.li = s.li;
-            t.first = first ? 1 : 0;
-            t.rb = s.rb;
-            t.pb = s.step & 1;
-            t.mb = s.step & 1;
-            t.max_dz = s.max_dz;
-            t.max_dn = s.max_dn;
+            if (i >= iter_bp())
+            {
+                phase = PH_FINAL;
+                break;
+            }
+            if (it == 5 && !(i > iter_bp() / 4 * 3 && max_dz >= 0.01f))
+            {
+                it = 0;
+                ++i;
+                continue;
+            }
+            break;
         }
-        return d;
-    };
-    auto timed = [&](bool on, auto &&f) {
-        if (on)
-            prof->mark(st);
-        f();
-        if (on)
-            prof->mark(st);
-    };
-    // breakdown profiling: kinds 0 node, 1 child, 2 neighbor, 3 set_cand,
-    // 4 cost step, 5 edges, 6 cost init, 7 init_nodes, 8 map
+    }
+    int kind() const { return it <= 3 ? 0 : it == 4 ? 1 : 2; }
+};
+
+struct BpScheduler::Impl
+{
+    HbpParams prm;
+    cudaStream_t st;
+    std::vector<View> views;
+    long ticks = 0;
+
+    Task task_of(const View &v, bool first, int pb, int mode) const
+    {
+        const ViewPlan &vp = *v.vp;
+        const ViewDev &vd = vp.impl->vd;
+        Task t{};
+        t.vd = vp.impl->vd_dev;
+        t.lvl = vd.lv + v.li;
+        t.lvh = v.li + 1 < vp.L ? vd.lv + v.li + 1 : t.lvl;
+        t.v = 0;
+        t.li = v.li;
+        t.first = first ? 1 : 0;
+        t.rb = v.rb;
+        t.pb = pb;
+        t.mb = v.step & 1;
+        t.mode = mode;
+        t.max_dz = v.max_dz;
+        t.max_dn = v.max_dn;
+        return t;
+    }
+    static int count_of(const View &v, int what)
+    {
+        const ViewPlan &vp = *v.vp;
+        const int n = vp.levelN[v.li], e = vp.levelE[v.li];
+        const int nh = v.li + 1 < vp.L ? vp.levelN[v.li + 1] : 1;
+        const int w = (vp.HW + PC_CHUNK - 1) / PC_CHUNK;
+        return what == CNT_NODES ? n : what == CNT_WINDOWS ? w : what == CNT_EDGES ? e
+               : what == CNT_PARENTS ? nh : std::max(n, nh);
+    }
+    // Launch f(desc) over the tasks in descriptors of at most MAXV tasks.
+    template <typename F>
+    void launch(const std::vector<const View *> &vs, const std::vector<Task> &ts, int what, F &&f)
+    {
+        for (size_t b = 0; b < ts.size(); b += MAXV)
+        {
+            StepDesc d{};
+            d.nt = (int)std::min<size_t>(MAXV, ts.size() - b);
+            d.pre[0] = 0;
+            for (int k = 0; k < d.nt; ++k)
+            {
+                d.t[k] = ts[b + k];
+                d.pre[k + 1] = d.pre[k] + count_of(*vs[b + k], what);
+            }
+            if (d.pre[d.nt] > 0)
+                f(d);
+        }
+    }
+};
+
+BpScheduler::BpScheduler(const HbpParams &prm, cudaStream_t st) : impl(new Impl)
+{
+    impl->prm = prm;
+    impl->st = st;
+}
+
+BpScheduler::~BpScheduler() { delete impl; }
+
+int BpScheduler::active() const { return (int)impl->views.size(); }
+
+void BpScheduler::add(ViewPlan *vp, void *user)
+{
+    View v;
+    v.vp = vp;
+    v.user = user;
+    if (vp->L - 2 >= vp->min_level)
+        v.enter_level(vp->L - 2);
+    else
+    {
+        v.li = vp->min_level;
+        v.phase = PH_MAP;
+    }
+    impl->views.push_back(v);
+}
+
+// One tick: every active view takes one action; one launch per kernel kind
+// (per 32 views) serves all of them. Views never read one another's data, so
+// a view's results do not depend on what else is in flight.
+void BpScheduler::tick(std::vector<void *> &finished)
+{
+    Impl &I = *impl;
+    const cudaStream_t st = I.st;
+    KernelProf *prof = I.prm.prof && I.prm.prof->on ? I.prm.prof : nullptr;
     KernelProf *bprof = prof && prof->breakdown ? prof : nullptr;
-    long substep = 0;
-    bool sample = false;
+    const long tk = I.ticks++;
+    const bool sample = bprof && tk % 8 == 0;
     auto run = [&](int kind, int li, auto &&f) {
         if (!bprof)
         {
@@ -1210,141 +1293,166 @@ void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, A
             f();
     };
 
-    std::vector<TaskState> state(nv);
-    for (int li = maxL - 2; li >= m; --li)
+    std::vector<const View *> vi, vn, vs, vc, vm;
+    std::vector<Task> ti, tn, ts, tc, tm;
+    for (const View &v : I.views)
     {
-        std::vector<TaskState *> act;
-        for (int i = 0; i < nv; ++i)
-            if (views[i]->L - 2 >= li)
-            {
-                TaskState &s = state[i];
-                s.v = i;
-                s.li = li;
-                s.step = 0;
-                s.max_dz = (float)views[i]->D / 2.0f * (float)li / (float)views[i]->L;
-                s.max_dn = 1.0f * (float)li / (float)views[i]->L;
-                act.push_back(&s);
-            }
-        if (act.empty())
-            continue;
-        char rname[32];
-        std::snprintf(rname, sizeof(rname), "bp_level_%d", li);
-        NvtxRange level_range(rname);
-        // init_bp: priors and their data cost (partials in pc[0]), then costs,
-        // beliefs and seeds per node
+        const bool first = v.step == 0;
+        const int pb = v.step & 1;
+        switch (v.phase)
         {
-            sample = true;
-            StepDesc d = desc(act, 1, true);
-            for (int k = 0; k < d.nt; ++k)
-                d.t[k].pb = 0;
-            run(6, li, [&] { launch_cost(V, d, COST_INIT, st); });
-            StepDesc dn = desc(act, 4, true);
-            for (int k = 0; k < dn.nt; ++k)
-                dn.t[k].pb = 0;
-            run(7, li, [&] { k_init_nodes<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
-            note_launch();
-            HBP_LAUNCH_CHECK();
-        }
-        const int iter_bp = 10 + 10 * li;
-        for (int i = 0; i < iter_bp; ++i)
+        case PH_INIT:
+            vi.push_back(&v);
+            ti.push_back(I.task_of(v, true, 0, NODE_SELECT));
+            break;
+        case PH_STEP:
         {
-            for (int it = 0; it <= 5; ++it)
+            const int k = v.kind();
+            const int mode = k == 0 ? NODE_SELECT_RANSAC : k == 2 ? NODE_SELECT_RANDOM : NODE_SELECT;
+            vn.push_back(&v);
+            tn.push_back(I.task_of(v, first, pb, mode));
+            if (k == 1)
             {
-                std::vector<TaskState *> ts;
-                int kind;
-                if (it <= 3)
-                {
-                    kind = 0;
-                    ts = act;
-                }
-                else if (it == 4)
-                {
-                    kind = 1;
-                    ts = act;
-                }
-                else
-                {
-                    kind = 2;
-                    for (TaskState *s : act)
-                        if (i > iter_bp / 4 * 3 && s->max_dz >= 0.01f)
-                            ts.push_back(s);
-                    if (ts.empty())
-                        break;
-                }
-                const bool first = ts[0]->step == 0; // all tasks start a level together
-                const bool tp = prof && (prof_step++ % 16 == 0);
-                sample = substep++ % 8 == 0;
-                StepDesc dn = desc(ts, 0, first);
-                dn.mode = kind == 0 ? NODE_SELECT_RANSAC : kind == 2 ? NODE_SELECT_RANDOM : NODE_SELECT;
-                run(0, li, [&] { k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
-                note_launch();
-                if (kind == 1)
-                {
-                    StepDesc dp = desc(ts, 3, first);
-                    run(1, li, [&] { k_child<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp); });
-                    note_launch();
-                    run(2, li, [&] { k_neighbor<<<blocks(dp.pre[dp.nt], 128), 128, 0, st>>>(V, dp); });
-                    note_launch();
-                    run(3, li, [&] { k_set_cand<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
-                    note_launch();
-                }
-                StepDesc dc = desc(ts, 1, first);
-                run(4, li, [&] { timed(tp, [&] { launch_cost(V, dc, COST_STEP, st); }); });
-                StepDesc de = desc(ts, 2, first);
-                run(5, li, [&] { k_edges<<<blocks(de.pre[de.nt], 128), 128, 0, st>>>(V, de); });
-                note_launch();
-                HBP_LAUNCH_CHECK();
-                if (tp)
-                {
-                    // compulsory bytes of the timed data-cost launch: every
-                    // pixel's packed id (4 B) and two volume bytes per candidate,
-                    // plus per chunk the node's 4 planes in and 4 partial sums out
-                    for (TaskState *s : ts)
-                    {
-                        const ViewPlan &vp = *views[s->v];
-                        prof->bytes += (double)vp.HW * (4 + 2 * P) + (double)vp.levelC[s->li] * (4 * 16 + 16);
-                    }
-                    prof->launches += 1;
-                }
-                for (TaskState *s : ts)
-                {
-                    s->step++;
-                    if (kind == 0 || kind == 2)
-                        s->rb ^= 1;
-                    if (kind == 2)
-                    {
-                        s->max_dz /= 2.0f;
-                        s->max_dn /= 2.0f;
-                    }
-                }
+                vs.push_back(&v);
+                ts.push_back(I.task_of(v, first, pb, mode));
             }
+            vc.push_back(&v);
+            tc.push_back(I.task_of(v, first, pb, mode));
+            break;
         }
-        // final select of the level
-        StepDesc dn = desc(act, 0, false);
-        dn.mode = NODE_SELECT;
-        sample = true;
-        run(0, li, [&] { k_node<<<blocks(dn.pre[dn.nt], 128), 128, 0, st>>>(V, dn); });
-        note_launch();
-        HBP_LAUNCH_CHECK();
+        case PH_FINAL:
+            vn.push_back(&v);
+            tn.push_back(I.task_of(v, false, pb, NODE_SELECT));
+            break;
+        case PH_MAP:
+            vm.push_back(&v);
+            tm.push_back(I.task_of(v, false, pb, NODE_SELECT));
+            break;
+        }
     }
-    // MAP at min_level for every view
+    // NVTX range named after the pyramid level of the tick's first view (the
+    // profiling recipes select one level of a lockstep batch with it)
+    char rname[32];
+    std::snprintf(rname, sizeof(rname), "bp_level_%d", I.views.empty() ? -1 : I.views[0].li);
+    NvtxRange tick_range(rname);
+    const int lvl_i = vi.empty() ? 0 : vi[0]->li, lvl_n = vn.empty() ? 0 : vn[0]->li;
+    const int lvl_c = vc.empty() ? 0 : vc[0]->li, lvl_s = vs.empty() ? 0 : vs[0]->li;
+    // level setup (init_bp): prior costs into pc[0], then costs, beliefs, seeds
+    I.launch(vi, ti, CNT_WINDOWS, [&](const StepDesc &d) {
+        run(6, lvl_i, [&] { launch_cost(nullptr, d, COST_INIT, st); });
+    });
+    I.launch(vi, ti, CNT_NODES_OR_PARENTS, [&](const StepDesc &d) {
+        run(7, lvl_i, [&] { k_init_nodes<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        note_launch();
+    });
+    // node phase: select of the previous step + the step's candidates
+    I.launch(vn, tn, CNT_NODES, [&](const StepDesc &d) {
+        run(0, lvl_n, [&] { k_node<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        note_launch();
+    });
+    // spatial candidates
+    I.launch(vs, ts, CNT_PARENTS, [&](const StepDesc &d) {
+        run(1, lvl_s, [&] { k_child<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        note_launch();
+        run(2, lvl_s, [&] { k_neighbor<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        note_launch();
+    });
+    I.launch(vs, ts, CNT_NODES, [&](const StepDesc &d) {
+        run(3, lvl_s, [&] { k_set_cand<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        note_launch();
+    });
+    // data cost of the candidates, then the BP sweep
+    const bool tp = prof && !vc.empty() && (tk % 16 == 0);
+    I.launch(vc, tc, CNT_WINDOWS, [&](const StepDesc &d) {
+        run(4, lvl_c, [&] {
+            if (tp)
+                prof->mark(st);
+            launch_cost(nullptr, d, COST_STEP, st);
+            if (tp)
+                prof->mark(st);
+        });
+    });
+    if (tp)
+    {
+        // compulsory bytes of the timed data-cost launches: every pixel's list
+        // entry (packed position 4 B + node 4 B) and two volume bytes per
+        // candidate, plus per chunk the node's 4 planes in and 4 sums out
+        for (const View *v : vc)
+            prof->bytes += (double)v->vp->HW * (8 + 2 * P) + (double)v->vp->levelC[v->li] * (4 * 16 + 16);
+        prof->launches += (long)((tc.size() + MAXV - 1) / MAXV);
+    }
+    I.launch(vc, tc, CNT_EDGES, [&](const StepDesc &d) {
+        run(5, lvl_c, [&] { k_edges<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        note_launch();
+    });
+    // MAP at min_level
+    if (!vm.empty())
     {
         NvtxRange map_range("bp_map");
-        std::vector<TaskState *> all;
-        for (int i = 0; i < nv; ++i)
-        {
-            state[i].v = i;
-            state[i].li = m;
-            all.push_back(&state[i]);
-        }
-        StepDesc d = desc(all, 0, false);
-        sample = true;
-        run(8, m, [&] { k_map<<<blocks((long)d.pre[d.nt] * 32, 128), 128, 0, st>>>(V, d); });
-        note_launch();
-        HBP_LAUNCH_CHECK();
+        I.launch(vm, tm, CNT_NODES, [&](const StepDesc &d) {
+            run(8, vm[0]->li, [&] { k_map<<<blocks((long)d.pre[d.nt] * 32, 128), 128, 0, st>>>(nullptr, d); });
+            note_launch();
+        });
     }
+    HBP_LAUNCH_CHECK();
+    // advance every view by the action it took
+    std::vector<View> keep;
+    keep.reserve(I.views.size());
+    for (View &v : I.views)
+    {
+        switch (v.phase)
+        {
+        case PH_INIT:
+            v.phase = PH_STEP;
+            v.settle();
+            break;
+        case PH_STEP:
+        {
+            const int k = v.kind();
+            v.step++;
+            if (k == 0 || k == 2)
+                v.rb ^= 1;
+            if (k == 2)
+            {
+                v.max_dz /= 2.0f;
+                v.max_dn /= 2.0f;
+            }
+            if (++v.it == 6)
+            {
+                v.it = 0;
+                ++v.i;
+            }
+            v.settle();
+            break;
+        }
+        case PH_FINAL:
+            if (v.li > v.vp->min_level)
+                v.enter_level(v.li - 1);
+            else
+                v.phase = PH_MAP;
+            break;
+        case PH_MAP:
+            v.phase = PH_DONE;
+            break;
+        }
+        if (v.phase == PH_DONE)
+            finished.push_back(v.user);
+        else
+            keep.push_back(v);
+    }
+    I.views.swap(keep);
+}
+
+// HBP_ISP::run_ms for every view (hbp_isp.cu:1313-1346), all admitted at once.
+void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &, cudaStream_t st)
+{
+    BpScheduler s(prm, st);
+    for (ViewPlan *vp : views)
+        s.add(vp, vp);
+    std::vector<void *> fin;
+    while (s.active())
+        s.tick(fin);
     HBP_CUDA(cudaStreamSynchronize(st));
-    tmp.rewind(mark);
 }
 
 } // namespace hbp
