@@ -8,7 +8,11 @@
 #include <string>
 #include <cstdlib>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
 #include <thread>
+#include <unordered_map>
 
 #include "engine.h"
 
@@ -212,12 +216,13 @@ void ensure_slot(Slot *sl, long pixels, int D)
 // pyramid(s) and BP level setup, all on the lane's stream; persistent data in
 // the pair's slot.
 void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint8_t *dR, int W, int H,
-                  int D, const hbp_params &p, float *disp, float *plane)
+                  int D, const hbp_params &p, float *disp, float *plane, bool reset_slot = true)
 {
     const long n = (long)W * H;
     cudaStream_t st = L->st;
     Arena &a = sl->mem;
-    a.reset();
+    if (reset_slot)
+        a.reset();
     L->tmp.reset();
     HBP_CUDA(cudaMemsetAsync(L->err_dev, 0, sizeof(int), st));
     const bool lr = p.post == 2;
@@ -803,6 +808,439 @@ hbp_status hbp_profile_breakdown(hbp_ctx *c, double *ms, long *timed, long *all)
     if (!c || !ms || !timed || !all)
         return fail(HBP_ERR_INVALID_ARG, "null pointer");
     return guarded([&] { c->prof.read_breakdown(ms, timed, all); });
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Request server: continuous batching of pairs of any size.
+//
+// Requests are admitted by their device footprint against the server's
+// budget, prepared (upload, cost volume, pyramid, BP setup) by preparation
+// lanes on their own streams, then join the BP scheduler at its next tick;
+// each tick advances every pair in flight by one BP action with one launch per
+// kernel kind. A pair leaves after its MAP, runs the driver's median and is
+// copied to pinned staging on the scheduler stream; its result reaches the
+// caller's buffer when that copy has completed.
+namespace
+{
+double now_ms()
+{
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct ServerSlot
+{
+    Slot slot;
+    size_t bytes = 0;       // device bytes of slot.mem
+    float *pinned = nullptr; // disparity staging (cap_pixels floats)
+    ~ServerSlot()
+    {
+        if (pinned)
+            cudaFreeHost(pinned);
+    }
+};
+
+enum ReqState
+{
+    RQ_QUEUED,
+    RQ_PREPARING,
+    RQ_BP,
+    RQ_FINISHING,
+    RQ_DONE
+};
+
+struct ServerReq
+{
+    long long id = 0;
+    const uint8_t *L = nullptr, *R = nullptr;
+    float *out = nullptr;
+    int W = 0, H = 0, D = 0;
+    size_t need = 0;
+    int state = RQ_QUEUED;
+    hbp_status st = HBP_OK;
+    std::string err;
+    double t_submit = 0, t_done = 0;
+    ServerSlot *ss = nullptr;
+    bool new_slot = false;
+    float *ddisp = nullptr, *dtmp = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_done = nullptr;
+};
+
+size_t request_bytes(int W, int H, int D) { return slab_bytes((long)W * H, D); }
+} // namespace
+
+struct hbp_server
+{
+    int device = 0;
+    hbp_params prm{};
+    size_t budget = 0, allocated = 0;
+    std::mutex mu;
+    std::condition_variable cv_prep, cv_sched, cv_done;
+    std::deque<ServerReq *> queued, to_prep, ready;
+    std::unordered_map<long long, std::unique_ptr<ServerReq>> reqs;
+    std::vector<std::unique_ptr<ServerSlot>> pool; // free slots
+    std::vector<std::unique_ptr<ServerSlot>> busy;  // slots of admitted requests
+    std::vector<std::unique_ptr<Lane>> lanes;
+    std::vector<std::thread> threads;
+    long long next_id = 1;
+    bool stop = false;
+    hbp_status fatal = HBP_OK;
+    std::string fatal_msg;
+    Lane sched; // scheduler stream (+ error word, unused arenas)
+
+    // Admit queued requests in arrival order while memory allows: a free
+    // slot large enough, else a new one within the budget (freeing pooled
+    // slots that are too small when that makes room). Caller holds mu.
+    void admit_locked()
+    {
+        while (!queued.empty())
+        {
+            ServerReq *r = queued.front();
+            const long px = (long)r->W * r->H;
+            int pick = -1;
+            for (size_t i = 0; i < pool.size(); ++i)
+                if (pool[i]->slot.cap_pixels >= px && pool[i]->slot.cap_disp >= r->D &&
+                    (pick < 0 || pool[i]->bytes < pool[(size_t)pick]->bytes))
+                    pick = (int)i;
+            if (pick >= 0)
+            {
+                r->ss = pool[(size_t)pick].get();
+                busy.push_back(std::move(pool[(size_t)pick]));
+                pool.erase(pool.begin() + pick);
+            }
+            else
+            {
+                while (allocated + r->need > budget && !pool.empty())
+                {
+                    allocated -= pool.back()->bytes;
+                    pool.pop_back(); // frees its device and pinned memory
+                }
+                if (allocated + r->need > budget)
+                    break; // wait for a request to finish
+                auto ns = std::make_unique<ServerSlot>();
+                ns->bytes = r->need;
+                allocated += r->need;
+                r->ss = ns.get();
+                r->new_slot = true;
+                busy.push_back(std::move(ns));
+            }
+            queued.pop_front();
+            r->state = RQ_PREPARING;
+            to_prep.push_back(r);
+            cv_prep.notify_one();
+        }
+    }
+
+    void release_slot_locked(ServerSlot *ss)
+    {
+        for (size_t i = 0; i < busy.size(); ++i)
+            if (busy[i].get() == ss)
+            {
+                pool.push_back(std::move(busy[i]));
+                busy.erase(busy.begin() + (long)i);
+                return;
+            }
+    }
+
+    void finish_locked(ServerReq *r, hbp_status st, const std::string &msg)
+    {
+        r->st = st;
+        r->err = msg;
+        r->t_done = now_ms();
+        r->state = RQ_DONE;
+        if (r->ss)
+            release_slot_locked(r->ss);
+        r->ss = nullptr;
+        admit_locked();
+        cv_done.notify_all();
+    }
+
+    void prep_loop(Lane *L)
+    {
+        cudaSetDevice(device);
+        for (;;)
+        {
+            ServerReq *r;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_prep.wait(lk, [&] { return stop || !to_prep.empty(); });
+                if (stop && to_prep.empty())
+                    return;
+                r = to_prep.front();
+                to_prep.pop_front();
+            }
+            std::string msg;
+            hbp_status st = guarded([&] {
+                ServerSlot *ss = r->ss;
+                const long n = (long)r->W * r->H;
+                if (!ss->pinned || ss->slot.cap_pixels < n)
+                {
+                    ensure_slot(&ss->slot, n, r->D);
+                    if (ss->pinned)
+                        cudaFreeHost(ss->pinned);
+                    ss->pinned = nullptr;
+                    HBP_CUDA(cudaMallocHost(&ss->pinned, sizeof(float) * (size_t)ss->slot.cap_pixels));
+                }
+                ensure_slot(&ss->slot, n, r->D);
+                if (L->cap_pixels < n)
+                {
+                    L->tmp.init(tmp_bytes(std::max<long>(n, L->cap_pixels)));
+                    L->cap_pixels = std::max<long>(n, L->cap_pixels);
+                }
+                Arena &a = ss->slot.mem;
+                a.reset();
+                uint8_t *dL = a.alloc<uint8_t>(3 * (size_t)n), *dR = a.alloc<uint8_t>(3 * (size_t)n);
+                r->ddisp = a.alloc<float>(n);
+                r->dtmp = a.alloc<float>(n);
+                HBP_CUDA(cudaMemcpyAsync(dL, r->L, 3 * (size_t)n, cudaMemcpyHostToDevice, L->st));
+                HBP_CUDA(cudaMemcpyAsync(dR, r->R, 3 * (size_t)n, cudaMemcpyHostToDevice, L->st));
+                hbp_params p = prm;
+                p.post = 1;
+                prepare_pair(nullptr, L, &ss->slot, dL, dR, r->W, r->H, r->D, p, r->ddisp, nullptr, false);
+                if (!r->ev_ready)
+                    HBP_CUDA(cudaEventCreateWithFlags(&r->ev_ready, cudaEventDisableTiming));
+                HBP_CUDA(cudaEventRecord(r->ev_ready, L->st));
+            });
+            if (st != HBP_OK)
+                msg = g_err;
+            std::lock_guard<std::mutex> lk(mu);
+            if (st == HBP_OK && fatal != HBP_OK)
+            {
+                st = fatal;
+                msg = fatal_msg;
+            }
+            if (st != HBP_OK)
+                finish_locked(r, st, msg);
+            else
+            {
+                r->state = RQ_BP;
+                ready.push_back(r);
+                cv_sched.notify_one();
+            }
+        }
+    }
+
+    void sched_loop()
+    {
+        cudaSetDevice(device);
+        HbpParams q = to_params(&prm);
+        BpScheduler bp(q, sched.st);
+        std::deque<ServerReq *> finishing;
+        std::vector<void *> fin;
+        for (;;)
+        {
+            std::vector<ServerReq *> join;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                if (!bp.active() && finishing.empty())
+                    cv_sched.wait(lk, [&] { return stop || !ready.empty(); });
+                if (stop && !bp.active() && finishing.empty() && ready.empty())
+                    return;
+                join.assign(ready.begin(), ready.end());
+                ready.clear();
+            }
+            hbp_status st = guarded([&] {
+                for (ServerReq *r : join)
+                {
+                    HBP_CUDA(cudaStreamWaitEvent(sched.st, r->ev_ready, 0));
+                    bp.add(&r->ss->slot.plan, r);
+                }
+                if (bp.active())
+                {
+                    fin.clear();
+                    bp.tick(fin);
+                    for (void *f : fin)
+                    {
+                        ServerReq *r = static_cast<ServerReq *>(f);
+                        const long n = (long)r->W * r->H;
+                        launch_driver_median(r->ddisp, r->dtmp, r->W, r->H, sched.st);
+                        HBP_CUDA(cudaMemcpyAsync(r->ss->pinned, r->ddisp, sizeof(float) * n,
+                                                 cudaMemcpyDeviceToHost, sched.st));
+                        if (!r->ev_done)
+                            HBP_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
+                        HBP_CUDA(cudaEventRecord(r->ev_done, sched.st));
+                        r->state = RQ_FINISHING;
+                        finishing.push_back(r);
+                    }
+                }
+                // completions, in order
+                while (!finishing.empty())
+                {
+                    ServerReq *r = finishing.front();
+                    cudaError_t q = bp.active() ? cudaEventQuery(r->ev_done) : cudaEventSynchronize(r->ev_done);
+                    if (q == cudaErrorNotReady)
+                        break;
+                    HBP_CUDA(q);
+                    std::memcpy(r->out, r->ss->pinned, sizeof(float) * (size_t)r->W * r->H);
+                    finishing.pop_front();
+                    std::lock_guard<std::mutex> lk(mu);
+                    finish_locked(r, HBP_OK, "");
+                }
+            });
+            if (st != HBP_OK)
+            {
+                // a CUDA failure on the scheduler stream ends the server: fail
+                // everything in flight and every later request
+                std::lock_guard<std::mutex> lk(mu);
+                fatal = st;
+                fatal_msg = g_err;
+                for (auto &kv : reqs)
+                    if (kv.second->state != RQ_DONE && kv.second->state != RQ_QUEUED &&
+                        kv.second->state != RQ_PREPARING)
+                        finish_locked(kv.second.get(), st, fatal_msg);
+                return;
+            }
+        }
+    }
+};
+
+extern "C" {
+
+size_t hbp_request_bytes(int W, int H, int D)
+{
+    return W > 0 && H > 0 && D > 0 ? request_bytes(W, H, D) : 0;
+}
+
+hbp_status hbp_server_create(int device, size_t budget_bytes, int prep_lanes, const hbp_params *prm,
+                             hbp_server **out)
+{
+    if (!out || budget_bytes == 0 || prep_lanes < 1 || prep_lanes > 64)
+        return fail(HBP_ERR_INVALID_ARG, "need a budget > 0 and 1..64 preparation lanes");
+    if (prm && (prm->post < 0 || prm->post > 1))
+        return fail(HBP_ERR_INVALID_ARG, "the server runs post = 0 or 1 (driver median)");
+    *out = nullptr;
+    auto s = std::make_unique<hbp_server>();
+    s->device = device;
+    s->budget = budget_bytes;
+    hbp_default_params(&s->prm);
+    if (prm)
+        s->prm = *prm;
+    hbp_status st = guarded([&] {
+        lane_init(&s->sched, device);
+        for (int i = 0; i < prep_lanes; ++i)
+        {
+            s->lanes.push_back(std::make_unique<Lane>());
+            lane_init(s->lanes.back().get(), device);
+        }
+    });
+    if (st != HBP_OK)
+        return st;
+    hbp_server *raw = s.get();
+    for (auto &l : s->lanes)
+        s->threads.emplace_back([raw, L = l.get()] { raw->prep_loop(L); });
+    s->threads.emplace_back([raw] { raw->sched_loop(); });
+    *out = s.release();
+    return HBP_OK;
+}
+
+void hbp_server_destroy(hbp_server *s)
+{
+    if (!s)
+        return;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        // finish what was admitted; drop what is still queued
+        for (ServerReq *r : s->queued)
+        {
+            r->st = HBP_ERR_TIMEOUT;
+            r->state = RQ_DONE;
+        }
+        s->queued.clear();
+        s->stop = true;
+        s->cv_done.notify_all();
+        s->cv_prep.notify_all();
+        s->cv_sched.notify_all();
+    }
+    for (auto &t : s->threads)
+        t.join();
+    for (auto &kv : s->reqs)
+    {
+        if (kv.second->ev_ready)
+            cudaEventDestroy(kv.second->ev_ready);
+        if (kv.second->ev_done)
+            cudaEventDestroy(kv.second->ev_done);
+    }
+    s->pool.clear();
+    s->busy.clear();
+    for (auto &l : s->lanes)
+        lane_release(l.get());
+    lane_release(&s->sched);
+    delete s;
+}
+
+hbp_status hbp_submit(hbp_server *s, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
+                      float *disp, long long *id)
+{
+    if (!s || !bgrL || !bgrR || !disp || !id)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, D);
+        auto r = std::make_unique<ServerReq>();
+        r->L = bgrL;
+        r->R = bgrR;
+        r->out = disp;
+        r->W = W;
+        r->H = H;
+        r->D = D;
+        r->need = request_bytes(W, H, D);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->fatal != HBP_OK)
+            throw StatusError{s->fatal, "the server stopped after a CUDA error"};
+        if (r->need > s->budget)
+            throw StatusError{HBP_ERR_ADMISSION_REJECTED, "the pair needs more device memory than the server's budget"};
+        r->id = s->next_id++;
+        r->t_submit = now_ms();
+        *id = r->id;
+        ServerReq *raw = r.get();
+        s->reqs.emplace(r->id, std::move(r));
+        s->queued.push_back(raw);
+        s->admit_locked();
+    });
+}
+
+hbp_status hbp_poll(hbp_server *s, long long id)
+{
+    if (!s)
+        return fail(HBP_ERR_INVALID_ARG, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end())
+        return fail(HBP_ERR_INVALID_ARG, "unknown request id");
+    if (it->second->state != RQ_DONE)
+        return HBP_ERR_NOT_READY;
+    if (it->second->st != HBP_OK)
+        return fail(it->second->st, it->second->err);
+    return HBP_OK;
+}
+
+hbp_status hbp_wait(hbp_server *s, long long id, double timeout_ms, double *latency_ms)
+{
+    if (!s)
+        return fail(HBP_ERR_INVALID_ARG, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end())
+        return fail(HBP_ERR_INVALID_ARG, "unknown request id");
+    ServerReq *r = it->second.get();
+    auto done = [&] { return r->state == RQ_DONE; };
+    if (timeout_ms < 0)
+        s->cv_done.wait(lk, done);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done))
+        return fail(HBP_ERR_TIMEOUT, "request still running");
+    const hbp_status st = r->st;
+    const std::string msg = r->err;
+    if (latency_ms)
+        *latency_ms = r->t_done - r->t_submit;
+    if (r->ev_ready)
+        cudaEventDestroy(r->ev_ready);
+    if (r->ev_done)
+        cudaEventDestroy(r->ev_done);
+    s->reqs.erase(it);
+    if (st != HBP_OK)
+        return fail(st, msg);
+    return HBP_OK;
 }
 
 } // extern "C"

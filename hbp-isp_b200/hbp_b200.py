@@ -51,6 +51,12 @@ def lib():
         L.hbp_ctx_stream.restype = P
         L.hbp_ctx_create.argtypes = [C.c_int, C.c_long, C.c_int, C.POINTER(P)]
         L.hbp_lab_d.argtypes = [P, P, C.c_long, P, P]
+        L.hbp_request_bytes.restype = C.c_size_t
+        L.hbp_server_create.argtypes = [C.c_int, C.c_size_t, C.c_int, P, C.POINTER(P)]
+        L.hbp_server_destroy.argtypes = [P]
+        L.hbp_submit.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, P, C.POINTER(C.c_longlong)]
+        L.hbp_poll.argtypes = [P, C.c_longlong]
+        L.hbp_wait.argtypes = [P, C.c_longlong, C.c_double, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -188,3 +194,60 @@ class Context:
 
     def driver_median_d(self, disp, W, H):
         _check(lib().hbp_driver_median_d(self.h, _p(disp), W, H, None))
+
+
+def request_bytes(W: int, H: int, D: int) -> int:
+    """Device footprint the server admits a W x H x D pair by."""
+    return lib().hbp_request_bytes(W, H, D)
+
+
+class Server:
+    """hbp_server: continuous-batching request server on one GPU. submit()
+    takes host arrays (kept referenced until wait() returns) and returns a
+    request id; wait() returns (disparity, latency_ms)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 120 << 30, prep_lanes: int = 4,
+                 params: Params | None = None):
+        h = P()
+        prm = params or default_params(post=1)
+        _check(lib().hbp_server_create(device, budget_bytes, prep_lanes, C.byref(prm), C.byref(h)))
+        self.h = h
+        self._live = {}
+
+    def submit(self, left: np.ndarray, right: np.ndarray, D: int) -> int:
+        left = np.ascontiguousarray(left, np.uint8)
+        right = np.ascontiguousarray(right, np.uint8)
+        H, W = left.shape[:2]
+        out = np.zeros((H, W), np.float32)
+        rid = C.c_longlong(0)
+        _check(lib().hbp_submit(self.h, _p(left), _p(right), W, H, D, _p(out), C.byref(rid)))
+        self._live[rid.value] = (left, right, out)
+        return rid.value
+
+    def poll(self, rid: int) -> bool:
+        st = lib().hbp_poll(self.h, rid)
+        if st == 7:
+            return False
+        _check(st)
+        return True
+
+    def wait(self, rid: int, timeout_ms: float = -1.0):
+        lat = C.c_double(0)
+        st = lib().hbp_wait(self.h, rid, timeout_ms, C.byref(lat))
+        if st == 6:  # still running: keep the buffers
+            _check(st)
+        _, _, out = self._live.pop(rid)
+        _check(st)
+        return out, lat.value
+
+    def close(self):
+        if self.h:
+            lib().hbp_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -166,6 +166,36 @@ hbp_status hbp_run_batch_d(hbp_ctx *ctx, int npairs, const uint8_t *const *bgrL,
 
 hbp_status hbp_set_lanes(hbp_ctx *ctx, int lanes);
 
+/* ------------------------------------------------------------ serving */
+
+/* A request server on one GPU (no reference counterpart: the reference runs
+ * one pair per process). Pairs of any size and disparity range are submitted
+ * from host buffers and run with continuous batching: a request is admitted
+ * when its device footprint (hbp_request_bytes) fits in the budget beside the
+ * requests in flight, prepared (upload, cost volume, pyramid, BP setup) by one
+ * of prep_lanes host threads on its own stream, and joins the BP of the pairs
+ * already running at the next BP step; it leaves after its MAP and the
+ * driver's median. Each result equals hbp_run_pair's (post 1) bit for bit,
+ * whatever runs beside it. prm applies to every request (post 0 or 1).
+ * The budget counts the pairs' device slabs; the preparation lanes' scratch
+ * (about 480 B per pixel of the largest pair, + 64 MB, per lane) comes on top.
+ * All functions are thread safe. Input and output buffers must stay valid
+ * until hbp_wait returns for the request. */
+typedef struct hbp_server hbp_server;
+size_t hbp_request_bytes(int W, int H, int D);
+hbp_status hbp_server_create(int device, size_t budget_bytes, int prep_lanes, const hbp_params *prm,
+                             hbp_server **out);
+/* Finishes the admitted requests, drops the queued ones, frees everything. */
+void hbp_server_destroy(hbp_server *srv);
+/* HBP_ERR_ADMISSION_REJECTED when the pair can never fit in the budget. */
+hbp_status hbp_submit(hbp_server *srv, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
+                      float *disp, long long *request_id);
+/* HBP_ERR_NOT_READY while running; otherwise the request's final status. */
+hbp_status hbp_poll(hbp_server *srv, long long request_id);
+/* Waits (timeout_ms < 0: without limit; HBP_ERR_TIMEOUT when it runs out),
+ * reports submit-to-result latency, and forgets the request. */
+hbp_status hbp_wait(hbp_server *srv, long long request_id, double timeout_ms, double *latency_ms);
+
 /* -------------------------------------------------------- measurement */
 
 /* Number of kernels the library has launched since it was loaded. */

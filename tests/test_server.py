@@ -1,0 +1,86 @@
+"""Request server (continuous batching): every result equals the single-pair
+path's bit for bit, alone and in a mix of sizes running together; admission
+by device footprint. GPU tests, plus argument checks that need no GPU."""
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import hbp_b200 as E
+    return E
+
+
+MIX = [(160, 120, 48, 21), (96, 64, 32, 22), (450, 375, 64, 23), (320, 240, 64, 24), (160, 120, 48, 25),
+       (200, 150, 40, 26)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp16", [0, 1])
+def test_results_alone_and_in_a_mix_equal_run_pair(gpu, fp16):
+    E = gpu
+    from scenes import make_scene
+    scenes = [make_scene(W, H, D, seed) for W, H, D, seed in MIX]
+    prm = E.default_params(post=1, msg_fp16=fp16)
+    ctx = E.Context(0)
+    try:
+        want = [ctx.run_pair(s.left, s.right, D, prm) for s, (_, _, D, _) in zip(scenes, MIX)]
+    finally:
+        ctx.close()
+    srv = E.Server(0, budget_bytes=16 << 30, prep_lanes=3, params=prm)
+    try:
+        # alone
+        rid = srv.submit(scenes[2].left, scenes[2].right, MIX[2][2])
+        alone, lat = srv.wait(rid)
+        assert lat > 0
+        assert np.array_equal(alone.view(np.uint32), want[2].view(np.uint32))
+        # all at once: they join the BP of those already running
+        ids = [srv.submit(s.left, s.right, D) for s, (_, _, D, _) in zip(scenes, MIX)]
+        for rid, w in zip(ids, want):
+            got, _ = srv.wait(rid)
+            assert np.array_equal(got.view(np.uint32), w.view(np.uint32))
+    finally:
+        srv.close()
+
+
+@pytest.mark.gpu
+def test_admission_by_footprint(gpu):
+    E = gpu
+    from scenes import make_scene
+    need = E.request_bytes(160, 120, 48)
+    prm = E.default_params(post=1)
+    srv = E.Server(0, budget_bytes=need + need // 2, prep_lanes=2, params=prm)  # one pair at a time
+    try:
+        with pytest.raises(E.HbpError) as ei:
+            s = make_scene(320, 240, 64, 1)
+            srv.submit(s.left, s.right, 64)
+        assert ei.value.status == 3  # admission rejected: can never fit
+        scenes = [make_scene(160, 120, 48, 30 + i) for i in range(4)]
+        ids = [srv.submit(s.left, s.right, 48) for s in scenes]
+        outs = [srv.wait(i)[0] for i in ids]
+    finally:
+        srv.close()
+    ctx = E.Context(0)
+    try:
+        for s, o in zip(scenes, outs):
+            assert np.array_equal(o, ctx.run_pair(s.left, s.right, 48, prm))
+    finally:
+        ctx.close()
+
+
+def test_server_arguments_checked_without_gpu():
+    import ctypes as C
+    import build as engine_build
+    engine_build.build()
+    import hbp_b200 as E
+    L = E.lib()
+    h = C.c_void_p()
+    assert L.hbp_server_create(0, 0, 2, None, C.byref(h)) == 1  # no budget
+    assert L.hbp_server_create(0, 1 << 30, 0, None, C.byref(h)) == 1  # no lanes
+    p = E.default_params(post=2)
+    assert L.hbp_server_create(0, 1 << 30, 2, C.byref(p), C.byref(h)) == 1  # LR post not served
+    assert E.request_bytes(720, 496, 128) > 720 * 496 * 128
+    assert L.hbp_poll(None, 1) == 1
