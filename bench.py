@@ -9,14 +9,18 @@ rectified pairs of 720x496 with D = 128: the quarter-scale batch workload.
 The scenes are seeded piecewise-planar synthetic pairs standing in for the
 Middlebury images the reference benchmarks on (data: "synthetic").
 
-One JSON line on rank 0:
+One JSON line on rank 0 (BP messages stored as FP16 unless --fp16 0):
   value       pairs/s with the pairs already in device memory (hbp_run_batch_d)
-  e2e         pairs/s through hbp_run_pair on pinned host buffers (uploads the
-              pair and downloads the disparity inside the timed region), with
-              per-pair p50/p99 latency
+  e2e         pairs/s served through the request server's C API (hbp_submit /
+              hbp_wait) from pinned host buffers, 16 requests in flight: upload,
+              whole path and download of each disparity inside the timed region
+  latency_ms  p50/p99 of the served requests (submit to result in host memory)
+  plain_fp32  the plain FP32 single-pair path (hbp_run_pair, one pair at a
+              time) on the same pairs: pairs/s and p50/p99
   roofline    the data-cost kernel (the dominant kernel): algorithmic bytes of
-              its launches / their CUDA-event time over the timed region
-              (first pair of every batch), against the measured HBM copy peak
+              its launches / their CUDA-event time over the timed region,
+              against the measured HBM copy peak; traffic from the committed
+              ncu capture, scaled to a 16-view launch
   cpu_baseline the CPU oracle (a port of the reference path, all host cores) on
               one pair of the same workload
   gpu_launches kernels this library launched inside the timed region
@@ -56,7 +60,7 @@ def parse():
     ap.add_argument("--W", type=int, default=720)
     ap.add_argument("--H", type=int, default=496)
     ap.add_argument("--D", type=int, default=128)
-    ap.add_argument("--fp16", type=int, default=0, help="store BP messages as FP16")
+    ap.add_argument("--fp16", type=int, default=1, help="store BP messages as FP16 (1) or FP32 (0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--breakdown", action="store_true",
@@ -313,28 +317,56 @@ def main():
         print(json.dumps(breakdown(E, ctx, step)), file=sys.stderr)
 
     # ------------------------------------------------------------ end to end
+    # Served: the same pairs through the request server's C API from pinned
+    # host buffers (upload, whole path, download of the disparity inside the
+    # timed region), a closed loop keeping NP requests in flight.
     e2e = None
     lat = []
+    plain = None
     if not args.no_e2e:
-        pinL = [torch.from_numpy(s.left).pin_memory() for s in scenes]
-        pinR = [torch.from_numpy(s.right).pin_memory() for s in scenes]
-        out = torch.empty((H, W), dtype=torch.float32).pin_memory()
-        ctx.run_pair(pinL[0].numpy(), pinR[0].numpy(), D, prm)  # warm
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for k in range(args.steps):
-            for i in range(NP):
-                a = time.perf_counter()
-                E._check(E.lib().hbp_run_pair(ctx.h, C.c_void_p(pinL[i].data_ptr()), C.c_void_p(pinR[i].data_ptr()),
-                                              W, H, D, C.byref(prm), C.c_void_p(out.data_ptr()), None))
-                lat.append((time.perf_counter() - a) * 1e3)
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
+        pinL = [torch.from_numpy(s.left).pin_memory().numpy() for s in scenes]
+        pinR = [torch.from_numpy(s.right).pin_memory().numpy() for s in scenes]
+        srv = E.Server(local, budget_bytes=120 << 30, prep_lanes=8, params=prm)
+        try:
+            ids = [srv.submit(pinL[i], pinR[i], D) for i in range(NP)]  # warm-up
+            for i in ids:
+                srv.wait(i)
+            if dist:
+                dist.barrier()
+            n_req = NP * args.steps
+            t0 = time.perf_counter()
+            inflight = []
+            for k in range(n_req):
+                if len(inflight) == NP:
+                    lat.append(srv.wait(inflight.pop(0))[1])
+                inflight.append(srv.submit(pinL[k % NP], pinR[k % NP], D))
+            for i in inflight:
+                lat.append(srv.wait(i)[1])
+            el = time.perf_counter() - t0
+        finally:
+            srv.close()
         el = max_over_ranks(el, dist, "cuda")
         e2e = {"value": whole_job_rate(NP, args.steps, world, el), "unit": "pairs/s",
-               "h2d_bytes_per_step": NP * 2 * 3 * W * H, "d2h_bytes_per_step": NP * 4 * W * H}
+               "h2d_bytes_per_step": NP * 2 * 3 * W * H, "d2h_bytes_per_step": NP * 4 * W * H,
+               "path": f"hbp_submit/hbp_wait, {NP} requests in flight, messages "
+                       + ("fp16" if args.fp16 else "fp32")}
+        # the plain FP32 single-pair path (hbp_run_pair, one pair at a time)
+        prm32 = E.default_params(msg_fp16=0, post=1)
+        out = np.zeros((H, W), np.float32)
+        ctx.run_pair(pinL[0], pinR[0], D, prm32)
+        plat = []
+        t0 = time.perf_counter()
+        for k in range(NP):
+            a = time.perf_counter()
+            E._check(E.lib().hbp_run_pair(ctx.h, pinL[k].ctypes.data_as(C.c_void_p),
+                                          pinR[k].ctypes.data_as(C.c_void_p), W, H, D, C.byref(prm32),
+                                          out.ctypes.data_as(C.c_void_p), None))
+            plat.append((time.perf_counter() - a) * 1e3)
+        pel = time.perf_counter() - t0
+        plat.sort()
+        plain = {"value": NP / pel, "unit": "pairs/s", "p50_ms": plat[len(plat) // 2],
+                 "p99_ms": plat[min(len(plat) - 1, int(0.99 * len(plat)))],
+                 "path": "hbp_run_pair, FP32 messages, one pair at a time, pinned host buffers"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -363,7 +395,9 @@ def main():
                        "msg": "fp16" if args.fp16 else "fp32", "parallelism": f"replicas x{world}",
                        "l2": "256 MiB buffer written between timed steps"},
             "latency_ms": {"p50": lat[len(lat) // 2] if lat else None,
-                           "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None},
+                           "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None,
+                           "of": "served requests, submit to result in host memory"},
+            "plain_fp32": plain,
             "roofline": {"kernel": "plane_cost_kernel (data cost of 4 candidate planes per pixel)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
