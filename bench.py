@@ -313,6 +313,23 @@ def main():
     t_max = max_over_ranks(ms, dist, "cuda")
     value = whole_job_rate(NP, args.steps, world, t_max / 1e3)
 
+    # accuracy of the FP16 messages at this workload: the same batch with FP32
+    # messages, pixel agreement and bad-2.0 against the generator's ground truth
+    accuracy = None
+    if args.fp16 and rank == 0:
+        prm32 = E.default_params(msg_fp16=0, post=1)
+        d16 = [t.cpu().numpy() for t in disp]
+        E._check(E.lib().hbp_run_batch_d(ctx.h, NP, arrL, arrR, W, H, D, C.byref(prm32), arrD, None))
+        torch.cuda.synchronize()
+        d32 = [t.cpu().numpy() for t in disp]
+        bad2 = lambda d, s: 100.0 * float(np.mean(np.abs(d - s.gt)[s.nonocc] > 2.0))
+        same = [float(np.mean(a == b)) for a, b in zip(d16, d32)]
+        accuracy = {"fp16_vs_fp32_identical_mean": float(np.mean(same)),
+                    "fp16_vs_fp32_identical_min": float(np.min(same)),
+                    "bad2_fp32_pct": float(np.mean([bad2(d, s) for d, s in zip(d32, scenes)])),
+                    "bad2_fp16_pct": float(np.mean([bad2(d, s) for d, s in zip(d16, scenes)])),
+                    "pairs": NP}
+
     if args.breakdown and rank == 0:
         print(json.dumps(breakdown(E, ctx, step)), file=sys.stderr)
 
@@ -398,6 +415,7 @@ def main():
                            "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None,
                            "of": "served requests, submit to result in host memory"},
             "plain_fp32": plain,
+            "accuracy": accuracy,
             "roofline": {"kernel": "plane_cost_kernel (data cost of 4 candidate planes per pixel)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,

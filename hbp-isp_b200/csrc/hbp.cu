@@ -19,8 +19,10 @@
 // plane costs by the segmented-scan order described at k_cost; beliefs =
 // cost + out-edge messages in edge order.
 // Everything else follows the reference operation for operation; this file is
-// compiled without multiply-add contraction so that each a*b+c rounds twice
-// like the CPU oracle.
+// compiled without multiply-add contraction, so each a*b+c rounds twice like
+// the CPU oracle except where a fused multiply-add is written out
+// (__fmaf_rn: the data cost's plane evaluation and interpolation, the
+// smoothness term and the message sum).
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
@@ -70,7 +72,7 @@ __device__ __forceinline__ int px_y(uint32_t xy) { return (int)(xy >> 16); }
 // read_plane_cost (hbp_isp.cu:205-227) for one pixel and one plane.
 __device__ __forceinline__ float pixel_cost(const Common &c, int x, int y, float4 pl)
 {
-    float d_f = (pl.x * (float)x + pl.y * (float)y) + pl.z;
+    float d_f = __fmaf_rn(pl.x, (float)x, __fmaf_rn(pl.y, (float)y, pl.z));
     int d = __float2int_rd(d_f);
     float cost;
     if (d < 0 || d >= c.D - 1)
@@ -80,7 +82,7 @@ __device__ __forceinline__ float pixel_cost(const Common &c, int x, int y, float
         const uint8_t *pv = c.vol + vol_offset(x, y, d, c.TX, c.D);
         float v0 = (float)pv[0];
         float v1 = (float)pv[VT_BYTES];
-        cost = ((float)(d + 1) - d_f) * v0 + (d_f - (float)d) * v1;
+        cost = __fmaf_rn((float)(d + 1) - d_f, v0, (d_f - (float)d) * v1);
     }
     return c.lambda * cost;
 }
@@ -275,6 +277,38 @@ __device__ __forceinline__ int find_task(const StepDesc &d, int item)
 // hbp_isp.cu:405-417, :432-472): belief = cost + out-edge messages in edge
 // order; a slot's rank counts the slots that beat it (a later slot loses
 // ties); slots ranked < P move to the front in slot order, in place.
+// S3 of the data-cost order: a node's chunk sums c0..c1-1 added in order;
+// the loads are issued 8 at a time (the additions stay sequential).
+__device__ __forceinline__ float4 sum_chunks(const float4 *pc, int c0, int c1)
+{
+    float4 a = pc[c0];
+    int ch = c0 + 1;
+    for (; ch + 8 <= c1; ch += 8)
+    {
+        float4 q[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            q[j] = pc[ch + j];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+        {
+            a.x = a.x + q[j].x;
+            a.y = a.y + q[j].y;
+            a.z = a.z + q[j].z;
+            a.w = a.w + q[j].w;
+        }
+    }
+    for (; ch < c1; ++ch)
+    {
+        const float4 q = pc[ch];
+        a.x = a.x + q.x;
+        a.y = a.y + q.y;
+        a.z = a.z + q.z;
+        a.w = a.w + q.w;
+    }
+    return a;
+}
+
 // msg_t[e][0..11] of buffer `buf` as floats. FP16 storage holds each value
 // rounded to nearest; the arithmetic on messages is FP32 either way.
 __device__ __forceinline__ void load_msg(const ViewBufs &b, int buf, size_t e, float v[K])
@@ -340,16 +374,7 @@ __device__ __forceinline__ void select_thread(const LevelDev &l, int n, const fl
     for (int k = 0; k < 2 * P; ++k)
         cs[k] = cst[k];
     {
-        int c0 = l.chunk_off[n], c1 = l.chunk_off[n + 1];
-        float4 a = pc[c0];
-        for (int ch = c0 + 1; ch < c1; ++ch)
-        {
-            float4 q = pc[ch];
-            a.x = a.x + q.x;
-            a.y = a.y + q.y;
-            a.z = a.z + q.z;
-            a.w = a.w + q.w;
-        }
+        const float4 a = sum_chunks(pc, l.chunk_off[n], l.chunk_off[n + 1]);
         cs[8] = a.x;
         cs[9] = a.y;
         cs[10] = a.z;
@@ -358,7 +383,22 @@ __device__ __forceinline__ void select_thread(const LevelDev &l, int n, const fl
 #pragma unroll
     for (int k = 0; k < K; ++k)
         b[k] = cs[k];
-    for (int e = l.nb_off[n]; e < l.nb_off[n + 1]; ++e)
+    // out-edge messages in edge order; loads issued 4 edges at a time
+    const int e0 = l.nb_off[n], e1 = l.nb_off[n + 1];
+    int e = e0;
+    for (; e + 4 <= e1; e += 4)
+    {
+        float m[4][K];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            load_msg(vb, mbuf, (size_t)(e + j), m[j]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                b[k] = b[k] + m[j][k];
+    }
+    for (; e < e1; ++e)
     {
         float m[K];
         load_msg(vb, mbuf, (size_t)e, m);
@@ -719,17 +759,7 @@ __global__ void __launch_bounds__(128) k_init_nodes(const ViewDev *__restrict__ 
     int n = item - d.pre[ti];
     if (n < l.N)
     {
-        int c0 = l.chunk_off[n], c1 = l.chunk_off[n + 1];
-        const float4 *pc = v.b.pc[t.pb];
-        float4 a = pc[c0];
-        for (int ch = c0 + 1; ch < c1; ++ch)
-        {
-            float4 q = pc[ch];
-            a.x = a.x + q.x;
-            a.y = a.y + q.y;
-            a.z = a.z + q.z;
-            a.w = a.w + q.w;
-        }
+        const float4 a = sum_chunks(v.b.pc[t.pb], l.chunk_off[n], l.chunk_off[n + 1]);
         float *cs = l.cost + (size_t)n * K;
         float *bl = l.belief + (size_t)n * K;
         cs[0] = cs[4] = a.x;
@@ -838,14 +868,13 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
     // reciprocals: qa is within 4 ulp of q, so qa * (1 - 2^-20) <= q (tiny
     // or NaN qa -> bound 0). Rounding is monotone, so with the bound qlb:
     // qlb >= tau_smooth means min(q, tau_smooth) == tau_smooth exactly, and
-    // mp + c0 * qlb >= the running minimum means the label cannot lower it.
+    // fma(c0, qlb, mp) >= the running minimum means the label cannot lower it.
     // Only the remaining labels need the exact divisions. Every label's phi
     // is evaluated (uniform across the warp); a label skipped this way or
     // with mp >= the minimum leaves the minimum unchanged, as does a NaN.
     const float tau = c.tau_smooth;
     const float inv_dp = 1.0f / dist_pos;
     const float inv3 = 1.0f / 3.0f;
-    const float ct = c0 * tau;
     __shared__ float s_out[K][128];
     float sum = 0.f;
 #pragma unroll 1
@@ -863,17 +892,17 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
                 const int q = g * P + k;
                 const float4 tp = pt[q];
                 float dx = ps.x - tp.x, dy = ps.y - tp.y, dz = ps.z - tp.z;
-                float phi = fabsf(dx * X[0] + dy * Y[0] + dz);
+                float phi = fabsf(__fmaf_rn(dx, X[0], __fmaf_rn(dy, Y[0], dz)));
 #pragma unroll
                 for (int i = 1; i < 6; ++i)
-                    phi = phi + fabsf(dx * X[i] + dy * Y[i] + dz);
+                    phi = phi + fabsf(__fmaf_rn(dx, X[i], __fmaf_rn(dy, Y[i], dz)));
                 const float qa = phi * inv3 * inv_dp;
                 const float qlb = qa >= 1e-30f ? qa * 0.99999905f : 0.0f; // 1 - 2^-20
                 float m;
                 if (qlb >= tau)
-                    m = mp[q] + ct;
-                else if (k == 0 || mp[q] + c0 * qlb < mn)
-                    m = mp[q] + c0 * fminf(phi / 3.0f / dist_pos, tau);
+                    m = __fmaf_rn(c0, tau, mp[q]);
+                else if (k == 0 || __fmaf_rn(c0, qlb, mp[q]) < mn)
+                    m = __fmaf_rn(c0, fminf(phi / 3.0f / dist_pos, tau), mp[q]);
                 else
                     m = mn;
                 if (m < mn)

@@ -17,6 +17,11 @@
 //   S3 the 256-window sums are added in order.
 //   belief[k][s] = cost[k][s] + msg_t of s's out-edges in edge order.
 //   dc colour term: (|dL| + |da|) + |db|; position term: dx*dx + dy*dy.
+// Fused multiply-adds (the reference's nvcc build contracts these expressions,
+// in an order its output does not pin down; HBP agreement with it is the same
+// for every order tried): data cost d = fma(a, x, fma(b, y, c)) and
+// cost = fma(d + 1 - d_f, V[d], (d_f - d) * V[d+1]); smoothness point term
+// |fma(dx, X, fma(dy, Y, dz))| and message fma(c0, phi, msg).
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
@@ -76,7 +81,7 @@ struct Engine
     R pixel_cost(int px, const P4<R> &pl) const
     {
         R x = (R)(px % W), y = (R)(px / W);
-        R d_f = pl.x * x + pl.y * y + pl.z;
+        R d_f = std::fma(pl.x, x, std::fma(pl.y, y, pl.z));
         int d = f2i_rd((float)d_f);
         if (sizeof(R) == 8)
         {
@@ -91,7 +96,7 @@ struct Engine
         {
             const size_t n = (size_t)W * H;
             R v0 = (R)vol[(size_t)d * n + px], v1 = (R)vol[(size_t)(d + 1) * n + px];
-            cost = ((R)(d + 1) - d_f) * v0 + (d_f - (R)d) * v1;
+            cost = std::fma((R)(d + 1) - d_f, v0, (d_f - (R)d) * v1);
         }
         return lambda * cost;
     }
@@ -304,11 +309,11 @@ struct Engine
                     R phi = 0;
                     for (int i = 0; i < 6; ++i)
                     {
-                        R term = std::fabs(dx * X[i] + dy * Y[i] + dz);
+                        R term = std::fabs(std::fma(dx, X[i], std::fma(dy, Y[i], dz)));
                         phi = i == 0 ? term : phi + term;
                     }
                     phi = std::fmin(phi / (R)3 / dist_pos, tau_smooth);
-                    R m = msg[(size_t)p * E + e] + c0 * phi;
+                    R m = std::fma(c0, phi, msg[(size_t)p * E + e]);
                     if (m < mn)
                         mn = m;
                 }

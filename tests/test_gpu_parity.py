@@ -224,14 +224,18 @@ def test_fp16_messages_match_oracle(eng, golden_dir, name):
 
 def test_fp16_messages_agree_with_fp32(eng):
     """FP16 messages against the FP32 path on the single-pair workload
-    (450x375, D 64): at least 99.9% of pixels identical, and bad-2.0 against
-    the generator's ground truth within 0.1 percentage point."""
+    (450x375, D 64), four scenes: on average at least 99.9% of pixels
+    identical (each scene at least 99.8%: a flipped slot choice moves a whole
+    superpixel), and bad-2.0 against the generator's ground truth within
+    0.1 percentage point per scene."""
     E, ctx, torch = eng
     from scenes import make_scene
-    for seed in (1000, 1001):
+    same = []
+    for seed in (1000, 1001, 1002, 1003):
         s = make_scene(450, 375, 64, seed)
         d32 = ctx.run_pair(s.left, s.right, 64, E.default_params(post=1))
         d16 = ctx.run_pair(s.left, s.right, 64, E.default_params(post=1, msg_fp16=1))
-        assert np.mean(d16 == d32) >= 0.999
+        same.append(float(np.mean(d16 == d32)))
         bad = lambda d: 100.0 * float(np.mean(np.abs(d - s.gt)[s.nonocc] > 2.0))
         assert abs(bad(d16) - bad(d32)) <= 0.1
+    assert min(same) >= 0.998 and np.mean(same) >= 0.999, same
