@@ -69,20 +69,30 @@ struct Common
 __device__ __forceinline__ int px_x(uint32_t xy) { return (int)(xy & 0xffffu); }
 __device__ __forceinline__ int px_y(uint32_t xy) { return (int)(xy >> 16); }
 
-// read_plane_cost (hbp_isp.cu:205-227) for one pixel and one plane.
-__device__ __forceinline__ float pixel_cost(const Common &c, int x, int y, float4 pl)
+// A byte as float without the conversion pipe: the bits 0x4B000000 | v are
+// the float 2^23 + v, so subtracting 2^23 gives v exactly.
+__device__ __forceinline__ float byte_to_float(uint32_t v)
 {
-    float d_f = __fmaf_rn(pl.x, (float)x, __fmaf_rn(pl.y, (float)y, pl.z));
+    return __uint_as_float(0x4B000000u | v) - 8388608.0f;
+}
+
+// read_plane_cost (hbp_isp.cu:205-227) for one pixel (xf, yf = its
+// coordinates as floats, base = vol_tile_base) and one plane. For d in
+// [0, D-1), (float)(d + 1) == (float)d + 1 exactly.
+__device__ __forceinline__ float pixel_cost(const Common &c, float xf, float yf, size_t base, float4 pl)
+{
+    float d_f = __fmaf_rn(pl.x, xf, __fmaf_rn(pl.y, yf, pl.z));
     int d = __float2int_rd(d_f);
     float cost;
     if (d < 0 || d >= c.D - 1)
         cost = c.tau;
     else
     {
-        const uint8_t *pv = c.vol + vol_offset(x, y, d, c.TX, c.D);
-        float v0 = (float)pv[0];
-        float v1 = (float)pv[VT_BYTES];
-        cost = __fmaf_rn((float)(d + 1) - d_f, v0, (d_f - (float)d) * v1);
+        const uint8_t *pv = c.vol + base + (size_t)d * VT_BYTES;
+        const float v0 = byte_to_float(pv[0]);
+        const float v1 = byte_to_float(pv[VT_BYTES]);
+        const float fd = (float)d;
+        cost = __fmaf_rn((fd + 1.0f) - d_f, v0, (d_f - fd) * v1);
     }
     return c.lambda * cost;
 }
@@ -625,9 +635,11 @@ enum CostMode
 // Data cost of 4 planes (read_plane_cost for every pixel, hbp_isp.cu:205-227,
 // and the per-node sum of compute_plane_cost, :1159-1174). One warp = one
 // 256-position window of the level's pixel list (sorted by node, raster order
-// inside a node), walked as 8 sub-windows of 32 positions, one per lane. The
-// node sum is taken in a fixed order (the reference's float atomics have
-// none; the CPU oracle restates it):
+// inside a node). The node sum is taken in a fixed order (the reference's
+// float atomics have none; the CPU oracle restates it):
+//   S0 a window that one node fills: lane j sums positions j, j+32, ...,
+//      j+224 in order, then an xor butterfly (offsets 16..1) over the lanes;
+// any other window is walked as 8 sub-windows of 32 positions, one per lane:
 //   S1 inside each 32-position sub-window the pixels of one node form a
 //      segment, summed by a segmented Hillis-Steele scan: for off = 1, 2, 4,
 //      8, 16, x[r] = x[r - off] + x[r] where r - off is still in the segment;
@@ -640,7 +652,7 @@ __device__ __forceinline__ void emit_chunk(const LevelDev &l, float4 *pc, int n,
     pc[l.chunk_off[n] + win - l.pix_off[n] / PC_CHUNK] = v;
 }
 
-__global__ void __launch_bounds__(256) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
+__global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
 {
     const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -654,6 +666,63 @@ __global__ void __launch_bounds__(256) k_cost(const ViewDev *__restrict__ V, Ste
     const int HW = c.W * c.H, N = l.N;
     const int win = item - d.pre[ti];
     float4 *pc = v.b.pc[t.pb];
+    // S0: a window that one node fills entirely
+    if ((win + 1) * PC_CHUNK <= HW)
+    {
+        const int q0 = win * PC_CHUNK;
+        const int n0 = l.pnode[q0];
+        const int b0 = l.pix_off[n0];
+        if (b0 <= q0 && l.pix_off[n0 + 1] >= q0 + PC_CHUNK) // warp-uniform
+        {
+            float4 pl[4];
+            if (mode == COST_INIT)
+            {
+                const int pn = l.clus[n0];
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+                    pl[p] = t.lvh->plane[(size_t)pn * K + p];
+                if (lane == 0 && b0 == q0) // the node's first pixel
+                {
+                    for (int k = 0; k < K; ++k)
+                        l.plane[(size_t)n0 * K + k] = pl[k % P];
+                    v.b.s_nb[n0] = (uint32_t)l.nb_off[n0];
+                    v.b.s_ransac[t.rb][n0] = (uint32_t)q0;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+                    pl[p] = l.plane[(size_t)n0 * K + 2 * P + p];
+            }
+            uint32_t xy[PC_CHUNK / 32];
+#pragma unroll
+            for (int k = 0; k < PC_CHUNK / 32; ++k)
+                xy[k] = l.pix[q0 + lane + 32 * k];
+            float a[4];
+#pragma unroll
+            for (int k = 0; k < PC_CHUNK / 32; ++k)
+            {
+                const int x = px_x(xy[k]), y = px_y(xy[k]);
+                const float xf = (float)x, yf = (float)y;
+                const size_t base = vol_tile_base(x, y, c.TX, c.D);
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+                {
+                    const float cv = pixel_cost(c, xf, yf, base, pl[p]);
+                    a[p] = k == 0 ? cv : a[p] + cv;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+                    a[p] = a[p] + __shfl_xor_sync(0xffffffffu, a[p], off);
+            if (lane == 0)
+                emit_chunk(l, pc, n0, win, make_float4(a[0], a[1], a[2], a[3]));
+            return;
+        }
+    }
     const unsigned upto = 0xffffffffu >> (31 - lane); // lanes 0..lane
     int carry_n = -1;
     float4 carry = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -711,9 +780,11 @@ __global__ void __launch_bounds__(256) k_cost(const ViewDev *__restrict__ V, Ste
                     pl[p] = l.plane[(size_t)n * K + 2 * P + p];
             }
             const int x = px_x(xy), y = px_y(xy);
+            const float xf = (float)x, yf = (float)y;
+            const size_t base = vol_tile_base(x, y, c.TX, c.D);
 #pragma unroll
             for (int p = 0; p < 4; ++p)
-                cc[p] = pixel_cost(c, x, y, pl[p]);
+                cc[p] = pixel_cost(c, xf, yf, base, pl[p]);
         }
         // S1
 #pragma unroll
@@ -787,7 +858,9 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
     const Common &c = v.c;
     const int e = item - d.pre[ti];
     int2 st = l.bd[e];
-    int4 ps4 = l.pid[st.x], pt4 = l.pid[st.y];
+    // the six points, lower-index node's three first (the same order for an
+    // edge and its reverse)
+    int4 ps4 = l.pid[min(st.x, st.y)], pt4 = l.pid[max(st.x, st.y)];
     uint32_t pts[6] = {(uint32_t)ps4.x, (uint32_t)ps4.y, (uint32_t)ps4.z,
                        (uint32_t)pt4.x, (uint32_t)pt4.y, (uint32_t)pt4.z};
     float X[6], Y[6];

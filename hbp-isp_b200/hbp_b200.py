@@ -13,7 +13,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libhbp_b200.so")
+LIB_PATH = os.environ.get("HBP_B200_LIB") or os.path.join(HERE, "lib", "libhbp_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "hbp_b200.h")
 
 P = C.c_void_p

@@ -59,6 +59,24 @@ inline float fmax_cuda(float a, float b) { return std::fmax(a, b); }
 // v[0..n) are laid out round-robin over 32 slots (slot j accumulates v[j],
 // v[j+32], ... sequentially from 0), then the slots are combined by an xor
 // butterfly with offsets 16, 8, 4, 2, 1 (slot i += slot i^off).
+// xor butterfly over 32 slots (offsets 16, 8, 4, 2, 1; a[i] = a[i] + a[i^off]),
+// the value of slot 0.
+template <typename R>
+inline R butterfly32(const R *slots)
+{
+    R a[32];
+    for (int i = 0; i < 32; ++i)
+        a[i] = slots[i];
+    for (int off = 16; off >= 1; off >>= 1)
+    {
+        R b[32];
+        for (int i = 0; i < 32; ++i)
+            b[i] = a[i] + a[i ^ off];
+        std::memcpy(a, b, sizeof(a));
+    }
+    return a[0];
+}
+
 // Last element of the Hillis-Steele inclusive scan of x[0..m) (m <= 32):
 // for off = 1, 2, 4, 8, 16: x[r] = x[r - off] + x[r] for r >= off.
 template <typename R>

@@ -9,7 +9,11 @@
 // Reduction orders fixed by the engine (the reference uses float atomics and
 // Thrust reduce_by_key, whose order is unspecified):
 //   plane cost of node n, candidate k, over the level's pixel list (sorted by
-//   node, raster order inside a node; list positions are absolute):
+//   node, raster order inside a node; list positions are absolute), cut into
+//   256-position chunks:
+//   S0 a chunk the node fills entirely: slot j = positions j, j+32, ...,
+//      j+224 added in order, the 32 slots combined by the xor butterfly of
+//      orc::butterfly32 (offsets 16..1); other chunks by S1 and S2:
 //   S1 the node's positions inside one 32-position window are summed by a
 //      Hillis-Steele inclusive scan (off = 1..16: x[r] = x[r-off] + x[r] for
 //      r >= off), taking its last element;
@@ -17,6 +21,8 @@
 //   S3 the 256-window sums are added in order.
 //   belief[k][s] = cost[k][s] + msg_t of s's out-edges in edge order.
 //   dc colour term: (|dL| + |da|) + |db|; position term: dx*dx + dy*dy.
+// Smoothness points: the lower-index node's three points, then the other's
+// (the reference takes the source's first; the order only moves roundings).
 // Fused multiply-adds (the reference's nvcc build contracts these expressions,
 // in an order its output does not pin down; HBP agreement with it is the same
 // for every order tried): data cost d = fma(a, x, fma(b, y, c)) and
@@ -117,6 +123,22 @@ struct Engine
                 {
                     const int lo = std::max(b, w256 * CHUNK), hi = std::min(e, (w256 + 1) * CHUNK);
                     R acc = 0;
+                    if (lo == w256 * CHUNK && hi == (w256 + 1) * CHUNK)
+                    {
+                        // the node fills the chunk: slot j sums positions
+                        // j, j+32, ..., j+224 in order; xor butterfly
+                        R slots[32];
+                        for (int j = 0; j < 32; ++j)
+                        {
+                            R a = pixel_cost(l.pix[lo + j], pl);
+                            for (int k = 1; k < CHUNK / 32; ++k)
+                                a = a + pixel_cost(l.pix[lo + j + 32 * k], pl);
+                            slots[j] = a;
+                        }
+                        acc = butterfly32(slots);
+                        total = w256 == b / CHUNK ? acc : total + acc;
+                        continue;
+                    }
                     for (int w32 = lo / 32; w32 <= (hi - 1) / 32; ++w32)
                     {
                         const int l2 = std::max(lo, w32 * 32), h2 = std::min(hi, (w32 + 1) * 32);
@@ -280,10 +302,14 @@ struct Engine
         for (int e = 0; e < E; ++e)
         {
             int s = l.bd[2 * (size_t)e], t = l.bd[2 * (size_t)e + 1];
+            // the six points in a fixed order for both directions of an edge:
+            // the lower-index node's three, then the other's (the message of
+            // an edge and of its reverse then share each plane distance)
+            const int lo = std::min(s, t), hi = std::max(s, t);
             R X[6], Y[6];
             for (int i = 0; i < 3; ++i)
             {
-                int a = l.pid[3 * (size_t)s + i], b = l.pid[3 * (size_t)t + i];
+                int a = l.pid[3 * (size_t)lo + i], b = l.pid[3 * (size_t)hi + i];
                 X[i] = (R)(a % W);
                 Y[i] = (R)(a / W);
                 X[3 + i] = (R)(b % W);
