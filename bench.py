@@ -307,9 +307,24 @@ def main():
     E._check(E.lib().hbp_last_phase_ms(ctx.h, ph))
     phases = {"prepare": ph[0], "bp": ph[1], "post": ph[2], "total": ph[3]}
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    pms, plaunch, pbytes = C.c_double(), C.c_long(), C.c_double()
-    E._check(E.lib().hbp_profile_read(ctx.h, C.byref(pms), C.byref(plaunch), C.byref(pbytes)))
+    pms, plaunch, pbytes, ppix = C.c_double(), C.c_long(), C.c_double(), C.c_double()
+    E._check(E.lib().hbp_profile_read(ctx.h, C.byref(pms), C.byref(plaunch), C.byref(pbytes), C.byref(ppix)))
     E._check(E.lib().hbp_profile_enable(ctx.h, 0))
+
+    # the same kernel alone on the device: one more batch (untimed) with the
+    # BP on a single stream, every 16th data-cost launch event-timed
+    iso = None
+    if rank == 0:
+        E._check(E.lib().hbp_set_bp_streams(ctx.h, 1))
+        E._check(E.lib().hbp_profile_enable(ctx.h, 2))
+        with torch.cuda.stream(stream):
+            flush.random_(0, 255)
+        step()
+        ims, ilaunch, ibytes, ipix = C.c_double(), C.c_long(), C.c_double(), C.c_double()
+        E._check(E.lib().hbp_profile_read(ctx.h, C.byref(ims), C.byref(ilaunch), C.byref(ibytes), C.byref(ipix)))
+        E._check(E.lib().hbp_profile_enable(ctx.h, 0))
+        E._check(E.lib().hbp_set_bp_streams(ctx.h, 0))
+        iso = (ims.value, ilaunch.value, ibytes.value, ipix.value)
     t_max = max_over_ranks(ms, dist, "cuda")
     value = whole_job_rate(NP, args.steps, world, t_max / 1e3)
 
@@ -392,6 +407,15 @@ def main():
     if rank == 0:
         peak, peak_kind = peaks()
         achieved = (pbytes.value / (pms.value / 1e3)) / 1e9 if pms.value > 0 else None
+        per_launch = lambda pix, n: KCOST_DRAM_BYTES_PER_PIXEL * pix / max(1, n)
+        roof_iso = None
+        if iso and iso[0] > 0:
+            a_iso = (iso[2] / (iso[0] / 1e3)) / 1e9
+            roof_iso = {"kernel": "k_cost, BP on one stream (the kernel alone on the device)", "bound": "hbm",
+                        "achieved": a_iso, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                        "frac": a_iso / peak, "traffic": per_launch(iso[3], iso[1]),
+                        "views_per_launch": iso[3] / max(1, iso[1]) / (W * H),
+                        "launches_timed": iso[1], "avg_launch_us": 1e3 * iso[0] / max(1, iso[1])}
         lat.sort()
         line = {
             "metric": METRIC,
@@ -416,15 +440,18 @@ def main():
                            "of": "served requests, submit to result in host memory"},
             "plain_fp32": plain,
             "accuracy": accuracy,
-            "roofline": {"kernel": "plane_cost_kernel (data cost of 4 candidate planes per pixel)",
+            "roofline": {"kernel": "k_cost (data cost of 4 candidate planes per pixel), timed region: "
+                                   "the first of the concurrent BP streams",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": KCOST_DRAM_BYTES_PER_PIXEL * NP * W * H,
+                         "traffic": per_launch(ppix.value, plaunch.value) if plaunch.value else None,
                          "traffic_source": "ncu dram__bytes_read+write of one k_cost launch over 4 views "
-                                           "(profiles/k_cost_level5_4x720x496_d128.md), per list position, "
-                                           "times the positions of one 16-view launch",
+                                           "(profiles/k_cost_level5_4x720x496_d128.md) per list position, "
+                                           "times the positions of a timed launch",
+                         "views_per_launch": ppix.value / max(1, plaunch.value) / (W * H),
                          "launches_timed": plaunch.value,
                          "avg_launch_us": 1e3 * pms.value / max(1, plaunch.value)},
+            "roofline_isolated": roof_iso,
             "cpu_baseline": cpu,
             "clocks": clk,
             "e2e": e2e,

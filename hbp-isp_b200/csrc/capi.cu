@@ -100,6 +100,7 @@ struct hbp_ctx : Lane
 {
     float *wtab = nullptr; // weighted-median weight table (766 floats)
     int prof_mode = 0;     // 0 off, 1 every pair, 2 first pair of each batch call
+    int bp_streams = 0;    // hbp_set_bp_streams
     int max_lanes = 8;
     std::vector<std::unique_ptr<Lane>> lanes; // extra lanes (1..)
     std::vector<std::unique_ptr<Slot>> slots;
@@ -672,6 +673,7 @@ void run_pairs(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, const uint8_t
                 views.push_back(&c->slots[i]->planR);
         }
         HbpParams q = to_params(&p, c->prof_mode ? &c->prof : nullptr);
+        q.bp_streams = c->bp_streams;
         c->prof.on = c->prof_mode != 0;
         c->tmp.reset();
         {
@@ -792,7 +794,7 @@ hbp_status hbp_profile_enable(hbp_ctx *c, int on)
     return HBP_OK;
 }
 
-hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *bytes)
+hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *bytes, double *pixels)
 {
     if (!c || !ms || !launches || !bytes)
         return fail(HBP_ERR_INVALID_ARG, "null pointer");
@@ -800,7 +802,17 @@ hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *byte
         *ms = c->prof.total_ms();
         *launches = c->prof.launches;
         *bytes = c->prof.bytes;
+        if (pixels)
+            *pixels = c->prof.pixels;
     });
+}
+
+hbp_status hbp_set_bp_streams(hbp_ctx *c, int streams)
+{
+    if (!c || streams < 0 || streams > 64)
+        return fail(HBP_ERR_INVALID_ARG, "streams must be 0 (automatic) .. 64");
+    c->bp_streams = streams;
+    return HBP_OK;
 }
 
 hbp_status hbp_profile_breakdown(hbp_ctx *c, double *ms, long *timed, long *all)
@@ -889,6 +901,7 @@ struct hbp_server
     hbp_status fatal = HBP_OK;
     std::string fatal_msg;
     Lane sched; // scheduler stream (+ error word, unused arenas)
+    std::vector<cudaStream_t> extra_st; // the other BP schedulers' streams
 
     // Admit queued requests in arrival order while memory allows: a free
     // slot large enough, else a new one within the budget (freeing pooled
@@ -1026,7 +1039,20 @@ struct hbp_server
     {
         cudaSetDevice(device);
         HbpParams q = to_params(&prm);
-        BpScheduler bp(q, sched.st);
+        // up to 8 schedulers on their own streams, ticked in turn; a joining
+        // pair goes to the one with the fewest pairs in flight
+        std::vector<std::unique_ptr<BpScheduler>> bps;
+        bps.push_back(std::make_unique<BpScheduler>(q, sched.st));
+        for (size_t i = 0; i < extra_st.size(); ++i)
+            bps.push_back(std::make_unique<BpScheduler>(q, extra_st[i]));
+        std::vector<cudaStream_t> bst{sched.st};
+        bst.insert(bst.end(), extra_st.begin(), extra_st.end());
+        auto active = [&] {
+            for (auto &b : bps)
+                if (b->active())
+                    return true;
+            return false;
+        };
         std::deque<ServerReq *> finishing;
         std::vector<void *> fin;
         for (;;)
@@ -1034,9 +1060,9 @@ struct hbp_server
             std::vector<ServerReq *> join;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                if (!bp.active() && finishing.empty())
+                if (!active() && finishing.empty())
                     cv_sched.wait(lk, [&] { return stop || !ready.empty(); });
-                if (stop && !bp.active() && finishing.empty() && ready.empty())
+                if (stop && !active() && finishing.empty() && ready.empty())
                     return;
                 join.assign(ready.begin(), ready.end());
                 ready.clear();
@@ -1044,37 +1070,47 @@ struct hbp_server
             hbp_status st = guarded([&] {
                 for (ServerReq *r : join)
                 {
-                    HBP_CUDA(cudaStreamWaitEvent(sched.st, r->ev_ready, 0));
-                    bp.add(&r->ss->slot.plan, r);
+                    size_t bi = 0;
+                    for (size_t i = 1; i < bps.size(); ++i)
+                        if (bps[i]->active() < bps[bi]->active())
+                            bi = i;
+                    HBP_CUDA(cudaStreamWaitEvent(bst[bi], r->ev_ready, 0));
+                    bps[bi]->add(&r->ss->slot.plan, r);
                 }
-                if (bp.active())
+                for (size_t bi = 0; bi < bps.size(); ++bi)
                 {
+                    if (!bps[bi]->active())
+                        continue;
                     fin.clear();
-                    bp.tick(fin);
+                    bps[bi]->tick(fin);
                     for (void *f : fin)
                     {
                         ServerReq *r = static_cast<ServerReq *>(f);
                         const long n = (long)r->W * r->H;
-                        launch_driver_median(r->ddisp, r->dtmp, r->W, r->H, sched.st);
+                        launch_driver_median(r->ddisp, r->dtmp, r->W, r->H, bst[bi]);
                         HBP_CUDA(cudaMemcpyAsync(r->ss->pinned, r->ddisp, sizeof(float) * n,
-                                                 cudaMemcpyDeviceToHost, sched.st));
+                                                 cudaMemcpyDeviceToHost, bst[bi]));
                         if (!r->ev_done)
                             HBP_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
-                        HBP_CUDA(cudaEventRecord(r->ev_done, sched.st));
+                        HBP_CUDA(cudaEventRecord(r->ev_done, bst[bi]));
                         r->state = RQ_FINISHING;
                         finishing.push_back(r);
                     }
                 }
-                // completions, in order
-                while (!finishing.empty())
+                // completions (streams finish out of order: check each)
+                const bool busy_bp = active();
+                for (size_t i = 0; i < finishing.size();)
                 {
-                    ServerReq *r = finishing.front();
-                    cudaError_t q = bp.active() ? cudaEventQuery(r->ev_done) : cudaEventSynchronize(r->ev_done);
+                    ServerReq *r = finishing[i];
+                    cudaError_t q = busy_bp || i > 0 ? cudaEventQuery(r->ev_done) : cudaEventSynchronize(r->ev_done);
                     if (q == cudaErrorNotReady)
-                        break;
+                    {
+                        ++i;
+                        continue;
+                    }
                     HBP_CUDA(q);
                     std::memcpy(r->out, r->ss->pinned, sizeof(float) * (size_t)r->W * r->H);
-                    finishing.pop_front();
+                    finishing.erase(finishing.begin() + (long)i);
                     std::lock_guard<std::mutex> lk(mu);
                     finish_locked(r, HBP_OK, "");
                 }
@@ -1119,6 +1155,12 @@ hbp_status hbp_server_create(int device, size_t budget_bytes, int prep_lanes, co
         s->prm = *prm;
     hbp_status st = guarded([&] {
         lane_init(&s->sched, device);
+        for (int i = 0; i < 7; ++i)
+        {
+            cudaStream_t x;
+            HBP_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+            s->extra_st.push_back(x);
+        }
         for (int i = 0; i < prep_lanes; ++i)
         {
             s->lanes.push_back(std::make_unique<Lane>());
@@ -1166,6 +1208,11 @@ void hbp_server_destroy(hbp_server *s)
     s->busy.clear();
     for (auto &l : s->lanes)
         lane_release(l.get());
+    for (cudaStream_t x : s->extra_st)
+    {
+        cudaStreamSynchronize(x);
+        cudaStreamDestroy(x);
+    }
     lane_release(&s->sched);
     delete s;
 }

@@ -118,7 +118,8 @@ struct KernelProf
     bool on = false;
     std::vector<cudaEvent_t> ev; // start/stop pairs, reused
     size_t used = 0;
-    double bytes = 0; // algorithmic bytes of the timed launches
+    double bytes = 0;  // algorithmic bytes of the timed launches
+    double pixels = 0; // list positions (pixels) the timed launches covered
     long launches = 0;
     // breakdown mode: every BP kernel of every 8th step timed, per (kind, level)
     static constexpr int KINDS = 10, LEVELS = 32;
@@ -131,6 +132,7 @@ struct KernelProf
     {
         used = 0;
         bytes = 0;
+        pixels = 0;
         launches = 0;
         usedb = 0;
         tagb.clear();
@@ -194,6 +196,7 @@ struct HbpParams
     float tau_smooth = 0.6f;
     int min_level = 2;
     int msg_fp16 = 0;
+    int bp_streams = 0; // BP scheduler streams of a batch (0: automatic)
     KernelProf *prof = nullptr;
 };
 

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
+#include <memory>
 #include <vector>
 
 #include <cuda_fp16.h>
@@ -1480,7 +1481,10 @@ void BpScheduler::tick(std::vector<void *> &finished)
         // entry (packed position 4 B + node 4 B) and two volume bytes per
         // candidate, plus per chunk the node's 4 planes in and 4 sums out
         for (const View *v : vc)
+        {
             prof->bytes += (double)v->vp->HW * (8 + 2 * P) + (double)v->vp->levelC[v->li] * (4 * 16 + 16);
+            prof->pixels += (double)v->vp->HW;
+        }
         prof->launches += (long)((tc.size() + MAXV - 1) / MAXV);
     }
     I.launch(vc, tc, CNT_EDGES, [&](const StepDesc &d) {
@@ -1546,15 +1550,49 @@ void BpScheduler::tick(std::vector<void *> &finished)
 }
 
 // HBP_ISP::run_ms for every view (hbp_isp.cu:1313-1346), all admitted at once.
+// The views are dealt to up to 8 schedulers, two views each, on their own
+// streams, ticked in turn from this thread: kernels of different schedulers
+// (a latency-bound data cost beside an issue-bound message pass) share the
+// GPU. Only the first scheduler feeds the profiler.
 void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &, cudaStream_t st)
 {
-    BpScheduler s(prm, st);
-    for (ViewPlan *vp : views)
-        s.add(vp, vp);
-    std::vector<void *> fin;
-    while (s.active())
-        s.tick(fin);
-    HBP_CUDA(cudaStreamSynchronize(st));
+    const int S = prm.bp_streams > 0 ? std::min<int>(prm.bp_streams, (int)std::max<size_t>(views.size(), 1))
+                                      : std::max(1, std::min(8, (int)(views.size() + 1) / 2));
+    std::vector<cudaStream_t> ss(S, st);
+    HbpParams quiet = prm;
+    quiet.prof = nullptr;
+    std::vector<std::unique_ptr<BpScheduler>> sc;
+    try
+    {
+        for (int i = 1; i < S; ++i)
+            HBP_CUDA(cudaStreamCreateWithFlags(&ss[i], cudaStreamNonBlocking));
+        for (int i = 0; i < S; ++i)
+            sc.push_back(std::make_unique<BpScheduler>(i == 0 ? prm : quiet, ss[i]));
+        for (size_t i = 0; i < views.size(); ++i)
+            sc[i % S]->add(views[i], views[i]);
+        std::vector<void *> fin;
+        for (bool any = true; any;)
+        {
+            any = false;
+            for (auto &x : sc)
+                if (x->active())
+                {
+                    x->tick(fin);
+                    any = true;
+                }
+        }
+        for (int i = 0; i < S; ++i)
+            HBP_CUDA(cudaStreamSynchronize(ss[i]));
+    }
+    catch (...)
+    {
+        for (int i = 1; i < S; ++i)
+            if (ss[i] != st)
+                cudaStreamDestroy(ss[i]);
+        throw;
+    }
+    for (int i = 1; i < S; ++i)
+        HBP_CUDA(cudaStreamDestroy(ss[i]));
 }
 
 } // namespace hbp

@@ -165,6 +165,10 @@ hbp_status hbp_run_batch_d(hbp_ctx *ctx, int npairs, const uint8_t *const *bgrL,
                            float *const *disp, float *const *plane);
 
 hbp_status hbp_set_lanes(hbp_ctx *ctx, int lanes);
+/* BP of a batch runs on up to 8 streams (two pairs each) by default, so that
+ * kernels of different pairs share the GPU; streams > 0 fixes the number
+ * (1 = every BP kernel alone on the device). 0 restores the default. */
+hbp_status hbp_set_bp_streams(hbp_ctx *ctx, int streams);
 
 /* ------------------------------------------------------------ serving */
 
@@ -205,12 +209,12 @@ long hbp_launch_count(void);
  * [1] batched BP, [2] post stages, [3] whole call. */
 hbp_status hbp_last_phase_ms(hbp_ctx *ctx, double *out4);
 /* While enabled, launches of the data-cost kernel (the dominant kernel of the
- * path) are bracketed by CUDA events on the context stream: mode 1 times every
- * launch, mode 2 only those of the first pair of each hbp_run_batch_d call
- * (0 = off). Read returns the summed device time, the launch count and the
- * algorithmic bytes of the timed launches. Enabling resets the totals. */
+ * path) of every 16th BP tick of the first BP stream are bracketed by CUDA
+ * events (modes 1 and 2; 0 = off). Read returns the summed device time, the
+ * launch count, the algorithmic bytes and the pixels (list positions) of the
+ * timed launches (pixels may be NULL). Enabling resets the totals. */
 hbp_status hbp_profile_enable(hbp_ctx *ctx, int on);
-hbp_status hbp_profile_read(hbp_ctx *ctx, double *ms, long *launches, double *bytes);
+hbp_status hbp_profile_read(hbp_ctx *ctx, double *ms, long *launches, double *bytes, double *pixels);
 /* Mode 3 additionally times every BP kernel of every 8th BP step. Breakdown
  * fills three arrays of 10 x 32 entries indexed [kind][level] (kinds: 0 node
  * select, 1 child candidates, 2 neighbour candidates, 3 set candidates,
