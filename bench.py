@@ -176,15 +176,18 @@ KINDS = ["node_select", "child_cand", "neighbor_cand", "set_cand", "data_cost", 
 
 
 def breakdown(E, ctx, step):
-    """One untimed step with the BP kernels event-timed (mode 3): estimated
-    device ms per step by kernel kind and by (kind, pyramid level)."""
+    """One untimed step with the BP on one stream and its kernels event-timed
+    (mode 3): estimated device ms per step by kernel kind and by (kind,
+    pyramid level)."""
     import ctypes as C
     n = 10 * 32
     ms, timed, allc = (C.c_double * n)(), (C.c_long * n)(), (C.c_long * n)()
+    E._check(E.lib().hbp_set_bp_streams(ctx.h, 1))  # kernels alone: times add up
     E._check(E.lib().hbp_profile_enable(ctx.h, 3))
     step()
     E._check(E.lib().hbp_profile_breakdown(ctx.h, ms, timed, allc))
     E._check(E.lib().hbp_profile_enable(ctx.h, 0))
+    E._check(E.lib().hbp_set_bp_streams(ctx.h, 0))
     by_kind, by_level = {}, {}
     for k, name in enumerate(KINDS):
         for lv in range(32):

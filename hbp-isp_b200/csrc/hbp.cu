@@ -376,47 +376,13 @@ __device__ __forceinline__ void store_msg(const ViewBufs &b, int buf, size_t e, 
     }
 }
 
-__device__ __forceinline__ void select_thread(const LevelDev &l, int n, const float4 *pc, const ViewBufs &vb,
-                                              int mbuf)
+// get_belief_order + select_belief (hbp_isp.cu:432-472) for node n given its
+// 12 costs cs and beliefs b: a slot's rank counts the slots that beat it (a
+// later slot loses ties); slots ranked < P move to the front in slot order,
+// in place; keep[n] records which.
+__device__ __forceinline__ void select_finish(const LevelDev &l, int n, const float cs[K], const float b[K])
 {
-    float cs[K], b[K];
     float *cst = l.cost + (size_t)n * K;
-#pragma unroll
-    for (int k = 0; k < 2 * P; ++k)
-        cs[k] = cst[k];
-    {
-        const float4 a = sum_chunks(pc, l.chunk_off[n], l.chunk_off[n + 1]);
-        cs[8] = a.x;
-        cs[9] = a.y;
-        cs[10] = a.z;
-        cs[11] = a.w;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        b[k] = cs[k];
-    // out-edge messages in edge order; loads issued 4 edges at a time
-    const int e0 = l.nb_off[n], e1 = l.nb_off[n + 1];
-    int e = e0;
-    for (; e + 4 <= e1; e += 4)
-    {
-        float m[4][K];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            load_msg(vb, mbuf, (size_t)(e + j), m[j]);
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-                b[k] = b[k] + m[j][k];
-    }
-    for (; e < e1; ++e)
-    {
-        float m[K];
-        load_msg(vb, mbuf, (size_t)e, m);
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            b[k] = b[k] + m[k];
-    }
     int ord[K];
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -456,6 +422,107 @@ __device__ __forceinline__ void select_thread(const LevelDev &l, int n, const fl
         }
     l.keep[n] = kl | (unsigned long long)nb;
 }
+__device__ __forceinline__ void select_thread(const LevelDev &l, int n, const float4 *pc, const ViewBufs &vb,
+                                              int mbuf)
+{
+    float cs[K], b[K];
+    const float *cst = l.cost + (size_t)n * K;
+#pragma unroll
+    for (int k = 0; k < 2 * P; ++k)
+        cs[k] = cst[k];
+    {
+        const float4 a = sum_chunks(pc, l.chunk_off[n], l.chunk_off[n + 1]);
+        cs[8] = a.x;
+        cs[9] = a.y;
+        cs[10] = a.z;
+        cs[11] = a.w;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        b[k] = cs[k];
+    // out-edge messages in edge order; loads issued 4 edges at a time
+    const int e0 = l.nb_off[n], e1 = l.nb_off[n + 1];
+    int e = e0;
+    for (; e + 4 <= e1; e += 4)
+    {
+        float m[4][K];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            load_msg(vb, mbuf, (size_t)(e + j), m[j]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                b[k] = b[k] + m[j][k];
+    }
+    for (; e < e1; ++e)
+    {
+        float m[K];
+        load_msg(vb, mbuf, (size_t)e, m);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            b[k] = b[k] + m[k];
+    }
+    select_finish(l, n, cs, b);
+}
+
+// The same select with one warp per node, for nodes with many chunks and
+// edges (the coarse levels): the lanes load 32 chunk sums or 32 edges'
+// messages at a time and walk them in order through shuffles, so the sums
+// are the sequential ones of select_thread, bit for bit. Lane 0 writes.
+__device__ __forceinline__ void select_warp(const LevelDev &l, int n, const float4 *pc, const ViewBufs &vb,
+                                            int mbuf, int lane)
+{
+    float cs[K], b[K];
+    const float *cst = l.cost + (size_t)n * K;
+#pragma unroll
+    for (int k = 0; k < 2 * P; ++k)
+        cs[k] = cst[k];
+    const int c0 = l.chunk_off[n], c1 = l.chunk_off[n + 1];
+    float4 a = pc[c0];
+    for (int base = c0 + 1; base < c1; base += 32)
+    {
+        const int ch = base + lane;
+        const float4 q = ch < c1 ? pc[ch] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int cnt = min(32, c1 - base);
+        for (int j = 0; j < cnt; ++j)
+        {
+            a.x = a.x + __shfl_sync(0xffffffffu, q.x, j);
+            a.y = a.y + __shfl_sync(0xffffffffu, q.y, j);
+            a.z = a.z + __shfl_sync(0xffffffffu, q.z, j);
+            a.w = a.w + __shfl_sync(0xffffffffu, q.w, j);
+        }
+    }
+    cs[8] = a.x;
+    cs[9] = a.y;
+    cs[10] = a.z;
+    cs[11] = a.w;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        b[k] = cs[k];
+    const int e0 = l.nb_off[n], e1 = l.nb_off[n + 1];
+    for (int base = e0; base < e1; base += 32)
+    {
+        const int e = base + lane;
+        float m[K];
+        if (e < e1)
+            load_msg(vb, mbuf, (size_t)e, m);
+        else
+        {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                m[k] = 0.f;
+        }
+        const int cnt = min(32, e1 - base);
+        for (int j = 0; j < cnt; ++j)
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                b[k] = b[k] + __shfl_sync(0xffffffffu, m[k], j);
+    }
+    if (lane == 0)
+        select_finish(l, n, cs, b);
+}
+
 
 __device__ __forceinline__ void ransac_thread(const LevelDev &l, const Common &c, int n, uint32_t s,
                                               uint32_t *s_out)
@@ -549,6 +616,29 @@ __global__ void __launch_bounds__(128) k_node(const ViewDev *__restrict__ V, Ste
     const int n = item - d.pre[find_task(d, item)];
     if (!t.first)
         select_thread(l, n, v.b.pc[t.pb ^ 1], v.b, t.mb ^ 1);
+    if (t.mode == NODE_SELECT_RANSAC)
+        ransac_thread(l, v.c, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n]);
+    else if (t.mode == NODE_SELECT_RANDOM)
+        random_thread(l, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n], t.max_dz, t.max_dn);
+}
+
+// k_node with one warp per node (the select's sums as in select_warp; lane 0
+// then draws the node's candidates).
+__global__ void __launch_bounds__(128) k_node_warp(const ViewDev *__restrict__ V, StepDesc d)
+{
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (item >= d.pre[d.nt]) // warp-uniform
+        return;
+    const int ti = find_task(d, item);
+    const Task &t = d.t[ti];
+    const ViewDev &v = *t.vd;
+    const LevelDev &l = *t.lvl;
+    const int n = item - d.pre[ti];
+    if (!t.first)
+        select_warp(l, n, v.b.pc[t.pb ^ 1], v.b, t.mb ^ 1, lane);
+    if (lane != 0)
+        return;
     if (t.mode == NODE_SELECT_RANSAC)
         ransac_thread(l, v.c, n, v.b.s_ransac[t.rb][n], &v.b.s_ransac[t.rb ^ 1][n]);
     else if (t.mode == NODE_SELECT_RANDOM)
@@ -1449,8 +1539,21 @@ void BpScheduler::tick(std::vector<void *> &finished)
         note_launch();
     });
     // node phase: select of the previous step + the step's candidates
+    // large nodes (16+ chunks on average): a warp per node shortens the
+    // select's serial sums; otherwise a thread per node (the same arithmetic
+    // either way)
+    double nch = 0, nnodes = 0;
+    for (const View *v : vn)
+    {
+        nch += v->vp->levelC[v->li];
+        nnodes += v->vp->levelN[v->li];
+    }
+    const bool warp_nodes = nnodes > 0 && nch >= 16.0 * nnodes;
     I.launch(vn, tn, CNT_NODES, [&](const StepDesc &d) {
-        run(0, lvl_n, [&] { k_node<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        if (warp_nodes)
+            run(0, lvl_n, [&] { k_node_warp<<<blocks((long)d.pre[d.nt] * 32, 128), 128, 0, st>>>(nullptr, d); });
+        else
+            run(0, lvl_n, [&] { k_node<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
         note_launch();
     });
     // spatial candidates
