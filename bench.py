@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--fp16", type=int, default=1, help="store BP messages as FP16 (1) or FP32 (0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--window", type=int, default=0,
+                    help="served requests in flight (default: the pairs per step)")
     ap.add_argument("--breakdown", action="store_true",
                     help="after the timed region, one extra step with every BP kernel of every 8th "
                          "BP step event-timed; per-kernel/per-level estimate printed to stderr")
@@ -369,10 +371,11 @@ def main():
             if dist:
                 dist.barrier()
             n_req = NP * args.steps
+            window = args.window or NP
             t0 = time.perf_counter()
             inflight = []
             for k in range(n_req):
-                if len(inflight) == NP:
+                if len(inflight) == window:
                     lat.append(srv.wait(inflight.pop(0))[1])
                 inflight.append(srv.submit(pinL[k % NP], pinR[k % NP], D))
             for i in inflight:
@@ -383,7 +386,7 @@ def main():
         el = max_over_ranks(el, dist, "cuda")
         e2e = {"value": whole_job_rate(NP, args.steps, world, el), "unit": "pairs/s",
                "h2d_bytes_per_step": NP * 2 * 3 * W * H, "d2h_bytes_per_step": NP * 4 * W * H,
-               "path": f"hbp_submit/hbp_wait, {NP} requests in flight, messages "
+               "path": f"hbp_submit/hbp_wait, {args.window or NP} requests in flight, messages "
                        + ("fp16" if args.fp16 else "fp32")}
         # the plain FP32 single-pair path (hbp_run_pair, one pair at a time)
         prm32 = E.default_params(msg_fp16=0, post=1)

@@ -900,8 +900,7 @@ struct hbp_server
     bool stop = false;
     hbp_status fatal = HBP_OK;
     std::string fatal_msg;
-    Lane sched; // scheduler stream (+ error word, unused arenas)
-    std::vector<cudaStream_t> extra_st; // the other BP schedulers' streams
+    Lane sched; // error word and stream of the scheduler thread's own work
 
     // Admit queued requests in arrival order while memory allows: a free
     // slot large enough, else a new one within the budget (freeing pooled
@@ -1039,22 +1038,20 @@ struct hbp_server
     {
         cudaSetDevice(device);
         HbpParams q = to_params(&prm);
-        // up to 8 schedulers on their own streams, ticked in turn; a joining
-        // pair goes to the one with the fewest pairs in flight
-        std::vector<std::unique_ptr<BpScheduler>> bps;
-        bps.push_back(std::make_unique<BpScheduler>(q, sched.st));
-        for (size_t i = 0; i < extra_st.size(); ++i)
-            bps.push_back(std::make_unique<BpScheduler>(q, extra_st[i]));
-        std::vector<cudaStream_t> bst{sched.st};
-        bst.insert(bst.end(), extra_st.begin(), extra_st.end());
-        auto active = [&] {
-            for (auto &b : bps)
-                if (b->active())
-                    return true;
-            return false;
-        };
+        // 8 schedulers on their own streams, ticked in turn; a joining pair
+        // goes to the one with the fewest pairs in flight
+        std::unique_ptr<BpPool> pool;
+        hbp_status pst = guarded([&] { pool = std::make_unique<BpPool>(q, 8); });
+        if (pst != HBP_OK)
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            fatal = pst;
+            fatal_msg = g_err;
+            return;
+        }
+        auto active = [&] { return pool->active(); };
         std::deque<ServerReq *> finishing;
-        std::vector<void *> fin;
+        std::vector<std::pair<void *, int>> fin;
         for (;;)
         {
             std::vector<ServerReq *> join;
@@ -1070,29 +1067,25 @@ struct hbp_server
             hbp_status st = guarded([&] {
                 for (ServerReq *r : join)
                 {
-                    size_t bi = 0;
-                    for (size_t i = 1; i < bps.size(); ++i)
-                        if (bps[i]->active() < bps[bi]->active())
-                            bi = i;
-                    HBP_CUDA(cudaStreamWaitEvent(bst[bi], r->ev_ready, 0));
-                    bps[bi]->add(&r->ss->slot.plan, r);
+                    const int bi = pool->least_loaded();
+                    HBP_CUDA(cudaStreamWaitEvent(pool->stream(bi), r->ev_ready, 0));
+                    pool->add(bi, &r->ss->slot.plan, r);
                 }
-                for (size_t bi = 0; bi < bps.size(); ++bi)
+                if (pool->active())
                 {
-                    if (!bps[bi]->active())
-                        continue;
                     fin.clear();
-                    bps[bi]->tick(fin);
-                    for (void *f : fin)
+                    pool->tick(fin);
+                    for (auto &f : fin)
                     {
-                        ServerReq *r = static_cast<ServerReq *>(f);
+                        ServerReq *r = static_cast<ServerReq *>(f.first);
+                        const cudaStream_t bs = pool->stream(f.second);
                         const long n = (long)r->W * r->H;
-                        launch_driver_median(r->ddisp, r->dtmp, r->W, r->H, bst[bi]);
+                        launch_driver_median(r->ddisp, r->dtmp, r->W, r->H, bs);
                         HBP_CUDA(cudaMemcpyAsync(r->ss->pinned, r->ddisp, sizeof(float) * n,
-                                                 cudaMemcpyDeviceToHost, bst[bi]));
+                                                 cudaMemcpyDeviceToHost, bs));
                         if (!r->ev_done)
                             HBP_CUDA(cudaEventCreateWithFlags(&r->ev_done, cudaEventDisableTiming));
-                        HBP_CUDA(cudaEventRecord(r->ev_done, bst[bi]));
+                        HBP_CUDA(cudaEventRecord(r->ev_done, bs));
                         r->state = RQ_FINISHING;
                         finishing.push_back(r);
                     }
@@ -1155,12 +1148,6 @@ hbp_status hbp_server_create(int device, size_t budget_bytes, int prep_lanes, co
         s->prm = *prm;
     hbp_status st = guarded([&] {
         lane_init(&s->sched, device);
-        for (int i = 0; i < 7; ++i)
-        {
-            cudaStream_t x;
-            HBP_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
-            s->extra_st.push_back(x);
-        }
         for (int i = 0; i < prep_lanes; ++i)
         {
             s->lanes.push_back(std::make_unique<Lane>());
@@ -1208,11 +1195,6 @@ void hbp_server_destroy(hbp_server *s)
     s->busy.clear();
     for (auto &l : s->lanes)
         lane_release(l.get());
-    for (cudaStream_t x : s->extra_st)
-    {
-        cudaStreamSynchronize(x);
-        cudaStreamDestroy(x);
-    }
     lane_release(&s->sched);
     delete s;
 }

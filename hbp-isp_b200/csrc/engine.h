@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -248,6 +249,35 @@ class BpScheduler
     struct Impl;
     Impl *impl;
 };
+
+// BpSchedulers on their own streams, ticked in turn from one host thread, so
+// that kernels of different views share the GPU (a latency-bound data cost
+// beside an issue-bound message pass). The caller picks a scheduler for a
+// view (least_loaded(): fewest views in flight), orders the view's setup
+// before that scheduler's stream, and adds it; tick() reports each finished
+// view with its scheduler's index.
+class BpPool
+{
+  public:
+    BpPool(const HbpParams &prm, int streams);
+    ~BpPool();
+    BpPool(const BpPool &) = delete;
+    BpPool &operator=(const BpPool &) = delete;
+    int least_loaded() const;
+    void add(int i, ViewPlan *vp, void *user);
+    bool active() const;
+    void tick(std::vector<std::pair<void *, int>> &finished);
+    void sync();
+    cudaStream_t stream(int i) const { return st_[(size_t)i]; }
+    int size() const { return (int)st_.size(); }
+
+  private:
+    std::vector<cudaStream_t> st_;
+    std::vector<std::unique_ptr<BpScheduler>> sc_;
+};
+
+// Streams a batch of `views` uses by default: two views per stream, at most 8.
+int bp_default_streams(int views);
 
 // ---------------------------------------------------------------------------
 // post.cu

@@ -1652,50 +1652,93 @@ void BpScheduler::tick(std::vector<void *> &finished)
     I.views.swap(keep);
 }
 
-// HBP_ISP::run_ms for every view (hbp_isp.cu:1313-1346), all admitted at once.
-// The views are dealt to up to 8 schedulers, two views each, on their own
-// streams, ticked in turn from this thread: kernels of different schedulers
-// (a latency-bound data cost beside an issue-bound message pass) share the
-// GPU. Only the first scheduler feeds the profiler.
-void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &, cudaStream_t st)
+BpPool::BpPool(const HbpParams &prm, int streams)
 {
-    const int S = prm.bp_streams > 0 ? std::min<int>(prm.bp_streams, (int)std::max<size_t>(views.size(), 1))
-                                      : std::max(1, std::min(8, (int)(views.size() + 1) / 2));
-    std::vector<cudaStream_t> ss(S, st);
     HbpParams quiet = prm;
-    quiet.prof = nullptr;
-    std::vector<std::unique_ptr<BpScheduler>> sc;
+    quiet.prof = nullptr; // only the first scheduler feeds the profiler
+    const int S = std::max(1, std::min(streams, 64));
     try
     {
-        for (int i = 1; i < S; ++i)
-            HBP_CUDA(cudaStreamCreateWithFlags(&ss[i], cudaStreamNonBlocking));
         for (int i = 0; i < S; ++i)
-            sc.push_back(std::make_unique<BpScheduler>(i == 0 ? prm : quiet, ss[i]));
-        for (size_t i = 0; i < views.size(); ++i)
-            sc[i % S]->add(views[i], views[i]);
-        std::vector<void *> fin;
-        for (bool any = true; any;)
         {
-            any = false;
-            for (auto &x : sc)
-                if (x->active())
-                {
-                    x->tick(fin);
-                    any = true;
-                }
+            cudaStream_t x;
+            HBP_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+            st_.push_back(x);
+            sc_.push_back(std::make_unique<BpScheduler>(i == 0 ? prm : quiet, x));
         }
-        for (int i = 0; i < S; ++i)
-            HBP_CUDA(cudaStreamSynchronize(ss[i]));
     }
     catch (...)
     {
-        for (int i = 1; i < S; ++i)
-            if (ss[i] != st)
-                cudaStreamDestroy(ss[i]);
+        sc_.clear();
+        for (cudaStream_t x : st_)
+            cudaStreamDestroy(x);
         throw;
     }
-    for (int i = 1; i < S; ++i)
-        HBP_CUDA(cudaStreamDestroy(ss[i]));
+}
+
+BpPool::~BpPool()
+{
+    for (cudaStream_t x : st_)
+        cudaStreamSynchronize(x);
+    sc_.clear();
+    for (cudaStream_t x : st_)
+        cudaStreamDestroy(x);
+}
+
+int BpPool::least_loaded() const
+{
+    size_t bi = 0;
+    for (size_t i = 1; i < sc_.size(); ++i)
+        if (sc_[i]->active() < sc_[bi]->active())
+            bi = i;
+    return (int)bi;
+}
+
+void BpPool::add(int i, ViewPlan *vp, void *user) { sc_[(size_t)i]->add(vp, user); }
+
+bool BpPool::active() const
+{
+    for (auto &x : sc_)
+        if (x->active())
+            return true;
+    return false;
+}
+
+void BpPool::tick(std::vector<std::pair<void *, int>> &finished)
+{
+    std::vector<void *> fin;
+    for (size_t i = 0; i < sc_.size(); ++i)
+        if (sc_[i]->active())
+        {
+            fin.clear();
+            sc_[i]->tick(fin);
+            for (void *f : fin)
+                finished.emplace_back(f, (int)i);
+        }
+}
+
+void BpPool::sync()
+{
+    for (cudaStream_t x : st_)
+        HBP_CUDA(cudaStreamSynchronize(x));
+}
+
+int bp_default_streams(int views) { return std::max(1, std::min(8, (views + 1) / 2)); }
+
+// HBP_ISP::run_ms for every view (hbp_isp.cu:1313-1346), all admitted at once,
+// on a BpPool (up to 8 streams, two views each, by default).
+void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &, cudaStream_t st)
+{
+    HBP_CUDA(cudaStreamSynchronize(st)); // the views' setup may sit on st
+    const int S = prm.bp_streams > 0 ? std::min<int>(prm.bp_streams, (int)std::max<size_t>(views.size(), 1))
+                                      : bp_default_streams((int)views.size());
+    BpPool pool(prm, S);
+    for (size_t i = 0; i < views.size(); ++i)
+        pool.add((int)(i % (size_t)S), views[i], views[i]);
+    std::vector<std::pair<void *, int>> fin;
+    while (pool.active())
+        pool.tick(fin);
+    pool.sync();
 }
 
 } // namespace hbp
