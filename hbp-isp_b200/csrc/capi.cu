@@ -582,6 +582,53 @@ hbp_status hbp_weighted_median_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t 
     });
 }
 
+hbp_status hbp_plane_to_disp_d(hbp_ctx *c, const float *plane, float *disp, int W, int H, void *stream)
+{
+    if (!c || !plane || !disp)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 2);
+        HBP_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = pick(c, stream);
+        launch_plane_to_disp(plane, disp, W, H, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_dev_alloc(int device, size_t bytes, void **ptr)
+{
+    if (!ptr || bytes == 0)
+        return fail(HBP_ERR_INVALID_ARG, "bad arguments");
+    *ptr = nullptr;
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(device));
+        if (cudaMalloc(ptr, bytes) != cudaSuccess)
+        {
+            cudaGetLastError();
+            *ptr = nullptr;
+            throw StatusError{HBP_ERR_OUT_OF_MEMORY, "device allocation failed"};
+        }
+    });
+}
+
+hbp_status hbp_dev_free(void *ptr)
+{
+    return guarded([&] {
+        if (ptr)
+            HBP_CUDA(cudaFree(ptr));
+    });
+}
+
+hbp_status hbp_copy(void *dst, const void *src, size_t bytes)
+{
+    if ((!dst || !src) && bytes)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        if (bytes)
+            HBP_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+    });
+}
+
 hbp_status hbp_driver_median_d(hbp_ctx *c, float *disp, int W, int H, void *stream)
 {
     if (!c || !disp)

@@ -119,6 +119,9 @@ hbp_status hbp_lr_check_d(hbp_ctx *ctx, const float *dispL, const float *dispR, 
 /* PostProcess::median_filter + plane_label_to_disp (post_process.cu:112-185). */
 hbp_status hbp_weighted_median_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *fail,
                                  float *plane, float *disp_out, int W, int H, void *stream);
+/* PostProcess::plane_label_to_disp for one view (post_process.cu:373-390):
+ * disp = a*x + b*y + c of each pixel's plane. */
+hbp_status hbp_plane_to_disp_d(hbp_ctx *ctx, const float *plane, float *disp, int W, int H, void *stream);
 /* medianFilter of the single-pair driver (main_stereo_hbp_isp.cu:120-192). */
 hbp_status hbp_driver_median_d(hbp_ctx *ctx, float *disp, int W, int H, void *stream);
 
@@ -144,6 +147,13 @@ hbp_status hbp_driver_median_d(hbp_ctx *ctx, float *disp, int W, int H, void *st
  *     order them on one stream or with events. */
 #define HBP_NOALLOC_MAX_PIXELS 2097152L
 hbp_status hbp_driver_median_noalloc_d(float *disp, int W, int H, void *stream);
+
+/* Device memory for callers that hold no CUDA runtime of their own (the C++
+ * classes in include/hbp_isp/ use these): allocation on a device, release,
+ * and a synchronous copy in any direction (host or device pointers). */
+hbp_status hbp_dev_alloc(int device, size_t bytes, void **ptr);
+hbp_status hbp_dev_free(void *ptr);
+hbp_status hbp_copy(void *dst, const void *src, size_t bytes);
 
 /* ------------------------------------------------------------ whole pair */
 

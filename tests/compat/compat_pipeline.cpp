@@ -1,0 +1,94 @@
+// The reference's two driver flows written against the reference-interface
+// classes of include/hbp_isp/:
+//   single: main_stereo_hbp_isp.cu:33-76 (SegHAC -> ISPData, StereoCost ->
+//           StereoData, HBP_ISP::run_ms, medianFilter)
+//   lr:     main_bench_middv3.cu:169-219 (both views, LR check, fill,
+//           weighted median, plane -> disparity)
+// usage: compat_pipeline left.bgr right.bgr W H D single.f32 lr.f32
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+
+#include "hbp_isp/hbp_isp_all.hpp"
+
+using hbp_isp::Mat;
+
+static Mat read_bgr(const char *path, int W, int H)
+{
+    Mat m(H, W, hbp_isp::MAT_8UC3);
+    std::ifstream f(path, std::ios::binary);
+    f.read(reinterpret_cast<char *>(m.data), (std::streamsize)m.bytes());
+    if (!f)
+        throw std::runtime_error(std::string("cannot read ") + path);
+    return m;
+}
+
+static void write_f32(const char *path, const Mat &m)
+{
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char *>(m.data), (std::streamsize)m.bytes());
+}
+
+int main(int argc, char **argv)
+{
+    if (argc != 8)
+    {
+        std::fprintf(stderr, "usage: %s left.bgr right.bgr W H D single.f32 lr.f32\n", argv[0]);
+        return 2;
+    }
+    const int W = std::atoi(argv[3]), H = std::atoi(argv[4]), D = std::atoi(argv[5]);
+    try
+    {
+        Mat L = read_bgr(argv[1], W, H), R = read_bgr(argv[2], W, H);
+        const float alpha = 1000.1f, tau_smooth = 0.6f;
+        const int min_level = 2;
+
+        // single-pair driver
+        SegHAC *seg = new SegHAC(L, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+        seg->run_ms();
+        ISPData *isp = new ISPData(seg);
+        delete seg;
+        StereoCost *sc = new StereoCost(L, R, D, "");
+        sc->compute_stereo_cost("Census");
+        StereoData *sd = new StereoData(sc, true);
+        delete sc;
+        HBP_ISP *hbp = new HBP_ISP(isp, sd, alpha, tau_smooth);
+        auto results_left = hbp->run_ms(min_level);
+        Mat disp = results_left.first.clone();
+        medianFilter(disp);
+        write_f32(argv[6], disp);
+
+        // MidV3_LR: the right view, then LR check, fill and weighted median
+        SegHAC *seg_r = new SegHAC(R, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+        seg_r->run_ms();
+        ISPData *isp_r = new ISPData(seg_r);
+        delete seg_r;
+        StereoCost *sc_r = new StereoCost(L, R, D, "");
+        sc_r->compute_stereo_cost("Census");
+        sc_r->cost_to_right();
+        StereoData *sd_r = new StereoData(sc_r, true);
+        delete sc_r;
+        HBP_ISP *hbp_r = new HBP_ISP(isp_r, sd_r, alpha, tau_smooth);
+        auto results_right = hbp_r->run_ms(min_level);
+        PostProcess *post = new PostProcess(L, R);
+        post->left_right_check(results_left, results_right);
+        post->plane_label_to_disp(results_left, results_right);
+        post->median_filter(results_left, results_right);
+        post->plane_label_to_disp(results_left, results_right);
+        write_f32(argv[7], results_left.first);
+
+        delete post;
+        delete hbp_r;
+        delete sd_r;
+        delete isp_r;
+        delete hbp;
+        delete sd;
+        delete isp;
+    }
+    catch (const std::exception &e)
+    {
+        std::fprintf(stderr, "compat_pipeline: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}
