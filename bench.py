@@ -63,6 +63,12 @@ def parse():
     ap.add_argument("--fp16", type=int, default=1, help="store BP messages as FP16 (1) or FP32 (0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--config", default="batch", choices=["batch", "uneven", "precision", "serve"],
+                    help="batch: the contract line (16 pairs 720x496 D128); uneven: 32 pairs of mixed "
+                         "sizes and disparity ranges in flight together; precision: 8 pairs 1440x992 D256, "
+                         "FP16 vs FP32 messages; serve: Poisson arrivals of a size mix")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
     ap.add_argument("--window", type=int, default=0,
                     help="served requests in flight (default: the pairs per step)")
     ap.add_argument("--breakdown", action="store_true",
@@ -248,6 +254,107 @@ def run_reference(args, rank):
     print(json.dumps(out))
 
 
+def run_config(args, E, torch):
+    """The other workloads (one JSON line each, not the contract line)."""
+    from scenes import make_scene
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    bad = lambda d, s, t: 100.0 * float(np.mean(np.abs(d - s.gt)[s.nonocc] > t))
+    if args.config == "uneven":
+        rng = np.random.default_rng(7)
+        sizes = [(450, 375), (720, 496), (1080, 744), (1440, 992)]
+        work = []
+        for i in range(32):
+            W, H = sizes[rng.integers(4)]
+            D = int(rng.choice([64, 128, 192, 256]))
+            work.append((make_scene(W, H, D, 5000 + i), D))
+        prm = E.default_params(msg_fp16=args.fp16, post=1)
+        srv = E.Server(local, budget_bytes=120 << 30, prep_lanes=8, params=prm)
+        try:
+            for s, D in work[:4]:  # warm-up
+                srv.wait(srv.submit(s.left, s.right, D))
+            t0 = time.perf_counter()
+            ids = [srv.submit(s.left, s.right, D) for s, D in work]
+            lat = sorted(srv.wait(i)[1] for i in ids)
+            el = time.perf_counter() - t0
+        finally:
+            srv.close()
+        px = sum(s.left.shape[0] * s.left.shape[1] for s, _ in work)
+        return {"config": "uneven", "pairs": 32, "value": 32 / el, "unit": "pairs/s",
+                "mpixels_per_s": px / el / 1e6, "seconds": el,
+                "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[-1]},
+                "workload": "32 synthetic pairs, sizes from {450x375, 720x496, 1080x744, 1440x992}, D from "
+                            "{64,128,192,256}, submitted together to the request server (seed 7)",
+                "msg": "fp16" if args.fp16 else "fp32"}
+    if args.config == "precision":
+        W, H, D, n = 1440, 992, 256, 8
+        scenes = [make_scene(W, H, D, 6000 + i, n_seg=40) for i in range(n)]
+        ctx = E.Context(local, W * H, D)
+        import ctypes as C
+        dL = [torch.from_numpy(s.left).cuda() for s in scenes]
+        dR = [torch.from_numpy(s.right).cuda() for s in scenes]
+        out = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in scenes]
+        arr = lambda ts: (C.c_void_p * n)(*[t.data_ptr() for t in ts])
+        res = {}
+        for name, f16 in (("fp32", 0), ("fp16", 1)):
+            prm = E.default_params(msg_fp16=f16, post=1)
+            E._check(E.lib().hbp_run_batch_d(ctx.h, n, arr(dL), arr(dR), W, H, D, C.byref(prm), arr(out), None))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            E._check(E.lib().hbp_run_batch_d(ctx.h, n, arr(dL), arr(dR), W, H, D, C.byref(prm), arr(out), None))
+            torch.cuda.synchronize()
+            el = time.perf_counter() - t0
+            d = [t.cpu().numpy() for t in out]
+            res[name] = {"pairs_per_s": n / el, "disp": d,
+                         "bad1_pct": float(np.mean([bad(x, s, 1.0) for x, s in zip(d, scenes)])),
+                         "bad2_pct": float(np.mean([bad(x, s, 2.0) for x, s in zip(d, scenes)]))}
+        same = [float(np.mean(a == b)) for a, b in zip(res["fp16"]["disp"], res["fp32"]["disp"])]
+        ctx.close()
+        for r in res.values():
+            r.pop("disp")
+        return {"config": "precision", "workload": f"{n} synthetic pairs {W}x{H} D{D}, 40 segments, "
+                                                   "hbp_run_batch_d", "fp32": res["fp32"], "fp16": res["fp16"],
+                "fp16_vs_fp32_identical_mean": float(np.mean(same)),
+                "fp16_vs_fp32_identical_min": float(np.min(same))}
+    # serve: Poisson arrivals of the size mix, FP16 messages, 120 GB budget
+    rng = np.random.default_rng(11)
+    mix = [((450, 375, 64), 0.4), ((720, 496, 128), 0.3), ((1440, 992, 256), 0.2), ((2880, 1984, 384), 0.1)]
+    kinds = [m for m, _ in mix]
+    pool = {k: make_scene(k[0], k[1], k[2], 7000 + i) for i, k in enumerate(kinds)}
+    n_req = max(1, int(args.rate * args.duration))
+    gaps = rng.exponential(1.0 / args.rate, n_req)
+    pick = rng.choice(len(kinds), n_req, p=[p for _, p in mix])
+    prm = E.default_params(msg_fp16=1, post=1)
+    srv = E.Server(local, budget_bytes=120 << 30, prep_lanes=8, params=prm)
+    try:
+        for k in kinds:  # warm-up, one of each size
+            s = pool[k]
+            srv.wait(srv.submit(s.left, s.right, k[2]))
+        t0 = time.perf_counter()
+        t_next = t0
+        ids = []
+        for g, j in zip(gaps, pick):
+            t_next += g
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            s = pool[kinds[j]]
+            ids.append((srv.submit(s.left, s.right, kinds[j][2]), j))
+        lat = [srv.wait(i)[1] for i, _ in ids]
+        el = time.perf_counter() - t0
+    finally:
+        srv.close()
+    ls = sorted(lat)
+    per = {}
+    for (i, j), l in zip(ids, lat):
+        per.setdefault(f"{kinds[j][0]}x{kinds[j][1]}xD{kinds[j][2]}", []).append(l)
+    return {"config": "serve", "offered_rate": args.rate, "arrival_seconds": args.duration,
+            "requests": n_req, "completed_per_s": n_req / el, "seconds_to_drain": el,
+            "latency_ms": {"p50": ls[len(ls) // 2], "p99": ls[min(len(ls) - 1, int(0.99 * len(ls)))]},
+            "latency_p50_by_size_ms": {k: sorted(v)[len(v) // 2] for k, v in per.items()},
+            "workload": "Poisson arrivals; 40% 450x375 D64, 30% 720x496 D128, 20% 1440x992 D256, "
+                        "10% 2880x1984 D384; FP16 messages; 120 GB admission budget (seed 11)"}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -260,6 +367,10 @@ def main():
     import hbp_b200 as E
 
     torch.cuda.set_device(local)
+    if args.config != "batch":
+        if rank == 0:
+            print(json.dumps(run_config(args, E, torch)))
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist

@@ -24,6 +24,11 @@ struct Arena
     size_t cap = 0, off = 0;
     bool owned = false;
 
+    Arena() = default;
+    ~Arena() { release(); }
+    Arena(const Arena &) = delete;
+    Arena &operator=(const Arena &) = delete;
+
     void init(size_t bytes);
     void attach(void *p, size_t bytes);
     void release();

@@ -84,3 +84,33 @@ def test_server_arguments_checked_without_gpu():
     assert L.hbp_server_create(0, 1 << 30, 2, C.byref(p), C.byref(h)) == 1  # LR post not served
     assert E.request_bytes(720, 496, 128) > 720 * 496 * 128
     assert L.hbp_poll(None, 1) == 1
+
+
+@pytest.mark.gpu
+def test_device_memory_returns_after_contexts_and_servers(gpu):
+    """Destroying a context or a server frees its slabs, including the slabs the
+    server's pool frees to make room for a larger pair."""
+    E = gpu
+    import torch
+    from scenes import make_scene
+    small, big = make_scene(160, 120, 48, 40), make_scene(320, 240, 64, 41)
+    prm = E.default_params(post=1)
+
+    def cycle():
+        ctx = E.Context(0)
+        ctx.run_pair(small.left, small.right, 48, prm)
+        ctx.close()
+        need = E.request_bytes(320, 240, 64)
+        srv = E.Server(0, budget_bytes=need + need // 2, prep_lanes=1, params=prm)
+        for s, D in ((small, 48), (big, 64), (small, 48), (big, 64)):
+            srv.wait(srv.submit(s.left, s.right, D))
+        srv.close()
+
+    cycle()  # the first use loads modules and creates the runtime's own state
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        cycle()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < (64 << 20), (free0, free1)
