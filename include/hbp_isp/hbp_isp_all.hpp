@@ -5,3 +5,4 @@
 #include "post_process.hpp"
 #include "segment.hpp"
 #include "stereo_cost.hpp"
+#include "io.hpp"
