@@ -69,6 +69,10 @@ def parse():
                          "FP16 vs FP32 messages; serve: Poisson arrivals of a size mix")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="skip the untimed extra batches (accuracy, isolated roofline): for profiler captures")
+    ap.add_argument("--bp-streams", type=int, default=0,
+                    help="BP streams of a batch (0: the engine's default; 1 for profiler captures)")
     ap.add_argument("--window", type=int, default=0,
                     help="served requests in flight (default: the pairs per step)")
     ap.add_argument("--breakdown", action="store_true",
@@ -391,6 +395,8 @@ def main():
     arrR = (C.c_void_p * NP)(*[t.data_ptr() for t in dR])
     arrD = (C.c_void_p * NP)(*[t.data_ptr() for t in disp])
 
+    E._check(E.lib().hbp_set_bp_streams(ctx.h, args.bp_streams))
+
     def step():
         E._check(E.lib().hbp_run_batch_d(ctx.h, NP, arrL, arrR, W, H, D, C.byref(prm), arrD, None))
 
@@ -430,7 +436,7 @@ def main():
     # the same kernel alone on the device: one more batch (untimed) with the
     # BP on a single stream, every 16th data-cost launch event-timed
     iso = None
-    if rank == 0:
+    if rank == 0 and not args.profile_run:
         E._check(E.lib().hbp_set_bp_streams(ctx.h, 1))
         E._check(E.lib().hbp_profile_enable(ctx.h, 2))
         with torch.cuda.stream(stream):
@@ -439,7 +445,7 @@ def main():
         ims, ilaunch, ibytes, ipix = C.c_double(), C.c_long(), C.c_double(), C.c_double()
         E._check(E.lib().hbp_profile_read(ctx.h, C.byref(ims), C.byref(ilaunch), C.byref(ibytes), C.byref(ipix)))
         E._check(E.lib().hbp_profile_enable(ctx.h, 0))
-        E._check(E.lib().hbp_set_bp_streams(ctx.h, 0))
+        E._check(E.lib().hbp_set_bp_streams(ctx.h, args.bp_streams))
         iso = (ims.value, ilaunch.value, ibytes.value, ipix.value)
     t_max = max_over_ranks(ms, dist, "cuda")
     value = whole_job_rate(NP, args.steps, world, t_max / 1e3)
@@ -447,7 +453,7 @@ def main():
     # accuracy of the FP16 messages at this workload: the same batch with FP32
     # messages, pixel agreement and bad-2.0 against the generator's ground truth
     accuracy = None
-    if args.fp16 and rank == 0:
+    if args.fp16 and rank == 0 and not args.profile_run:
         prm32 = E.default_params(msg_fp16=0, post=1)
         d16 = [t.cpu().numpy() for t in disp]
         E._check(E.lib().hbp_run_batch_d(ctx.h, NP, arrL, arrR, W, H, D, C.byref(prm32), arrD, None))
