@@ -532,7 +532,10 @@ __device__ __forceinline__ void ransac_thread(const LevelDev &l, const Common &c
     const int cn = l.pix_off[n + 1] - l.pix_off[n], cp = l.pix_off[n];
     if (cn <= 0)
         return;
-    uint32_t xy[3] = {0, 0, 0};
+    // all draws first, then the pixel and WTA loads of the four candidates
+    // together (two memory round trips instead of eight)
+    int idx[P][3];
+#pragma unroll
     for (int p = 0; p < P; ++p)
     {
         s = lcg(s);
@@ -555,21 +558,28 @@ __device__ __forceinline__ void ransac_thread(const LevelDev &l, const Common &c
             else if (p2 == p1)
                 p2 = (p0 == cn - 2) ? cn - 1 : cn - 2;
         }
-        xy[0] = l.pix[cp + p0];
-        xy[1] = l.pix[cp + p1];
-        xy[2] = l.pix[cp + p2];
-        float X[3], Y[3], Z[3];
+        idx[p][0] = p0;
+        idx[p][1] = p1;
+        idx[p][2] = p2;
+    }
+    uint32_t xy[P][3];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-        {
-            int x = px_x(xy[k]), y = px_y(xy[k]);
-            X[k] = (float)x;
-            Y[k] = (float)y;
-            Z[k] = c.wta[(size_t)y * c.W + x];
-        }
-        l.plane[(size_t)n * K + 2 * P + p] = fit_plane(X[0], Y[0], Z[0], X[1], Y[1], Z[1], X[2], Y[2], Z[2]);
-    }
-    l.pid[n] = make_int4((int)xy[0], (int)xy[1], (int)xy[2], 0);
+            xy[p][k] = l.pix[cp + idx[p][k]];
+    float Z[P][3];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            Z[p][k] = c.wta[(size_t)px_y(xy[p][k]) * c.W + px_x(xy[p][k])];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+        l.plane[(size_t)n * K + 2 * P + p] =
+            fit_plane((float)px_x(xy[p][0]), (float)px_y(xy[p][0]), Z[p][0], (float)px_x(xy[p][1]),
+                      (float)px_y(xy[p][1]), Z[p][1], (float)px_x(xy[p][2]), (float)px_y(xy[p][2]), Z[p][2]);
+    l.pid[n] = make_int4((int)xy[P - 1][0], (int)xy[P - 1][1], (int)xy[P - 1][2], 0);
     *s_out = s;
 }
 
