@@ -543,6 +543,47 @@ hbp_status hbp_infer_d(hbp_ctx *c, const uint8_t *vol, const float *wta, int D, 
     });
 }
 
+size_t hbp_volume_f32_bytes(int W, int H, int D)
+{
+    return W > 0 && H > 0 && D > 0 ? volume_f32_bytes(W, H, D) : 0;
+}
+
+hbp_status hbp_cost_f32_d(hbp_ctx *c, const float *src, int W, int H, int D, float tau, float *vol, float *wta,
+                          void *stream)
+{
+    if (!c || !src || !vol || !wta || !(tau > 0.0f))
+        return fail(HBP_ERR_INVALID_ARG, "null pointer or tau <= 0");
+    return guarded([&] {
+        check_dims(W, H, D);
+        HBP_CUDA(cudaSetDevice(c->device));
+        launch_ingest_f32(src, W, H, D, tau, vol, wta, pick(c, stream));
+    });
+}
+
+hbp_status hbp_infer_f32_d(hbp_ctx *c, const float *vol, const float *wta, int D, float tau, const hbp_params *prm,
+                           float *disp, float *plane, void *stream)
+{
+    if (!c || !vol || !wta || !disp || !c->have_pyr || !(tau > 0.0f))
+        return fail(HBP_ERR_INVALID_ARG, "bad arguments, tau <= 0 or no pyramid");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        check_dims(c->pyr.W, c->pyr.H, D);
+        cudaStream_t st = pick(c, stream);
+        HbpParams q = to_params(prm, c->prof.on ? &c->prof : nullptr);
+        Slot *sl = slot_at(c, 0);
+        ensure_slot(sl, (long)c->pyr.W * c->pyr.H, D);
+        sl->mem.reset();
+        c->tmp.reset();
+        CostVolume cv;
+        cv.f32 = vol;
+        cv.tau = tau;
+        hbp_prepare(c->pyr, cv, wta, D, q, disp, plane, sl->mem, c->tmp, st, sl->plan);
+        c->tmp.reset();
+        std::vector<ViewPlan *> views{&sl->plan};
+        hbp_run_views(views, q, c->tmp, st);
+    });
+}
+
 hbp_status hbp_lr_check_d(hbp_ctx *c, const float *dispL, const float *dispR, float *planeL,
                           uint8_t *fail_mask, float *disp_out, int W, int H, void *stream)
 {

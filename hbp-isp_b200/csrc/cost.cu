@@ -12,6 +12,8 @@
 // data-cost kernel, whose warps walk compact superpixels, touches few sectors
 // per load. Values are min(popcount, 25) (exact in 8 bits; the reference's
 // float volume holds the same integers).
+#include <cfloat>
+
 #include "engine.h"
 
 namespace hbp
@@ -172,7 +174,58 @@ __global__ void __launch_bounds__(HM_THREADS)
     if (in)
         wtaR[(size_t)y * W + x] = (float)arg;
 }
+
+// The MC-CNN volume ingest (stereo_cost.cu:396-418 and WTA_D_k, :249-266):
+// src is the network's [D][H][W] float volume. Pixels left of the first
+// valid column (x <= d) take the value at x = d (fill_out_of_view_k with
+// is_left), every value is truncated at tau, and WTA keeps the first minimum.
+// Same block and tile geometry as the Hamming kernel: warp w writes tile w of
+// a 64x4 strip, 32 consecutive floats per disparity; each lane reads its row
+// segment of eight columns (32-byte sectors).
+__global__ void __launch_bounds__(HM_THREADS)
+    ingest_f32_kernel(const float *__restrict__ src, int W, int H, int D, float tau, int TX,
+                      float *__restrict__ vol, float *__restrict__ wta)
+{
+    const int xs = blockIdx.x * HM_COLS, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = (xs >> 3) + w;
+    if (tx >= TX)
+        return;
+    const int x = xs + w * VT_W + (lane & 7), y = blockIdx.y * VT_H + (lane >> 3);
+    const bool in = x < W && y < H;
+    float *out = vol + ((size_t)blockIdx.y * TX + tx) * D * VT_BYTES + lane;
+    const float *row = src + (size_t)(in ? y : 0) * W;
+    const size_t plane = (size_t)H * W;
+    float best = FLT_MAX;
+    int arg = 0;
+#pragma unroll 4
+    for (int d = 0; d < D; ++d)
+    {
+        float v = 0.0f;
+        if (in)
+        {
+            v = fminf(__ldg(row + (size_t)d * plane + max(x, d)), tau);
+            if (v < best)
+            {
+                best = v;
+                arg = d;
+            }
+        }
+        out[(size_t)d * VT_BYTES] = v;
+    }
+    if (in)
+        wta[(size_t)y * W + x] = (float)arg;
+}
 } // namespace
+
+void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta,
+                       cudaStream_t st)
+{
+    const int TX = ceil_div(W, VT_W);
+    dim3 g(ceil_div(W, HM_COLS), ceil_div(H, VT_H));
+    ingest_f32_kernel<<<g, HM_THREADS, 0, st>>>(src, W, H, D, tau, TX, vol, wta);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+}
 
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,

@@ -70,6 +70,11 @@ inline size_t volume_bytes(int W, int H, int D)
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
                  cudaStream_t st);
+// The MC-CNN path's volume: src [D][H][W] floats -> the tiled float layout
+// (volume_f32_bytes), with the out-of-view fill and truncation at tau, and WTA.
+inline size_t volume_f32_bytes(int W, int H, int D) { return volume_bytes(W, H, D) * sizeof(float); }
+void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta,
+                       cudaStream_t st);
 
 // lab.cu
 void launch_lab(const uint8_t *bgr, int n, float4 *lab, cudaStream_t st);
@@ -221,11 +226,29 @@ struct ViewPlan
     ViewPlan &operator=(const ViewPlan &) = delete;
 };
 
+// The data term's cost volume in the tiled layout: uint8 Census costs
+// (truncation 25, stereo_cost.cu:433) or floats (MC-CNN, truncation 0.5,
+// stereo_cost.cu:438). tau is also the cost of a disparity outside [0, D-1).
+struct CostVolume
+{
+    const uint8_t *u8 = nullptr;
+    const float *f32 = nullptr;
+    float tau = CENSUS_TAU;
+};
+
 // Level setup of one view (persistent data in `persist`, temporaries in `tmp`);
 // BP writes disparity (HW floats) and planes (HW x 3, may be null) there.
-void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D,
+void hbp_prepare(const Pyramid &pyr, const CostVolume &cv, const float *wta, int D,
                  const HbpParams &prm, float *disp, float *plane, Arena &persist, Arena &tmp,
                  cudaStream_t st, ViewPlan &vp);
+inline void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D,
+                        const HbpParams &prm, float *disp, float *plane, Arena &persist, Arena &tmp,
+                        cudaStream_t st, ViewPlan &vp)
+{
+    CostVolume cv;
+    cv.u8 = vol;
+    hbp_prepare(pyr, cv, wta, D, prm, disp, plane, persist, tmp, st, vp);
+}
 // HBP_ISP::run_ms for prepared views, run together to completion.
 void hbp_run_views(const std::vector<ViewPlan *> &views, const HbpParams &prm, Arena &tmp,
                    cudaStream_t st);

@@ -62,8 +62,9 @@ struct LevelDev
 struct Common
 {
     int W, H, D, TX; // TX: volume tiles per row
-    float lambda, tau, tau_smooth;
-    const uint8_t *vol; // tiled, vol_offset()
+    float lambda, tau, tau_smooth; // tau: the data cost outside [0, D-1)
+    const uint8_t *vol; // tiled, vol_offset() (Census: uint8 costs)
+    const float *volf;  // or the same layout in floats (MC-CNN); null for uint8
     const float *wta;   // HW
 };
 
@@ -89,9 +90,19 @@ __device__ __forceinline__ float pixel_cost(const Common &c, float xf, float yf,
         cost = c.tau;
     else
     {
-        const uint8_t *pv = c.vol + base + (size_t)d * VT_BYTES;
-        const float v0 = byte_to_float(pv[0]);
-        const float v1 = byte_to_float(pv[VT_BYTES]);
+        float v0, v1;
+        if (c.volf)
+        {
+            const float *pv = c.volf + base + (size_t)d * VT_BYTES;
+            v0 = pv[0];
+            v1 = pv[VT_BYTES];
+        }
+        else
+        {
+            const uint8_t *pv = c.vol + base + (size_t)d * VT_BYTES;
+            v0 = byte_to_float(pv[0]);
+            v1 = byte_to_float(pv[VT_BYTES]);
+        }
         const float fd = (float)d;
         cost = __fmaf_rn((fd + 1.0f) - d_f, v0, (d_f - fd) * v1);
     }
@@ -1181,10 +1192,12 @@ ViewPlan::~ViewPlan() { delete impl; }
 // run_ms: setup_D4, reverse_bd_id, compute_dist_color_pos, sort_clus;
 // hbp_isp.cu:871-891, :952-1019), the BP buffers, and the view descriptor.
 // Persistent data go to `persist`, sort/scan temporaries to `tmp`.
-void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D,
+void hbp_prepare(const Pyramid &pyr, const CostVolume &cv, const float *wta, int D,
                  const HbpParams &prm, float *disp, float *plane_out, Arena &persist, Arena &tmp,
                  cudaStream_t st, ViewPlan &vp)
 {
+    if ((cv.u8 != nullptr) == (cv.f32 != nullptr) || !(cv.tau > 0.0f))
+        throw StatusError{HBP_ERR_INVALID_ARG, "exactly one cost volume (uint8 or float) and tau > 0"};
     const int L = pyr.L, W = pyr.W, H = pyr.H, HW = W * H;
     const int m = prm.min_level;
     if (L < 1 || m < 0 || m > L - 1)
@@ -1192,7 +1205,7 @@ void hbp_prepare(const Pyramid &pyr, const uint8_t *vol, const float *wta, int D
     if ((int)pyr.N.size() != L || (int)pyr.E.size() != L || (int)pyr.node_off.size() != L ||
         (int)pyr.edge_off.size() != L || (int)pyr.child_base.size() != L || (int)pyr.nb_base.size() != L)
         throw StatusError{HBP_ERR_INTERNAL, "pyramid bookkeeping inconsistent"};
-    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, CENSUS_TAU, prm.tau_smooth, vol, wta};
+    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, cv.tau, prm.tau_smooth, cv.u8, cv.f32, wta};
     std::vector<LevelDev> &lv = vp.impl->lv;
     lv.assign(L, LevelDev{});
     vp.L = L;

@@ -89,6 +89,21 @@ def default_params(**kw) -> Params:
     return p
 
 
+def volume_f32_bytes(W: int, H: int, D: int) -> int:
+    """Size of the tiled float volume of the MC-CNN path."""
+    f = lib().hbp_volume_f32_bytes
+    f.restype = C.c_size_t
+    return f(W, H, D)
+
+
+def volume_f32_to_dhw(vol: np.ndarray, W: int, H: int, D: int) -> np.ndarray:
+    """Tiled float volume -> [D][H*W]."""
+    TX, TY = (W + 7) // 8, (H + 3) // 4
+    v = np.asarray(vol, np.float32)[: TX * TY * D * 32].reshape(TY, TX, D, 4, 8)
+    v = v.transpose(2, 0, 3, 1, 4).reshape(D, TY * 4, TX * 8)[:, :H, :W]
+    return np.ascontiguousarray(v.reshape(D, H * W))
+
+
 def volume_bytes(W: int, H: int, D: int) -> int:
     """Size of the tiled cost volume (see hbp_volume_bytes in the header)."""
     f = lib().hbp_volume_bytes
@@ -153,6 +168,14 @@ class Context:
     def cost_census_d(self, bgrL, bgrR, W, H, D, censusL, censusR, vol, wta, volR=None, wtaR=None):
         _check(lib().hbp_cost_census_d(self.h, _p(bgrL), _p(bgrR), W, H, D, _p(censusL), _p(censusR),
                                        _p(vol), _p(wta), _p(volR), _p(wtaR), None))
+
+    def cost_f32_d(self, src, W, H, D, tau, vol, wta):
+        _check(lib().hbp_cost_f32_d(self.h, _p(src), W, H, D, C.c_float(tau), _p(vol), _p(wta), None))
+
+    def infer_f32_d(self, vol, wta, D, tau, params: Params | None, disp, plane=None):
+        prm = params or default_params()
+        _check(lib().hbp_infer_f32_d(self.h, _p(vol), _p(wta), D, C.c_float(tau), C.byref(prm), _p(disp),
+                                     _p(plane), None))
 
     def lab_d(self, bgr, n, lab4):
         _check(lib().hbp_lab_d(self.h, _p(bgr), n, _p(lab4), None))

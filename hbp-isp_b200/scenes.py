@@ -130,3 +130,25 @@ def make_scene(W: int, H: int, D: int, seed: int, n_seg: int | None = None) -> S
         D=D,
         seed=seed,
     )
+
+
+def mccnn_like_volume(scene: Scene, D: int, seed: int) -> np.ndarray:
+    """A float matching-cost volume [D][H][W] in [0, 1] standing in for an
+    MC-CNN output (im0.acrt): the 5x5 mean of |grey_L(x) - grey_R(x - d)|
+    (column 0 where x - d < 0) scaled by 1/48, plus Gaussian noise sigma 0.02,
+    clipped to [0, 1]; seeded."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = np.array([0.114, 0.587, 0.299])
+    gl = scene.left.astype(np.float64) @ w
+    gr = scene.right.astype(np.float64) @ w
+    H, W = gl.shape
+    xs = np.arange(W)
+    out = np.empty((D, H, W), np.float32)
+    k = np.ones(5) / 5.0
+    for d in range(D):
+        diff = np.abs(gl - gr[:, np.maximum(xs - d, 0)])
+        diff = np.apply_along_axis(lambda r: np.convolve(r, k, mode="same"), 1, diff)
+        diff = np.apply_along_axis(lambda c: np.convolve(c, k, mode="same"), 0, diff)
+        out[d] = diff / 48.0
+    out += rng.normal(0.0, 0.02, out.shape)
+    return np.clip(out, 0.0, 1.0).astype(np.float32)

@@ -84,6 +84,17 @@ hbp_status hbp_cost_census_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *b
                              int D, uint32_t *censusL, uint32_t *censusR, uint8_t *vol,
                              float *wta, uint8_t *volR, float *wtaR, void *stream);
 
+/* The MC-CNN cost path: StereoCost::compute_stereo_cost("MC-CNN")
+ * (stereo_cost.cu:436-441, read_volume_from_file :396-418, WTA_D_k :249-266).
+ * src is the network's device volume [D][H][W] (float, as in im0.acrt, which
+ * the reference reads from disk). Columns x <= d take the value at x = d,
+ * values are truncated at tau (the reference uses 0.5) and WTA keeps the
+ * first minimum. vol (hbp_volume_f32_bytes) receives the volume in the tiled
+ * layout above, in floats; wta the H x W WTA disparity. */
+size_t hbp_volume_f32_bytes(int W, int H, int D);
+hbp_status hbp_cost_f32_d(hbp_ctx *ctx, const float *src, int W, int H, int D, float tau, float *vol,
+                          float *wta, void *stream);
+
 /* BGR -> CIELAB float4 (L, a, b, 1) (imutil.cu:4-40, segment.cu:795-809). */
 hbp_status hbp_lab_d(hbp_ctx *ctx, const uint8_t *bgr, long n, float *lab4, void *stream);
 
@@ -110,6 +121,11 @@ hbp_status hbp_pyramid_copy(hbp_ctx *ctx, int *clus, float *mean, int *bd, int *
  * and plane labels (H x W x 3; may be NULL). */
 hbp_status hbp_infer_d(hbp_ctx *ctx, const uint8_t *vol, const float *wta, int D,
                        const hbp_params *prm, float *disp, float *plane, void *stream);
+/* The same on a float volume from hbp_cost_f32_d, with its truncation tau
+ * (also the cost of a plane outside [0, D-1); hbp_isp.cu:205-227). The
+ * reference's MC-CNN runs use alpha 1.3 (bench_MiddV3_train.sh:6). */
+hbp_status hbp_infer_f32_d(hbp_ctx *ctx, const float *vol, const float *wta, int D, float tau,
+                           const hbp_params *prm, float *disp, float *plane, void *stream);
 
 /* PostProcess::left_right_check + plane_label_to_disp (post_process.cu:4-110,
  * :373-390): updates planeL in place, writes the failure mask (0/255) and the

@@ -12,6 +12,7 @@ void orc_census(const uint8_t *img, int W, int H, uint32_t *out);
 void orc_cost_volume(const uint32_t *cL, const uint32_t *cR, int W, int H, int D, uint8_t *vol,
                      float *wta);
 void orc_cost_to_right(const uint8_t *volL, int W, int H, int D, uint8_t *volR, float *wta);
+void orc_cost_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta);
 void orc_lab_set_overrides(const uint32_t *keys, const float *vals, int n);
 void orc_lab(const uint8_t *bgr, int n, float *lab4);
 void orc_nn_grid(const float *lab4, int W, int H, int *nn, float *dist_min, int *bd);
@@ -28,6 +29,10 @@ int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, c
             const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
             float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
             float *plane, float *state_belief, float *state_plane);
+int orc_hbp_f32(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+                const int *bdl, const float *volf, const float *wta, int W, int H, int D, float data_tau,
+                float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
+                float *plane, float *state_belief, float *state_plane);
 
 // post-processing (oracle_post.cpp)
 void orc_lr_check(const float *dispL, const float *dispR, float *planeL, int W, int H,

@@ -2,6 +2,7 @@
 // oracle_common.h). Each function cites the reference code it restates.
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 
 #include "oracle_api.h"
 #include "oracle_common.h"
@@ -74,6 +75,33 @@ void orc_cost_volume(const uint32_t *cL, const uint32_t *cR, int W, int H, int D
             }
             if (wta)
                 wta[p] = (float)arg;
+        }
+}
+
+// StereoCost::compute_stereo_cost("MC-CNN") (stereo_cost.cu:436-444):
+// read_volume_from_file (:396-418) copies the network's [D][H][W] volume,
+// fill_out_of_view_k (:367-390, is_left) gives columns x <= d the value at
+// x = d, truncate_data_k (:231-246) takes fminf(v, tau), and WTA_D_k
+// (:249-266) keeps the first minimum. vol is [D][H*W] floats.
+void orc_cost_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta)
+{
+    const size_t n = (size_t)W * H;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+        {
+            float best = FLT_MAX;
+            int arg = 0;
+            for (int d = 0; d < D; ++d)
+            {
+                const float v = std::fmin(src[((size_t)d * H + y) * W + (x > d ? x : d)], tau);
+                vol[(size_t)d * n + (size_t)y * W + x] = v;
+                if (v < best)
+                {
+                    best = v;
+                    arg = d;
+                }
+            }
+            wta[(size_t)y * W + x] = (float)arg;
         }
 }
 

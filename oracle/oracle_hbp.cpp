@@ -73,7 +73,8 @@ struct Engine
 {
     int W, H, D, L;
     R lambda, tau, tau_smooth;
-    const uint8_t *vol; // D x HW
+    const uint8_t *vol;           // D x HW (Census: uint8 costs)
+    const float *volf = nullptr;  // or floats (MC-CNN); used when set
     const float *wta;
     std::vector<Level<R>> lv;
     std::vector<R> msg, msg_t;
@@ -101,7 +102,17 @@ struct Engine
         else
         {
             const size_t n = (size_t)W * H;
-            R v0 = (R)vol[(size_t)d * n + px], v1 = (R)vol[(size_t)(d + 1) * n + px];
+            R v0, v1;
+            if (volf)
+            {
+                v0 = (R)volf[(size_t)d * n + px];
+                v1 = (R)volf[(size_t)(d + 1) * n + px];
+            }
+            else
+            {
+                v0 = (R)vol[(size_t)d * n + px];
+                v1 = (R)vol[(size_t)(d + 1) * n + px];
+            }
             cost = std::fma((R)(d + 1) - d_f, v0, (d_f - (R)d) * v1);
         }
         return lambda * cost;
@@ -578,7 +589,8 @@ template <typename R>
 int run(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
         const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
         float tau_smooth, int min_level, long max_steps, float *disp, float *plane_out,
-        float *state_belief, float *state_plane, bool fp16_msg = false)
+        float *state_belief, float *state_plane, bool fp16_msg = false, const float *volf = nullptr,
+        float data_tau = 25.0f)
 {
     if (L < 1 || min_level < 0 || min_level > L - 1)
         return -1;
@@ -588,9 +600,10 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
     eng.D = D;
     eng.L = L;
     eng.lambda = (R)alpha;
-    eng.tau = (R)25.0f;
+    eng.tau = (R)data_tau; // StereoCost::m_tau: 25 Census, 0.5 MC-CNN (stereo_cost.cu:421-441)
     eng.tau_smooth = (R)tau_smooth;
     eng.vol = vol;
+    eng.volf = volf;
     eng.wta = wta;
     eng.max_steps = max_steps;
     eng.fp16_msg = fp16_msg;
@@ -689,6 +702,24 @@ int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, c
                            state_plane);
     return run<float>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth,
                       min_level, max_steps, disp, plane, state_belief, state_plane);
+}
+
+// The same on a float cost volume [D][H*W] (the MC-CNN path,
+// stereo_cost.cu:436-441: StereoData copies the float volume and m_tau =
+// data_tau, hbp_isp.hpp:91-105). Modes as orc_hbp.
+int orc_hbp_f32(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+                const int *bdl, const float *volf, const float *wta, int W, int H, int D, float data_tau,
+                float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
+                float *plane, float *state_belief, float *state_plane)
+{
+    if (!volf || !(data_tau > 0.0f))
+        return -1;
+    if (mode == 1)
+        return run<double>(level_sizes, L, clus, mean, bd, bdl, nullptr, wta, W, H, D, alpha, tau_smooth,
+                           min_level, max_steps, disp, plane, state_belief, state_plane, false, volf,
+                           data_tau);
+    return run<float>(level_sizes, L, clus, mean, bd, bdl, nullptr, wta, W, H, D, alpha, tau_smooth, min_level,
+                      max_steps, disp, plane, state_belief, state_plane, mode == 2, volf, data_tau);
 }
 
 } // extern "C"

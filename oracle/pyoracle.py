@@ -41,6 +41,10 @@ def lib():
         _lib.orc_hbp.restype = C.c_int
         _lib.orc_hbp.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
                                  C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
+        _lib.orc_hbp_f32.restype = C.c_int
+        _lib.orc_hbp_f32.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
+                                     C.c_float, C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
+        _lib.orc_cost_f32.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
     return _lib
 
 
@@ -194,6 +198,45 @@ def cost_stage(L, R, D):
     cL, cR = census(gL), census(gR)
     vol, wta = cost_volume(cL, cR, D)
     return dict(greyL=gL, greyR=gR, censusL=cL, censusR=cR, vol=vol, wta=wta)
+
+
+def cost_f32(src, tau=0.5):
+    """The MC-CNN cost path on a float volume src [D][H][W]: (vol [D][H*W], wta HxW)."""
+    src = np.ascontiguousarray(src, np.float32)
+    D, H, W = src.shape
+    vol = np.zeros((D, H * W), np.float32)
+    wta = np.zeros((H, W), np.float32)
+    lib().orc_cost_f32(_p(src), W, H, D, tau, _p(vol), _p(wta))
+    return vol, wta
+
+
+def hbp_f32(seg, volf, wta, W, H, D, tau=0.5, alpha=1.3, tau_smooth=0.6, min_level=2, fp64=False,
+            fp16_msg=False):
+    """HBP on a float cost volume [D][H*W] (the MC-CNN path): (disparity, plane)."""
+    sizes = np.ascontiguousarray(seg["level_sizes"], np.int32)
+    L = sizes.shape[0]
+    disp = np.zeros((H, W), np.float32)
+    plane = np.zeros((H, W, 3), np.float32)
+    mean = np.ascontiguousarray(seg["mean"], np.float32)
+    steps = lib().orc_hbp_f32(_p(sizes), L, _p(np.ascontiguousarray(seg["clus"], np.int32)), _p(mean),
+                              _p(np.ascontiguousarray(seg["bd"], np.int32)),
+                              _p(np.ascontiguousarray(seg["bdl"], np.int32)),
+                              _p(np.ascontiguousarray(volf, np.float32)), _p(np.ascontiguousarray(wta, np.float32)),
+                              W, H, D, tau, alpha, tau_smooth, min_level, 2 if fp16_msg else int(fp64), -1,
+                              _p(disp), _p(plane), None, None)
+    if steps < 0:
+        raise ValueError("orc_hbp_f32 rejected its input")
+    return disp, plane
+
+
+def pipeline_f32(L, src, tau=0.5, alpha=1.3, tau_smooth=0.6, min_level=2):
+    """The reference's MC-CNN single-view path (main_bench_middv3.cu:73-108 with
+    cost "MC-CNN"): the volume ingest, the left image's pyramid and HBP."""
+    D, H, W = np.asarray(src).shape
+    vol, wta = cost_f32(src, tau)
+    seg = segment(lab(L))
+    disp, plane = hbp_f32(seg, vol, wta, W, H, D, tau, alpha, tau_smooth, min_level)
+    return dict(disp=disp, plane=plane, vol=vol, wta=wta, seg=seg)
 
 
 def pipeline(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False, right_view=False,

@@ -8,7 +8,9 @@
 // code on a CUDA error, and runs synchronously on the legacy default stream
 // exactly as the reference drivers do (main_stereo_hbp_isp.cu:31-76).
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <unistd.h>
 #include <vector>
 
 #include "hbp_isp.hpp"
@@ -289,6 +291,59 @@ int ref_post(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, float *disp
     std::memcpy(dispL, left.first.data, n * 4);
     std::memcpy(planeL, left.second.data, n * 12);
     return 0;
+}
+
+// The MC-CNN single-view path (main_bench_middv3.cu:73-108 with cost
+// "MC-CNN"): the float volume src [D][H][W] goes through the reference's own
+// file reader (stereo_cost.cu:396-418: out-of-view fill, truncation at 0.5)
+// from a raw temporary file, then WTA, SegHAC on the left image and
+// HBP_ISP(alpha, tau_smooth).run_ms(min_level). vol_f32 ([D][HW]) and wta
+// receive the stored volume and WTA (optional). Returns the number of levels.
+int ref_hbp_f32(const uint8_t *bgrL, const uint8_t *bgrR, const float *src, int W, int H, int D,
+                float alpha, float tau_smooth, int min_level, float *vol_f32, float *wta, float *disp,
+                float *plane)
+{
+    char path[] = "/tmp/hbpref_volXXXXXX";
+    int fd = mkstemp(path);
+    if (fd < 0)
+        return -1000;
+    size_t n = (size_t)W * H, bytes = n * D * sizeof(float);
+    bool ok = write(fd, src, bytes) == (ssize_t)bytes;
+    close(fd);
+    if (!ok)
+    {
+        unlink(path);
+        return -1001;
+    }
+    int levels = 0;
+    int rc;
+    {
+        cv::Mat L = wrap_bgr(bgrL, W, H), R = wrap_bgr(bgrR, W, H);
+        SegHAC *seg = new SegHAC(L, CentoridLink, 4, 0.0, LabelISPFormat, 1, false);
+        seg->run_ms();
+        ISPData *isp = new ISPData(seg);
+        levels = (int)seg->g_num_clus_isp().size();
+        delete seg;
+        StereoCost *sc = new StereoCost(L, R, D, std::string(path));
+        sc->compute_stereo_cost("MC-CNN");
+        d2h(vol_f32, sc->g_img_cost_d(), n * D);
+        d2h(wta, sc->g_img_D_d(), n);
+        StereoData *sd = new StereoData(sc, true);
+        delete sc;
+        HBP_ISP *hbp = new HBP_ISP(isp, sd, alpha, tau_smooth);
+        std::pair<cv::Mat, cv::Mat> res = hbp->run_ms(min_level);
+        rc = last_error();
+        std::memcpy(disp, res.first.data, sizeof(float) * n);
+        std::memcpy(plane, res.second.data, sizeof(float) * n * 3);
+        delete hbp;
+        delete sd;
+        delete isp;
+    }
+    unlink(path);
+    int rc2 = last_error();
+    if (rc || rc2)
+        return rc ? rc : rc2;
+    return levels;
 }
 
 } // extern "C"

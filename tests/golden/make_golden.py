@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir>
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -22,7 +22,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, os.path.join(ROOT, "hbp-isp_b200"))
-from scenes import make_scene  # noqa: E402
+from scenes import make_scene, mccnn_like_volume  # noqa: E402
 
 P = C.c_void_p
 
@@ -38,10 +38,12 @@ class RefLib:
         path = path or os.path.join(ROOT, "oracle", "_ref", "libhbpref.so")
         self.lib = C.CDLL(path)
         for name in ("ref_grey", "ref_lab", "ref_1nn_grid", "ref_crtrees", "ref_cost",
-                     "ref_segment", "ref_hbp_pair", "ref_post"):
+                     "ref_segment", "ref_hbp_pair", "ref_post", "ref_hbp_f32"):
             getattr(self.lib, name).restype = C.c_int
         self.lib.ref_hbp_pair.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_int, C.c_int, P, P]
+        self.lib.ref_hbp_f32.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                                         P, P, P, P]
 
     def grey(self, bgr):
         H, W, _ = bgr.shape
@@ -111,6 +113,17 @@ class RefLib:
                                        int(right_view), ptr(disp), ptr(plane))
         assert levels > 0, levels
         return disp, plane, levels
+
+    def hbp_f32(self, L, R, src, alpha=1.3, tau_smooth=0.6, min_level=2):
+        D, H, W = src.shape
+        vol = np.zeros((D, H * W), np.float32)
+        wta = np.zeros((H, W), np.float32)
+        disp = np.zeros((H, W), np.float32)
+        plane = np.zeros((H, W, 3), np.float32)
+        levels = self.lib.ref_hbp_f32(ptr(L), ptr(R), ptr(np.ascontiguousarray(src, np.float32)), W, H, D,
+                                      alpha, tau_smooth, min_level, ptr(vol), ptr(wta), ptr(disp), ptr(plane))
+        assert levels > 0, levels
+        return vol, wta, disp, plane, levels
 
     def post(self, L, R, dispL, planeL, dispR, planeR, median=True):
         H, W, _ = L.shape
@@ -208,13 +221,35 @@ def scene_record(ref: RefLib, W, H, D, seed, full: bool):
     return rec
 
 
+MCCNN_CASES = [(96, 64, 32, 7, "mccnn_96x64_d32_s7"), (160, 120, 48, 11, "mccnn_160x120_d48_s11")]
+
+
+def mccnn_record(ref: RefLib, W, H, D, seed):
+    """The MC-CNN path on a seeded synthetic float volume (scenes.mccnn_like_volume
+    with seed + 1; the tests regenerate it and check its hash)."""
+    s = make_scene(W, H, D, seed)
+    src = mccnn_like_volume(s, D, seed + 1)
+    vol, wta, disp, plane, levels = ref.hbp_f32(s.left, s.right, src)
+    return dict(W=W, H=H, D=D, seed=seed, sha_src=sha(src), sha_vol_f32=sha(vol),
+                wta=wta.astype(np.uint16), disp=disp, plane=plane, levels=levels)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
+    ap.add_argument("--only", choices=["census", "mccnn"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     ref = RefLib(args.lib)
+
+    if args.only != "census":
+        for (W, H, D, seed, name) in MCCNN_CASES:
+            rec = mccnn_record(ref, W, H, D, seed)
+            np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
+            print(name, "levels", rec["levels"])
+    if args.only == "mccnn":
+        return
 
     for (W, H, D, seed, full, name) in [
         (96, 64, 32, 7, True, "tiny_96x64_d32_s7"),
