@@ -549,14 +549,16 @@ size_t hbp_volume_f32_bytes(int W, int H, int D)
 }
 
 hbp_status hbp_cost_f32_d(hbp_ctx *c, const float *src, int W, int H, int D, float tau, float *vol, float *wta,
-                          void *stream)
+                          float *volR, float *wtaR, void *stream)
 {
-    if (!c || !src || !vol || !wta || !(tau > 0.0f))
+    if (!c || !src || !(tau > 0.0f))
         return fail(HBP_ERR_INVALID_ARG, "null pointer or tau <= 0");
+    if (!vol != !wta || !volR != !wtaR || (!vol && !volR))
+        return fail(HBP_ERR_INVALID_ARG, "give vol and wta, volR and wtaR, or both pairs");
     return guarded([&] {
         check_dims(W, H, D);
         HBP_CUDA(cudaSetDevice(c->device));
-        launch_ingest_f32(src, W, H, D, tau, vol, wta, pick(c, stream));
+        launch_ingest_f32(src, W, H, D, tau, vol, wta, volR, wtaR, pick(c, stream));
     });
 }
 

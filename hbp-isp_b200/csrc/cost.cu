@@ -179,9 +179,14 @@ __global__ void __launch_bounds__(HM_THREADS)
 // src is the network's [D][H][W] float volume. Pixels left of the first
 // valid column (x <= d) take the value at x = d (fill_out_of_view_k with
 // is_left), every value is truncated at tau, and WTA keeps the first minimum.
+// RIGHT: the same volume after cost_to_right (:488-516): convert_vol_L2R_k
+// shifts each (d, y) row left by d and fill_out_of_view_k repeats column
+// W-1-d to the right, so VR[d][y][x] = VL[d][y][min(x + d, W - 1)], which is
+// min(src[d][y][min(x + d, W - 1)], tau) because min(x + d, W - 1) >= d.
 // Same block and tile geometry as the Hamming kernel: warp w writes tile w of
 // a 64x4 strip, 32 consecutive floats per disparity; each lane reads its row
 // segment of eight columns (32-byte sectors).
+template <bool RIGHT>
 __global__ void __launch_bounds__(HM_THREADS)
     ingest_f32_kernel(const float *__restrict__ src, int W, int H, int D, float tau, int TX,
                       float *__restrict__ vol, float *__restrict__ wta)
@@ -203,7 +208,7 @@ __global__ void __launch_bounds__(HM_THREADS)
         float v = 0.0f;
         if (in)
         {
-            v = fminf(__ldg(row + (size_t)d * plane + max(x, d)), tau);
+            v = fminf(__ldg(row + (size_t)d * plane + (RIGHT ? min(x + d, W - 1) : max(x, d))), tau);
             if (v < best)
             {
                 best = v;
@@ -217,14 +222,23 @@ __global__ void __launch_bounds__(HM_THREADS)
 }
 } // namespace
 
-void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta,
-                       cudaStream_t st)
+void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta, float *volR,
+                       float *wtaR, cudaStream_t st)
 {
     const int TX = ceil_div(W, VT_W);
     dim3 g(ceil_div(W, HM_COLS), ceil_div(H, VT_H));
-    ingest_f32_kernel<<<g, HM_THREADS, 0, st>>>(src, W, H, D, tau, TX, vol, wta);
-    note_launch();
-    HBP_LAUNCH_CHECK();
+    if (vol)
+    {
+        ingest_f32_kernel<false><<<g, HM_THREADS, 0, st>>>(src, W, H, D, tau, TX, vol, wta);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+    }
+    if (volR)
+    {
+        ingest_f32_kernel<true><<<g, HM_THREADS, 0, st>>>(src, W, H, D, tau, TX, volR, wtaR);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+    }
 }
 
 void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, uint32_t *cL,

@@ -71,10 +71,11 @@ void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, 
                  uint32_t *cR, uint8_t *vol, float *wta, uint8_t *volR, float *wtaR,
                  cudaStream_t st);
 // The MC-CNN path's volume: src [D][H][W] floats -> the tiled float layout
-// (volume_f32_bytes), with the out-of-view fill and truncation at tau, and WTA.
+// (volume_f32_bytes), with the out-of-view fill and truncation at tau, and WTA;
+// the left view into vol/wta and (each pair optional) the right view into volR/wtaR.
 inline size_t volume_f32_bytes(int W, int H, int D) { return volume_bytes(W, H, D) * sizeof(float); }
-void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta,
-                       cudaStream_t st);
+void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta, float *volR,
+                       float *wtaR, cudaStream_t st);
 
 // lab.cu
 void launch_lab(const uint8_t *bgr, int n, float4 *lab, cudaStream_t st);

@@ -169,8 +169,9 @@ class Context:
         _check(lib().hbp_cost_census_d(self.h, _p(bgrL), _p(bgrR), W, H, D, _p(censusL), _p(censusR),
                                        _p(vol), _p(wta), _p(volR), _p(wtaR), None))
 
-    def cost_f32_d(self, src, W, H, D, tau, vol, wta):
-        _check(lib().hbp_cost_f32_d(self.h, _p(src), W, H, D, C.c_float(tau), _p(vol), _p(wta), None))
+    def cost_f32_d(self, src, W, H, D, tau, vol, wta, volR=None, wtaR=None):
+        _check(lib().hbp_cost_f32_d(self.h, _p(src), W, H, D, C.c_float(tau), _p(vol), _p(wta), _p(volR),
+                                    _p(wtaR), None))
 
     def infer_f32_d(self, vol, wta, D, tau, params: Params | None, disp, plane=None):
         prm = params or default_params()

@@ -90,10 +90,12 @@ hbp_status hbp_cost_census_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *b
  * the reference reads from disk). Columns x <= d take the value at x = d,
  * values are truncated at tau (the reference uses 0.5) and WTA keeps the
  * first minimum. vol (hbp_volume_f32_bytes) receives the volume in the tiled
- * layout above, in floats; wta the H x W WTA disparity. */
+ * layout above, in floats; wta the H x W WTA disparity. volR / wtaR receive
+ * the volume after cost_to_right (stereo_cost.cu:488-516) and its WTA. Either
+ * pair may be NULL, not both. */
 size_t hbp_volume_f32_bytes(int W, int H, int D);
 hbp_status hbp_cost_f32_d(hbp_ctx *ctx, const float *src, int W, int H, int D, float tau, float *vol,
-                          float *wta, void *stream);
+                          float *wta, float *volR, float *wtaR, void *stream);
 
 /* BGR -> CIELAB float4 (L, a, b, 1) (imutil.cu:4-40, segment.cu:795-809). */
 hbp_status hbp_lab_d(hbp_ctx *ctx, const uint8_t *bgr, long n, float *lab4, void *stream);

@@ -1,6 +1,6 @@
 // ISPData, StereoData and HBP_ISP with the reference's interface
 // (hbp_isp.hpp:9-126, :288): hierarchical BP on the segmentation pyramid on
-// the B200 engine (hbp_infer_d). ISPData shares its SegHAC's pyramid and
+// the B200 engine (hbp_infer_d; hbp_infer_f32_d on an MC-CNN volume). ISPData shares its SegHAC's pyramid and
 // StereoData its StereoCost's volume (the reference deep-copies both), so
 // either producer may be deleted first, as the reference's drivers do.
 // Extension: set_msg_fp16() stores the BP messages as FP16.
@@ -59,7 +59,7 @@ class StereoData
   public:
     StereoData(const StereoCost *const sc, const bool use_cost_vol)
         : m_labels(sc->g_labels()), im_size(sc->g_im_size()), width(sc->g_width()), height(sc->g_height()),
-          use_cost_vol(use_cost_vol), vol(sc->vol), wta(sc->wta)
+          use_cost_vol(use_cost_vol), f32(sc->g_is_f32()), m_tau(sc->g_tau()), vol(sc->vol), wta(sc->wta)
     {
         if (!use_cost_vol)
             throw std::invalid_argument("StereoData: the path runs on the cost volume (use_cost_vol = true)");
@@ -70,11 +70,13 @@ class StereoData
     int g_im_size() const { return im_size; }
     float *g_im_D_d() const { return wta->as<float>(); }
     bool g_use_cost_vol() const { return use_cost_vol; }
-    const uint8_t *g_img_cost_d() const { return vol->as<uint8_t>(); }
-    float g_tau() const { return 25.0f; }
+    const uint8_t *g_img_cost_d() const { return f32 ? nullptr : vol->as<uint8_t>(); }
+    const float *g_img_cost_f32_d() const { return f32 ? vol->as<float>() : nullptr; }
+    float g_tau() const { return m_tau; }
 
     int m_labels, im_size, width, height;
-    bool use_cost_vol;
+    bool use_cost_vol, f32;
+    float m_tau;
     detail::Buf vol, wta;
 };
 
@@ -103,8 +105,12 @@ class HBP_ISP
         p.msg_fp16 = fp16 ? 1 : 0;
         p.post = 0;
         detail::Buf d = std::make_shared<detail::DevBuf>(4 * n), pl = std::make_shared<detail::DevBuf>(12 * n);
-        detail::check(hbp_infer_d(isp->ctx->h, sd->vol->as<uint8_t>(), sd->wta->as<float>(), sd->m_labels, &p,
-                                  d->as<float>(), pl->as<float>(), nullptr));
+        if (sd->f32)
+            detail::check(hbp_infer_f32_d(isp->ctx->h, sd->vol->as<float>(), sd->wta->as<float>(), sd->m_labels,
+                                          sd->m_tau, &p, d->as<float>(), pl->as<float>(), nullptr));
+        else
+            detail::check(hbp_infer_d(isp->ctx->h, sd->vol->as<uint8_t>(), sd->wta->as<float>(), sd->m_labels, &p,
+                                      d->as<float>(), pl->as<float>(), nullptr));
         Mat disp(isp->height, isp->width, MAT_32FC1), plane(isp->height, isp->width, MAT_32FC3);
         detail::download(disp, d);
         detail::download(plane, pl);

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <vector>
 
 #include "oracle_api.h"
 #include "oracle_common.h"
@@ -103,6 +104,40 @@ void orc_cost_f32(const float *src, int W, int H, int D, float tau, float *vol, 
             }
             wta[(size_t)y * W + x] = (float)arg;
         }
+}
+
+// The same volume after StereoCost::cost_to_right (stereo_cost.cu:488-516),
+// stated as the reference's three steps on the left volume: convert_vol_L2R_k
+// (:471-486) moves each (d, y) row left by d in place, fill_out_of_view_k
+// (:367-390, right side) copies column W-1-d over columns W-1-d .. W-1, and
+// WTA_D_k keeps the first minimum.
+void orc_cost_f32_right(const float *src, int W, int H, int D, float tau, float *volR, float *wta)
+{
+    const size_t n = (size_t)W * H;
+    std::vector<float> wl(n);
+    orc_cost_f32(src, W, H, D, tau, volR, wl.data());
+    for (int d = 0; d < D; ++d)
+        for (int y = 0; y < H; ++y)
+        {
+            float *row = volR + (size_t)d * n + (size_t)y * W;
+            for (int x = 0; x + d < W; ++x)
+                row[x] = row[x + d];
+            const float c = row[W - 1 - d];
+            for (int x = 0; x <= d; ++x)
+                row[W - 1 - x] = c;
+        }
+    for (size_t p = 0; p < n; ++p)
+    {
+        float best = FLT_MAX;
+        int arg = 0;
+        for (int d = 0; d < D; ++d)
+            if (volR[(size_t)d * n + p] < best)
+            {
+                best = volR[(size_t)d * n + p];
+                arg = d;
+            }
+        wta[p] = (float)arg;
+    }
 }
 
 // StereoCost::cost_to_right (stereo_cost.cu:488-516): convert_vol_L2R_k shifts

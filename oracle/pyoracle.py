@@ -45,6 +45,7 @@ def lib():
         _lib.orc_hbp_f32.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
                                      C.c_float, C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
         _lib.orc_cost_f32.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
+        _lib.orc_cost_f32_right.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
     return _lib
 
 
@@ -200,13 +201,15 @@ def cost_stage(L, R, D):
     return dict(greyL=gL, greyR=gR, censusL=cL, censusR=cR, vol=vol, wta=wta)
 
 
-def cost_f32(src, tau=0.5):
-    """The MC-CNN cost path on a float volume src [D][H][W]: (vol [D][H*W], wta HxW)."""
+def cost_f32(src, tau=0.5, right=False):
+    """The MC-CNN cost path on a float volume src [D][H][W]: (vol [D][H*W], wta HxW);
+    right: the volume after cost_to_right."""
     src = np.ascontiguousarray(src, np.float32)
     D, H, W = src.shape
     vol = np.zeros((D, H * W), np.float32)
     wta = np.zeros((H, W), np.float32)
-    lib().orc_cost_f32(_p(src), W, H, D, tau, _p(vol), _p(wta))
+    f = lib().orc_cost_f32_right if right else lib().orc_cost_f32
+    f(_p(src), W, H, D, tau, _p(vol), _p(wta))
     return vol, wta
 
 
@@ -229,12 +232,13 @@ def hbp_f32(seg, volf, wta, W, H, D, tau=0.5, alpha=1.3, tau_smooth=0.6, min_lev
     return disp, plane
 
 
-def pipeline_f32(L, src, tau=0.5, alpha=1.3, tau_smooth=0.6, min_level=2):
+def pipeline_f32(L, src, tau=0.5, alpha=1.3, tau_smooth=0.6, min_level=2, R=None):
     """The reference's MC-CNN single-view path (main_bench_middv3.cu:73-108 with
-    cost "MC-CNN"): the volume ingest, the left image's pyramid and HBP."""
+    cost "MC-CNN"): the volume ingest, the left image's pyramid and HBP. With
+    the right image R: its right view (main_bench_middv3.cu:189-203)."""
     D, H, W = np.asarray(src).shape
-    vol, wta = cost_f32(src, tau)
-    seg = segment(lab(L))
+    vol, wta = cost_f32(src, tau, right=R is not None)
+    seg = segment(lab(L if R is None else R))
     disp, plane = hbp_f32(seg, vol, wta, W, H, D, tau, alpha, tau_smooth, min_level)
     return dict(disp=disp, plane=plane, vol=vol, wta=wta, seg=seg)
 

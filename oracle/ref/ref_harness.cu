@@ -297,11 +297,13 @@ int ref_post(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, float *disp
 // "MC-CNN"): the float volume src [D][H][W] goes through the reference's own
 // file reader (stereo_cost.cu:396-418: out-of-view fill, truncation at 0.5)
 // from a raw temporary file, then WTA, SegHAC on the left image and
-// HBP_ISP(alpha, tau_smooth).run_ms(min_level). vol_f32 ([D][HW]) and wta
-// receive the stored volume and WTA (optional). Returns the number of levels.
+// HBP_ISP(alpha, tau_smooth).run_ms(min_level). With right_view != 0, the
+// right view of main_bench_middv3.cu:189-203 instead (SegHAC on the right
+// image, cost_to_right). vol_f32 ([D][HW]) and wta receive the stored volume
+// and WTA (optional). Returns the number of levels.
 int ref_hbp_f32(const uint8_t *bgrL, const uint8_t *bgrR, const float *src, int W, int H, int D,
-                float alpha, float tau_smooth, int min_level, float *vol_f32, float *wta, float *disp,
-                float *plane)
+                float alpha, float tau_smooth, int min_level, int right_view, float *vol_f32, float *wta,
+                float *disp, float *plane)
 {
     char path[] = "/tmp/hbpref_volXXXXXX";
     int fd = mkstemp(path);
@@ -319,13 +321,15 @@ int ref_hbp_f32(const uint8_t *bgrL, const uint8_t *bgrR, const float *src, int 
     int rc;
     {
         cv::Mat L = wrap_bgr(bgrL, W, H), R = wrap_bgr(bgrR, W, H);
-        SegHAC *seg = new SegHAC(L, CentoridLink, 4, 0.0, LabelISPFormat, 1, false);
+        SegHAC *seg = new SegHAC(right_view ? R : L, CentoridLink, 4, 0.0, LabelISPFormat, 1, false);
         seg->run_ms();
         ISPData *isp = new ISPData(seg);
         levels = (int)seg->g_num_clus_isp().size();
         delete seg;
         StereoCost *sc = new StereoCost(L, R, D, std::string(path));
         sc->compute_stereo_cost("MC-CNN");
+        if (right_view)
+            sc->cost_to_right();
         d2h(vol_f32, sc->g_img_cost_d(), n * D);
         d2h(wta, sc->g_img_D_d(), n);
         StereoData *sd = new StereoData(sc, true);

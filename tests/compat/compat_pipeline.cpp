@@ -4,7 +4,10 @@
 //           StereoData, HBP_ISP::run_ms, medianFilter)
 //   lr:     main_bench_middv3.cu:169-219 (both views, LR check, fill,
 //           weighted median, plane -> disparity)
+// with the Census cost (alpha 1000.1) and, given an im0.acrt-style volume
+// file, again with the MC-CNN cost (alpha 1.3, bench_MiddV3_train.sh:6).
 // usage: compat_pipeline left.bgr right.bgr W H D single.f32 lr.f32
+//                        [vol.acrt mccnn_single.f32 mccnn_lr.f32]
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -29,61 +32,70 @@ static void write_f32(const char *path, const Mat &m)
     f.write(reinterpret_cast<const char *>(m.data), (std::streamsize)m.bytes());
 }
 
+static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, const std::string &vol_dir,
+                  float alpha, const char *out_single, const char *out_lr)
+{
+    const float tau_smooth = 0.6f;
+    const int min_level = 2;
+
+    // single-pair driver
+    SegHAC *seg = new SegHAC(L, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+    seg->run_ms();
+    ISPData *isp = new ISPData(seg);
+    delete seg;
+    StereoCost *sc = new StereoCost(L, R, D, vol_dir);
+    sc->compute_stereo_cost(cost);
+    StereoData *sd = new StereoData(sc, true);
+    delete sc;
+    HBP_ISP *hbp = new HBP_ISP(isp, sd, alpha, tau_smooth);
+    auto results_left = hbp->run_ms(min_level);
+    Mat disp = results_left.first.clone();
+    medianFilter(disp);
+    write_f32(out_single, disp);
+
+    // MidV3_LR: the right view, then LR check, fill and weighted median
+    SegHAC *seg_r = new SegHAC(R, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+    seg_r->run_ms();
+    ISPData *isp_r = new ISPData(seg_r);
+    delete seg_r;
+    StereoCost *sc_r = new StereoCost(L, R, D, vol_dir);
+    sc_r->compute_stereo_cost(cost);
+    sc_r->cost_to_right();
+    StereoData *sd_r = new StereoData(sc_r, true);
+    delete sc_r;
+    HBP_ISP *hbp_r = new HBP_ISP(isp_r, sd_r, alpha, tau_smooth);
+    auto results_right = hbp_r->run_ms(min_level);
+    PostProcess *post = new PostProcess(L, R);
+    post->left_right_check(results_left, results_right);
+    post->plane_label_to_disp(results_left, results_right);
+    post->median_filter(results_left, results_right);
+    post->plane_label_to_disp(results_left, results_right);
+    write_f32(out_lr, results_left.first);
+
+    delete post;
+    delete hbp_r;
+    delete sd_r;
+    delete isp_r;
+    delete hbp;
+    delete sd;
+    delete isp;
+}
+
 int main(int argc, char **argv)
 {
-    if (argc != 8)
+    if (argc != 8 && argc != 11)
     {
-        std::fprintf(stderr, "usage: %s left.bgr right.bgr W H D single.f32 lr.f32\n", argv[0]);
+        std::fprintf(stderr, "usage: %s left.bgr right.bgr W H D single.f32 lr.f32 "
+                             "[vol.acrt mccnn_single.f32 mccnn_lr.f32]\n", argv[0]);
         return 2;
     }
     const int W = std::atoi(argv[3]), H = std::atoi(argv[4]), D = std::atoi(argv[5]);
     try
     {
         Mat L = read_bgr(argv[1], W, H), R = read_bgr(argv[2], W, H);
-        const float alpha = 1000.1f, tau_smooth = 0.6f;
-        const int min_level = 2;
-
-        // single-pair driver
-        SegHAC *seg = new SegHAC(L, CentoridLink, 4, 0, LabelISPFormat, 1, false);
-        seg->run_ms();
-        ISPData *isp = new ISPData(seg);
-        delete seg;
-        StereoCost *sc = new StereoCost(L, R, D, "");
-        sc->compute_stereo_cost("Census");
-        StereoData *sd = new StereoData(sc, true);
-        delete sc;
-        HBP_ISP *hbp = new HBP_ISP(isp, sd, alpha, tau_smooth);
-        auto results_left = hbp->run_ms(min_level);
-        Mat disp = results_left.first.clone();
-        medianFilter(disp);
-        write_f32(argv[6], disp);
-
-        // MidV3_LR: the right view, then LR check, fill and weighted median
-        SegHAC *seg_r = new SegHAC(R, CentoridLink, 4, 0, LabelISPFormat, 1, false);
-        seg_r->run_ms();
-        ISPData *isp_r = new ISPData(seg_r);
-        delete seg_r;
-        StereoCost *sc_r = new StereoCost(L, R, D, "");
-        sc_r->compute_stereo_cost("Census");
-        sc_r->cost_to_right();
-        StereoData *sd_r = new StereoData(sc_r, true);
-        delete sc_r;
-        HBP_ISP *hbp_r = new HBP_ISP(isp_r, sd_r, alpha, tau_smooth);
-        auto results_right = hbp_r->run_ms(min_level);
-        PostProcess *post = new PostProcess(L, R);
-        post->left_right_check(results_left, results_right);
-        post->plane_label_to_disp(results_left, results_right);
-        post->median_filter(results_left, results_right);
-        post->plane_label_to_disp(results_left, results_right);
-        write_f32(argv[7], results_left.first);
-
-        delete post;
-        delete hbp_r;
-        delete sd_r;
-        delete isp_r;
-        delete hbp;
-        delete sd;
-        delete isp;
+        flows(L, R, D, "Census", "", 1000.1f, argv[6], argv[7]);
+        if (argc == 11)
+            flows(L, R, D, "MC-CNN", argv[8], 1.3f, argv[9], argv[10]);
     }
     catch (const std::exception &e)
     {

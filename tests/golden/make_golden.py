@@ -43,7 +43,7 @@ class RefLib:
         self.lib.ref_hbp_pair.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_int, C.c_int, P, P]
         self.lib.ref_hbp_f32.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
-                                         P, P, P, P]
+                                         C.c_int, P, P, P, P]
 
     def grey(self, bgr):
         H, W, _ = bgr.shape
@@ -114,14 +114,15 @@ class RefLib:
         assert levels > 0, levels
         return disp, plane, levels
 
-    def hbp_f32(self, L, R, src, alpha=1.3, tau_smooth=0.6, min_level=2):
+    def hbp_f32(self, L, R, src, alpha=1.3, tau_smooth=0.6, min_level=2, right_view=False):
         D, H, W = src.shape
         vol = np.zeros((D, H * W), np.float32)
         wta = np.zeros((H, W), np.float32)
         disp = np.zeros((H, W), np.float32)
         plane = np.zeros((H, W, 3), np.float32)
         levels = self.lib.ref_hbp_f32(ptr(L), ptr(R), ptr(np.ascontiguousarray(src, np.float32)), W, H, D,
-                                      alpha, tau_smooth, min_level, ptr(vol), ptr(wta), ptr(disp), ptr(plane))
+                                      alpha, tau_smooth, min_level, int(right_view), ptr(vol), ptr(wta), ptr(disp),
+                                      ptr(plane))
         assert levels > 0, levels
         return vol, wta, disp, plane, levels
 
@@ -230,8 +231,11 @@ def mccnn_record(ref: RefLib, W, H, D, seed):
     s = make_scene(W, H, D, seed)
     src = mccnn_like_volume(s, D, seed + 1)
     vol, wta, disp, plane, levels = ref.hbp_f32(s.left, s.right, src)
+    volR, wtaR, dispR, planeR, levelsR = ref.hbp_f32(s.left, s.right, src, right_view=True)
     return dict(W=W, H=H, D=D, seed=seed, sha_src=sha(src), sha_vol_f32=sha(vol),
-                wta=wta.astype(np.uint16), disp=disp, plane=plane, levels=levels)
+                wta=wta.astype(np.uint16), disp=disp, plane=plane, levels=levels,
+                sha_vol_right=sha(volR), wta_right=wtaR.astype(np.uint16), disp_right=dispR,
+                plane_right=planeR, levels_right=levelsR)
 
 
 def main():

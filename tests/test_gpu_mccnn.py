@@ -73,6 +73,47 @@ def test_hbp_f32_bit_exact(eng, W, H, D, seed, fp16):
     assert np.array_equal(gp.view(np.uint32), op.view(np.uint32))
 
 
+@pytest.mark.parametrize("W,H,D,seed", CASES)
+def test_ingest_right_view_bit_exact(eng, W, H, D, seed):
+    """Both views in one call: the right view equals the oracle's cost_to_right."""
+    import pyoracle as O
+    from scenes import make_scene, mccnn_like_volume
+    E, ctx, torch = eng
+    src = mccnn_like_volume(make_scene(W, H, D, seed), D, seed + 1)
+    s = torch.from_numpy(src).cuda()
+    nv = E.volume_f32_bytes(W, H, D) // 4
+    vol, volR = (torch.full((nv,), float("nan"), device="cuda") for _ in range(2))
+    wta, wtaR = (torch.full((H * W,), float("nan"), device="cuda") for _ in range(2))
+    ctx.cost_f32_d(s, W, H, D, 0.5, vol, wta, volR, wtaR)
+    torch.cuda.synchronize()
+    for v, w, right in ((vol, wta, False), (volR, wtaR, True)):
+        ov, ow = O.cost_f32(src, 0.5, right=right)
+        got = E.volume_f32_to_dhw(v.cpu().numpy(), W, H, D)
+        assert np.array_equal(got.view(np.uint32), ov.view(np.uint32))
+        assert np.array_equal(w.cpu().numpy().reshape(H, W).view(np.uint32), ow.view(np.uint32))
+
+
+def test_right_view_hbp_bit_exact(eng):
+    """The right view's HBP (right image's pyramid, cost_to_right volume)
+    equals the oracle's bit for bit."""
+    import pyoracle as O
+    from scenes import make_scene, mccnn_like_volume
+    E, ctx, torch = eng
+    W, H, D, seed = 160, 120, 48, 11
+    sc = make_scene(W, H, D, seed)
+    src = mccnn_like_volume(sc, D, seed + 1)
+    nv = E.volume_f32_bytes(W, H, D) // 4
+    volR = torch.zeros(nv, device="cuda")
+    wtaR = torch.zeros(H * W, device="cuda")
+    ctx.cost_f32_d(torch.from_numpy(src).cuda(), W, H, D, 0.5, None, None, volR, wtaR)
+    ctx.segment_d(torch.from_numpy(np.ascontiguousarray(sc.right)).cuda(), W, H)
+    disp = torch.zeros(H * W, device="cuda")
+    ctx.infer_f32_d(volR, wtaR, D, 0.5, E.default_params(alpha=1.3), disp)
+    ref = O.pipeline_f32(sc.left, src, R=sc.right)
+    got = disp.cpu().numpy().reshape(H, W)
+    assert np.array_equal(got.view(np.uint32), ref["disp"].view(np.uint32)), float(np.mean(got != ref["disp"]))
+
+
 def test_mccnn_path_accuracy(eng):
     """On the synthetic MC-CNN-like volume the float path recovers the scene:
     bad-2.0 below 5% of non-occluded pixels (450x375, D 64)."""
