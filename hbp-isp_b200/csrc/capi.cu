@@ -562,6 +562,20 @@ hbp_status hbp_cost_f32_d(hbp_ctx *c, const float *src, int W, int H, int D, flo
     });
 }
 
+hbp_status hbp_cost_ad_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, float *greyL,
+                         float *greyR, float *vol, float *wta, float *volR, float *wtaR, void *stream)
+{
+    if (!c || !bgrL || !bgrR || !greyL || !greyR)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    if (!vol != !wta || !volR != !wtaR || (!vol && !volR))
+        return fail(HBP_ERR_INVALID_ARG, "give vol and wta, volR and wtaR, or both pairs");
+    return guarded([&] {
+        check_dims(W, H, D);
+        HBP_CUDA(cudaSetDevice(c->device));
+        launch_cost_ad(bgrL, bgrR, W, H, D, AD_TAU, greyL, greyR, vol, wta, volR, wtaR, pick(c, stream));
+    });
+}
+
 hbp_status hbp_infer_f32_d(hbp_ctx *c, const float *vol, const float *wta, int D, float tau, const hbp_params *prm,
                            float *disp, float *plane, void *stream)
 {

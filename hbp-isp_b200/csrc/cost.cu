@@ -220,7 +220,88 @@ __global__ void __launch_bounds__(HM_THREADS)
     if (in)
         wta[(size_t)y * W + x] = (float)arg;
 }
+
+// img_BGR_to_grey (imutil.cu:116-130) for both views: the float nearest to
+// B*0.114 + G*0.587 + R*0.299. That double sum lies within 1e-13 of k/1000
+// (k = 114B + 587G + 299R), and k/1000 is at least 7e-9 away from the
+// midpoint of two floats below 256 (such a midpoint is an odd multiple of
+// 2^-17 or finer, which k/1000 never is), so rounding the double sum and
+// rounding k/1000 itself give the same float: the correctly rounded quotient.
+__global__ void grey_f32_kernel(const uint8_t *__restrict__ bgrL, const uint8_t *__restrict__ bgrR, int n,
+                                float *__restrict__ gL, float *__restrict__ gR)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint8_t *l = bgrL + 3 * (size_t)i, *r = bgrR + 3 * (size_t)i;
+    gL[i] = __fdiv_rn((float)(114 * l[0] + 587 * l[1] + 299 * l[2]), 1000.0f);
+    gR[i] = __fdiv_rn((float)(114 * r[0] + 587 * r[1] + 299 * r[2]), 1000.0f);
+}
+
+// ad_cost (stereo_cost.cu:9-43) and WTA_D_k: V[d][y][x] = min(|gL(x) - gR(x - d)|,
+// tau) for x >= D - 1, and 0 for every d where x < D - 1 (the reference's
+// border). RIGHT: the volume after cost_to_right, VR[d][y][x] =
+// V[d][y][min(x + d, W - 1)]. Tiled float layout, geometry as the ingest.
+template <bool RIGHT>
+__global__ void __launch_bounds__(HM_THREADS)
+    ad_volume_kernel(const float *__restrict__ gL, const float *__restrict__ gR, int W, int H, int D, float tau,
+                     int TX, float *__restrict__ vol, float *__restrict__ wta)
+{
+    const int xs = blockIdx.x * HM_COLS, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = (xs >> 3) + w;
+    if (tx >= TX)
+        return;
+    const int x = xs + w * VT_W + (lane & 7), y = blockIdx.y * VT_H + (lane >> 3);
+    const bool in = x < W && y < H;
+    float *out = vol + ((size_t)blockIdx.y * TX + tx) * D * VT_BYTES + lane;
+    const float *rowL = gL + (size_t)(in ? y : 0) * W, *rowR = gR + (size_t)(in ? y : 0) * W;
+    const float ref = in && !RIGHT ? __ldg(rowL + x) : 0.0f;
+    float best = FLT_MAX;
+    int arg = 0;
+#pragma unroll 4
+    for (int d = 0; d < D; ++d)
+    {
+        float v = 0.0f;
+        if (in)
+        {
+            const int xl = RIGHT ? min(x + d, W - 1) : x; // the left-view column read
+            if (xl >= D - 1)
+                v = fminf(fabsf((RIGHT ? __ldg(rowL + xl) : ref) - __ldg(rowR + xl - d)), tau);
+            if (v < best)
+            {
+                best = v;
+                arg = d;
+            }
+        }
+        out[(size_t)d * VT_BYTES] = v;
+    }
+    if (in)
+        wta[(size_t)y * W + x] = (float)arg;
+}
 } // namespace
+
+void launch_cost_ad(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, float tau, float *greyL,
+                    float *greyR, float *vol, float *wta, float *volR, float *wtaR, cudaStream_t st)
+{
+    const int n = W * H;
+    grey_f32_kernel<<<ceil_div(n, 256), 256, 0, st>>>(bgrL, bgrR, n, greyL, greyR);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    const int TX = ceil_div(W, VT_W);
+    dim3 g(ceil_div(W, HM_COLS), ceil_div(H, VT_H));
+    if (vol)
+    {
+        ad_volume_kernel<false><<<g, HM_THREADS, 0, st>>>(greyL, greyR, W, H, D, tau, TX, vol, wta);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+    }
+    if (volR)
+    {
+        ad_volume_kernel<true><<<g, HM_THREADS, 0, st>>>(greyL, greyR, W, H, D, tau, TX, volR, wtaR);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+    }
+}
 
 void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta, float *volR,
                        float *wtaR, cudaStream_t st)

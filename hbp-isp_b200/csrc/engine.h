@@ -76,6 +76,11 @@ void launch_cost(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, 
 inline size_t volume_f32_bytes(int W, int H, int D) { return volume_bytes(W, H, D) * sizeof(float); }
 void launch_ingest_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta, float *volR,
                        float *wtaR, cudaStream_t st);
+// The AD cost (truncation tau = 30 in the reference): both views' float grey
+// images, then the tiled float volume(s) and WTA as launch_ingest_f32.
+constexpr float AD_TAU = 30.0f; // stereo_cost.cu:425
+void launch_cost_ad(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, float tau, float *greyL,
+                    float *greyR, float *vol, float *wta, float *volR, float *wtaR, cudaStream_t st);
 
 // lab.cu
 void launch_lab(const uint8_t *bgr, int n, float4 *lab, cudaStream_t st);

@@ -173,6 +173,10 @@ class Context:
         _check(lib().hbp_cost_f32_d(self.h, _p(src), W, H, D, C.c_float(tau), _p(vol), _p(wta), _p(volR),
                                     _p(wtaR), None))
 
+    def cost_ad_d(self, bgrL, bgrR, W, H, D, greyL, greyR, vol, wta, volR=None, wtaR=None):
+        _check(lib().hbp_cost_ad_d(self.h, _p(bgrL), _p(bgrR), W, H, D, _p(greyL), _p(greyR), _p(vol), _p(wta),
+                                   _p(volR), _p(wtaR), None))
+
     def infer_f32_d(self, vol, wta, D, tau, params: Params | None, disp, plane=None):
         prm = params or default_params()
         _check(lib().hbp_infer_f32_d(self.h, _p(vol), _p(wta), D, C.c_float(tau), C.byref(prm), _p(disp),

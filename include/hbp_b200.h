@@ -97,6 +97,17 @@ size_t hbp_volume_f32_bytes(int W, int H, int D);
 hbp_status hbp_cost_f32_d(hbp_ctx *ctx, const float *src, int W, int H, int D, float tau, float *vol,
                           float *wta, float *volR, float *wtaR, void *stream);
 
+/* The AD cost: StereoCost::compute_stereo_cost("AD") (stereo_cost.cu:421-429,
+ * ad_cost :9-43, grey img_BGR_to_grey imutil.cu:116-130, WTA_D_k :249-266).
+ * greyL / greyR (H x W floats) receive the float grey images; vol / wta (and
+ * volR / wtaR, the view after cost_to_right) as hbp_cost_f32_d, with
+ * min(|gL(x) - gR(x - d)|, 30) for x >= D - 1 and 0 for every d where
+ * x < D - 1 (the reference's border). HBP runs on it through hbp_infer_f32_d
+ * with tau 30. */
+hbp_status hbp_cost_ad_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,
+                         float *greyL, float *greyR, float *vol, float *wta, float *volR, float *wtaR,
+                         void *stream);
+
 /* BGR -> CIELAB float4 (L, a, b, 1) (imutil.cu:4-40, segment.cu:795-809). */
 hbp_status hbp_lab_d(hbp_ctx *ctx, const uint8_t *bgr, long n, float *lab4, void *stream);
 

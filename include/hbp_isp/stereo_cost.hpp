@@ -7,7 +7,8 @@
 //             as read_volume_from_file reads im0.acrt, stereo_cost.cu:396-418),
 //             then hbp_cost_f32_d; g_img_cost_f32_d() is the tiled float
 //             volume (hbp_volume_f32_bytes).
-// Other costs ("AD") are not offered and throw std::invalid_argument.
+//   "AD":     hbp_cost_ad_d (truncation 30); the volume as for "MC-CNN".
+// Any other name throws std::invalid_argument.
 #pragma once
 
 #include <fstream>
@@ -42,19 +43,29 @@ class StereoCost
         else if (algo == "MC-CNN")
         {
             f32 = true;
+            ad = false;
             m_tau = 0.5f;
             read_volume();
             run_f32(false);
         }
+        else if (algo == "AD")
+        {
+            f32 = true;
+            ad = true;
+            m_tau = 30.0f;
+            run_ad(false);
+        }
         else
-            throw std::invalid_argument("StereoCost: the \"Census\" and \"MC-CNN\" costs are offered");
+            throw std::invalid_argument("StereoCost: the \"Census\", \"MC-CNN\" and \"AD\" costs are offered");
     }
 
     // cost_to_right (stereo_cost.cu:488-516): the volume and WTA become the
     // right view's
     void cost_to_right()
     {
-        if (f32)
+        if (ad)
+            run_ad(true);
+        else if (f32)
             run_f32(true);
         else
             run(true);
@@ -87,6 +98,20 @@ class StereoCost
             throw std::runtime_error("StereoCost: cost volume file " + vol_dir + " is shorter than D x H x W floats");
         src = std::make_shared<detail::DevBuf>(bytes);
         detail::check(hbp_copy(src->p, host.data(), bytes));
+    }
+
+    void run_ad(bool right)
+    {
+        const size_t n = (size_t)width * height;
+        detail::Buf gL = std::make_shared<detail::DevBuf>(4 * n), gR = std::make_shared<detail::DevBuf>(4 * n);
+        detail::Buf v = std::make_shared<detail::DevBuf>(hbp_volume_f32_bytes(width, height, m_labels));
+        detail::Buf w = std::make_shared<detail::DevBuf>(4 * n);
+        detail::check(hbp_cost_ad_d(detail::shared_ctx()->h, imgL->as<uint8_t>(), imgR->as<uint8_t>(), width, height,
+                                    m_labels, gL->as<float>(), gR->as<float>(), right ? nullptr : v->as<float>(),
+                                    right ? nullptr : w->as<float>(), right ? v->as<float>() : nullptr,
+                                    right ? w->as<float>() : nullptr, nullptr));
+        vol = v;
+        wta = w;
     }
 
     void run_f32(bool right)
@@ -124,7 +149,7 @@ class StereoCost
     int width, height, m_labels;
     std::string vol_dir;
     detail::Buf imgL, imgR, src;
-    bool f32 = false;
+    bool f32 = false, ad = false;
     float m_tau = 25.0f;
 };
 } // namespace hbp_isp

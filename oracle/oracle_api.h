@@ -14,6 +14,9 @@ void orc_cost_volume(const uint32_t *cL, const uint32_t *cR, int W, int H, int D
 void orc_cost_to_right(const uint8_t *volL, int W, int H, int D, uint8_t *volR, float *wta);
 void orc_cost_f32(const float *src, int W, int H, int D, float tau, float *vol, float *wta);
 void orc_cost_f32_right(const float *src, int W, int H, int D, float tau, float *volR, float *wta);
+void orc_grey_f32(const uint8_t *bgr, int n, float *out);
+void orc_cost_ad(const float *gL, const float *gR, int W, int H, int D, float tau, int right, float *vol,
+                 float *wta);
 void orc_lab_set_overrides(const uint32_t *keys, const float *vals, int n);
 void orc_lab(const uint8_t *bgr, int n, float *lab4);
 void orc_nn_grid(const float *lab4, int W, int H, int *nn, float *dist_min, int *bd);

@@ -111,11 +111,9 @@ void orc_cost_f32(const float *src, int W, int H, int D, float tau, float *vol, 
 // (:471-486) moves each (d, y) row left by d in place, fill_out_of_view_k
 // (:367-390, right side) copies column W-1-d over columns W-1-d .. W-1, and
 // WTA_D_k keeps the first minimum.
-void orc_cost_f32_right(const float *src, int W, int H, int D, float tau, float *volR, float *wta)
+static void float_volume_to_right(float *volR, int W, int H, int D, float *wta)
 {
     const size_t n = (size_t)W * H;
-    std::vector<float> wl(n);
-    orc_cost_f32(src, W, H, D, tau, volR, wl.data());
     for (int d = 0; d < D; ++d)
         for (int y = 0; y < H; ++y)
         {
@@ -134,6 +132,54 @@ void orc_cost_f32_right(const float *src, int W, int H, int D, float tau, float 
             if (volR[(size_t)d * n + p] < best)
             {
                 best = volR[(size_t)d * n + p];
+                arg = d;
+            }
+        wta[p] = (float)arg;
+    }
+}
+
+void orc_cost_f32_right(const float *src, int W, int H, int D, float tau, float *volR, float *wta)
+{
+    std::vector<float> wl((size_t)W * H);
+    orc_cost_f32(src, W, H, D, tau, volR, wl.data());
+    float_volume_to_right(volR, W, H, D, wta);
+}
+
+// img_BGR_to_grey (imutil.cu:116-130): the double weighted sum stored as float.
+void orc_grey_f32(const uint8_t *bgr, int n, float *out)
+{
+    for (int i = 0; i < n; ++i)
+        out[i] = (float)(bgr[3 * i] * 0.114 + bgr[3 * i + 1] * 0.587 + bgr[3 * i + 2] * 0.299);
+}
+
+// compute_stereo_cost("AD") (stereo_cost.cu:421-429): ad_cost (:9-43) writes
+// V[d][y][x] = fminf(fabsf(gL(x) - gR(x - d)), tau) for x >= D - 1 and 0 for
+// every d where x < D - 1; WTA_D_k keeps the first minimum. right != 0 then
+// applies cost_to_right (:488-516) as orc_cost_f32_right does.
+void orc_cost_ad(const float *gL, const float *gR, int W, int H, int D, float tau, int right, float *vol,
+                 float *wta)
+{
+    const size_t n = (size_t)W * H;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+        {
+            const size_t i = (size_t)y * W + x;
+            for (int d = 0; d < D; ++d)
+                vol[(size_t)d * n + i] = x < D - 1 ? 0.0f : std::fmin(std::fabs(gL[i] - gR[i - d]), tau);
+        }
+    if (right)
+    {
+        float_volume_to_right(vol, W, H, D, wta);
+        return;
+    }
+    for (size_t p = 0; p < n; ++p)
+    {
+        float best = FLT_MAX;
+        int arg = 0;
+        for (int d = 0; d < D; ++d)
+            if (vol[(size_t)d * n + p] < best)
+            {
+                best = vol[(size_t)d * n + p];
                 arg = d;
             }
         wta[p] = (float)arg;

@@ -46,6 +46,8 @@ def lib():
                                      C.c_float, C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
         _lib.orc_cost_f32.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
         _lib.orc_cost_f32_right.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
+        _lib.orc_grey_f32.argtypes = [P, C.c_int, P]
+        _lib.orc_cost_ad.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P, P]
     return _lib
 
 
@@ -211,6 +213,33 @@ def cost_f32(src, tau=0.5, right=False):
     f = lib().orc_cost_f32_right if right else lib().orc_cost_f32
     f(_p(src), W, H, D, tau, _p(vol), _p(wta))
     return vol, wta
+
+
+def grey_f32(bgr):
+    """img_BGR_to_grey: float grey image of a BGR uint8 image."""
+    bgr = np.ascontiguousarray(bgr, np.uint8)
+    out = np.zeros(bgr.shape[:-1], np.float32)
+    lib().orc_grey_f32(_p(bgr), int(out.size), _p(out))
+    return out
+
+
+def cost_ad(L, R, D, tau=30.0, right=False):
+    """The AD cost: (vol [D][H*W], wta HxW, greyL, greyR); right: after cost_to_right."""
+    gL, gR = grey_f32(L), grey_f32(R)
+    H, W = gL.shape
+    vol = np.zeros((D, H * W), np.float32)
+    wta = np.zeros((H, W), np.float32)
+    lib().orc_cost_ad(_p(gL), _p(gR), W, H, D, tau, int(right), _p(vol), _p(wta))
+    return vol, wta, gL, gR
+
+
+def pipeline_ad(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, right_view=False):
+    """The AD single-view path: AD cost, pyramid of the view's image, HBP (tau 30)."""
+    H, W = L.shape[:2]
+    vol, wta, _, _ = cost_ad(L, R, D, right=right_view)
+    seg = segment(lab(R if right_view else L))
+    disp, plane = hbp_f32(seg, vol, wta, W, H, D, 30.0, alpha, tau_smooth, min_level)
+    return dict(disp=disp, plane=plane, vol=vol, wta=wta, seg=seg)
 
 
 def hbp_f32(seg, volf, wta, W, H, D, tau=0.5, alpha=1.3, tau_smooth=0.6, min_level=2, fp64=False,

@@ -54,6 +54,8 @@ struct StereoCostView : public StereoCost
     const uint8_t *cost_u8() const { return img_cost_u1_d; }
     const uint8_t *greyL() const { return imgL_u1_d; }
     const uint8_t *greyR() const { return imgR_u1_d; }
+    const float *greyL_f() const { return imgL_f1_d; }
+    const float *greyR_f() const { return imgR_f1_d; }
 };
 
 template <typename T>
@@ -344,6 +346,50 @@ int ref_hbp_f32(const uint8_t *bgrL, const uint8_t *bgrR, const float *src, int 
         delete isp;
     }
     unlink(path);
+    int rc2 = last_error();
+    if (rc || rc2)
+        return rc ? rc : rc2;
+    return levels;
+}
+
+// The AD cost path: StereoCost::compute_stereo_cost("AD") (stereo_cost.cu:
+// 421-429), optionally cost_to_right, then SegHAC on the view's image and
+// HBP_ISP(alpha, tau_smooth).run_ms(min_level) as ref_hbp_pair. greyL/greyR
+// (float HW), vol_f32 ([D][HW]) and wta are optional outputs. Returns the
+// number of levels.
+int ref_hbp_ad(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, float alpha, float tau_smooth,
+               int min_level, int right_view, float *greyL, float *greyR, float *vol_f32, float *wta, float *disp,
+               float *plane)
+{
+    size_t n = (size_t)W * H;
+    int levels = 0;
+    int rc;
+    {
+        cv::Mat L = wrap_bgr(bgrL, W, H), R = wrap_bgr(bgrR, W, H);
+        SegHAC *seg = new SegHAC(right_view ? R : L, CentoridLink, 4, 0.0, LabelISPFormat, 1, false);
+        seg->run_ms();
+        ISPData *isp = new ISPData(seg);
+        levels = (int)seg->g_num_clus_isp().size();
+        delete seg;
+        StereoCostView *sc = new StereoCostView(L, R, D, "");
+        sc->compute_stereo_cost("AD");
+        if (right_view)
+            sc->cost_to_right();
+        d2h(greyL, sc->greyL_f(), n);
+        d2h(greyR, sc->greyR_f(), n);
+        d2h(vol_f32, sc->g_img_cost_d(), n * D);
+        d2h(wta, sc->g_img_D_d(), n);
+        StereoData *sd = new StereoData(sc, true);
+        delete sc;
+        HBP_ISP *hbp = new HBP_ISP(isp, sd, alpha, tau_smooth);
+        std::pair<cv::Mat, cv::Mat> res = hbp->run_ms(min_level);
+        rc = last_error();
+        std::memcpy(disp, res.first.data, sizeof(float) * n);
+        std::memcpy(plane, res.second.data, sizeof(float) * n * 3);
+        delete hbp;
+        delete sd;
+        delete isp;
+    }
     int rc2 = last_error();
     if (rc || rc2)
         return rc ? rc : rc2;

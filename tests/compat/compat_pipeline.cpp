@@ -4,10 +4,10 @@
 //           StereoData, HBP_ISP::run_ms, medianFilter)
 //   lr:     main_bench_middv3.cu:169-219 (both views, LR check, fill,
 //           weighted median, plane -> disparity)
-// with the Census cost (alpha 1000.1) and, given an im0.acrt-style volume
-// file, again with the MC-CNN cost (alpha 1.3, bench_MiddV3_train.sh:6).
-// usage: compat_pipeline left.bgr right.bgr W H D single.f32 lr.f32
-//                        [vol.acrt mccnn_single.f32 mccnn_lr.f32]
+// with the Census and AD costs (alpha 1000.1) and, given an im0.acrt-style
+// volume file, the MC-CNN cost (alpha 1.3, bench_MiddV3_train.sh:6). Writes
+// <out_prefix>{census,ad,mccnn}_{single,lr}.f32.
+// usage: compat_pipeline left.bgr right.bgr W H D out_prefix [vol.acrt]
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -83,19 +83,21 @@ static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, co
 
 int main(int argc, char **argv)
 {
-    if (argc != 8 && argc != 11)
+    if (argc != 7 && argc != 8)
     {
-        std::fprintf(stderr, "usage: %s left.bgr right.bgr W H D single.f32 lr.f32 "
-                             "[vol.acrt mccnn_single.f32 mccnn_lr.f32]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s left.bgr right.bgr W H D out_prefix [vol.acrt]\n", argv[0]);
         return 2;
     }
     const int W = std::atoi(argv[3]), H = std::atoi(argv[4]), D = std::atoi(argv[5]);
+    const std::string out(argv[6]);
     try
     {
         Mat L = read_bgr(argv[1], W, H), R = read_bgr(argv[2], W, H);
-        flows(L, R, D, "Census", "", 1000.1f, argv[6], argv[7]);
-        if (argc == 11)
-            flows(L, R, D, "MC-CNN", argv[8], 1.3f, argv[9], argv[10]);
+        flows(L, R, D, "Census", "", 1000.1f, (out + "census_single.f32").c_str(), (out + "census_lr.f32").c_str());
+        flows(L, R, D, "AD", "", 1000.1f, (out + "ad_single.f32").c_str(), (out + "ad_lr.f32").c_str());
+        if (argc == 8)
+            flows(L, R, D, "MC-CNN", argv[7], 1.3f, (out + "mccnn_single.f32").c_str(),
+                  (out + "mccnn_lr.f32").c_str());
     }
     catch (const std::exception &e)
     {

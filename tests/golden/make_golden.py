@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir> [--only census|mccnn]
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -38,10 +38,12 @@ class RefLib:
         path = path or os.path.join(ROOT, "oracle", "_ref", "libhbpref.so")
         self.lib = C.CDLL(path)
         for name in ("ref_grey", "ref_lab", "ref_1nn_grid", "ref_crtrees", "ref_cost",
-                     "ref_segment", "ref_hbp_pair", "ref_post", "ref_hbp_f32"):
+                     "ref_segment", "ref_hbp_pair", "ref_post", "ref_hbp_f32", "ref_hbp_ad"):
             getattr(self.lib, name).restype = C.c_int
         self.lib.ref_hbp_pair.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_int, C.c_int, P, P]
+        self.lib.ref_hbp_ad.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int,
+                                        P, P, P, P, P, P]
         self.lib.ref_hbp_f32.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
                                          C.c_int, P, P, P, P]
 
@@ -125,6 +127,17 @@ class RefLib:
                                       ptr(plane))
         assert levels > 0, levels
         return vol, wta, disp, plane, levels
+
+    def hbp_ad(self, L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, right_view=False):
+        H, W, _ = L.shape
+        out = dict(greyL=np.zeros((H, W), np.float32), greyR=np.zeros((H, W), np.float32),
+                   vol=np.zeros((D, H * W), np.float32), wta=np.zeros((H, W), np.float32),
+                   disp=np.zeros((H, W), np.float32), plane=np.zeros((H, W, 3), np.float32))
+        levels = self.lib.ref_hbp_ad(ptr(L), ptr(R), W, H, D, alpha, tau_smooth, min_level, int(right_view),
+                                     *(ptr(out[k]) for k in ("greyL", "greyR", "vol", "wta", "disp", "plane")))
+        assert levels > 0, levels
+        out["levels"] = levels
+        return out
 
     def post(self, L, R, dispL, planeL, dispR, planeR, median=True):
         H, W, _ = L.shape
@@ -238,21 +251,40 @@ def mccnn_record(ref: RefLib, W, H, D, seed):
                 plane_right=planeR, levels_right=levelsR)
 
 
+AD_CASES = [(96, 64, 32, 7, "ad_96x64_d32_s7"), (160, 120, 48, 11, "ad_160x120_d48_s11")]
+
+
+def ad_record(ref: RefLib, W, H, D, seed):
+    """The AD cost path on a seeded synthetic scene, both views."""
+    s = make_scene(W, H, D, seed)
+    a = ref.hbp_ad(s.left, s.right, D)
+    b = ref.hbp_ad(s.left, s.right, D, right_view=True)
+    return dict(W=W, H=H, D=D, seed=seed, sha_greyL=sha(a["greyL"]), sha_greyR=sha(a["greyR"]),
+                sha_vol_f32=sha(a["vol"]), wta=a["wta"].astype(np.uint16), disp=a["disp"], plane=a["plane"],
+                sha_vol_right=sha(b["vol"]), wta_right=b["wta"].astype(np.uint16), disp_right=b["disp"],
+                levels=a["levels"], levels_right=b["levels"])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
-    ap.add_argument("--only", choices=["census", "mccnn"], default=None)
+    ap.add_argument("--only", choices=["census", "mccnn", "ad"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     ref = RefLib(args.lib)
 
-    if args.only != "census":
+    if args.only in (None, "mccnn"):
         for (W, H, D, seed, name) in MCCNN_CASES:
             rec = mccnn_record(ref, W, H, D, seed)
             np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
             print(name, "levels", rec["levels"])
-    if args.only == "mccnn":
+    if args.only in (None, "ad"):
+        for (W, H, D, seed, name) in AD_CASES:
+            rec = ad_record(ref, W, H, D, seed)
+            np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
+            print(name, "levels", rec["levels"])
+    if args.only in ("mccnn", "ad"):
         return
 
     for (W, H, D, seed, full, name) in [

@@ -27,32 +27,74 @@ def test_headers_compile():
     _compile(None, syntax_only=True)
 
 
+def _run_driver(tmp_path, s, W, H, D, src=None):
+    exe = str(tmp_path / "compat_pipeline")
+    _compile(exe)
+    (tmp_path / "l.bgr").write_bytes(np.ascontiguousarray(s.left).tobytes())
+    (tmp_path / "r.bgr").write_bytes(np.ascontiguousarray(s.right).tobytes())
+    args = [exe, str(tmp_path / "l.bgr"), str(tmp_path / "r.bgr"), str(W), str(H), str(D), str(tmp_path / "o_")]
+    if src is not None:
+        (tmp_path / "im0.acrt").write_bytes(np.ascontiguousarray(src, np.float32).tobytes())
+        args.append(str(tmp_path / "im0.acrt"))
+    r = subprocess.run(args, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return lambda name: np.fromfile(tmp_path / f"o_{name}.f32", np.float32).reshape(H, W)
+
+
+def _flows_via_stages(E, ctx, torch, s, D, vols, tau, alpha):
+    """Both driver flows through the engine's stage entry points on float
+    volumes (vol, wta, volR, wtaR): (single with the driver median, lr)."""
+    W, H = s.left.shape[1], s.left.shape[0]
+    n = W * H
+    cuda = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    f = lambda k=1: torch.zeros(k * n, dtype=torch.float32, device="cuda")
+    vol, wta, volR, wtaR = vols
+    prm = E.default_params(alpha=alpha)
+    dL, pL, dR, pR = f(), f(3), f(), f(3)
+    ctx.segment_d(cuda(s.left), W, H)
+    ctx.infer_f32_d(vol, wta, D, tau, prm, dL, pL)
+    single = dL.clone()
+    ctx.driver_median_d(single, W, H)
+    ctx.segment_d(cuda(s.right), W, H)
+    ctx.infer_f32_d(volR, wtaR, D, tau, prm, dR, pR)
+    fail = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    dout = f()
+    ctx.lr_check_d(dL, dR, pL, fail, dout, W, H)
+    ctx.weighted_median_d(cuda(s.left), fail, pL, dout, W, H)
+    torch.cuda.synchronize()
+    return single.cpu().numpy().reshape(H, W), dout.cpu().numpy().reshape(H, W)
+
+
+def _same(a, b):
+    return np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 @pytest.mark.gpu
 def test_driver_flows_match_the_engine(tmp_path):
+    """Census and AD, both driver flows: the Census ones against hbp_run_pair,
+    the AD ones against the engine's stage entry points, bit for bit."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     import hbp_b200 as E
     from scenes import make_scene
-    exe = str(tmp_path / "compat_pipeline")
-    _compile(exe)
     W, H, D = 160, 120, 48
     s = make_scene(W, H, D, 77)
-    (tmp_path / "l.bgr").write_bytes(np.ascontiguousarray(s.left).tobytes())
-    (tmp_path / "r.bgr").write_bytes(np.ascontiguousarray(s.right).tobytes())
-    r = subprocess.run([exe, str(tmp_path / "l.bgr"), str(tmp_path / "r.bgr"), str(W), str(H), str(D),
-                        str(tmp_path / "single.f32"), str(tmp_path / "lr.f32")], capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr
-    single = np.fromfile(tmp_path / "single.f32", np.float32).reshape(H, W)
-    lr = np.fromfile(tmp_path / "lr.f32", np.float32).reshape(H, W)
+    out = _run_driver(tmp_path, s, W, H, D)
     ctx = E.Context(0)
     try:
         want1 = ctx.run_pair(s.left, s.right, D, E.default_params(post=1))
         want2 = ctx.run_pair(s.left, s.right, D, E.default_params(post=2))
+        cuda = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        nv = E.volume_f32_bytes(W, H, D) // 4
+        vols = [torch.zeros(k, dtype=torch.float32, device="cuda") for k in (nv, W * H, nv, W * H)]
+        gL, gR = (torch.zeros(W * H, dtype=torch.float32, device="cuda") for _ in range(2))
+        ctx.cost_ad_d(cuda(s.left), cuda(s.right), W, H, D, gL, gR, *vols)
+        ad1, ad2 = _flows_via_stages(E, ctx, torch, s, D, vols, 30.0, 1000.1)
     finally:
         ctx.close()
-    assert np.array_equal(single.view(np.uint32), want1.view(np.uint32))
-    assert np.array_equal(lr.view(np.uint32), want2.view(np.uint32))
+    assert _same(out("census_single"), want1) and _same(out("census_lr"), want2)
+    assert _same(out("ad_single"), ad1) and _same(out("ad_lr"), ad2)
 
 
 @pytest.mark.gpu
@@ -65,47 +107,16 @@ def test_mccnn_driver_flows_match_the_engine(tmp_path):
         pytest.skip("no CUDA device")
     import hbp_b200 as E
     from scenes import make_scene, mccnn_like_volume
-    exe = str(tmp_path / "compat_pipeline")
-    _compile(exe)
     W, H, D = 160, 120, 48
     s = make_scene(W, H, D, 78)
     src = mccnn_like_volume(s, D, 79)
-    (tmp_path / "l.bgr").write_bytes(np.ascontiguousarray(s.left).tobytes())
-    (tmp_path / "r.bgr").write_bytes(np.ascontiguousarray(s.right).tobytes())
-    (tmp_path / "im0.acrt").write_bytes(src.tobytes())
-    outs = [str(tmp_path / n) for n in ("c1.f32", "c2.f32", "m1.f32", "m2.f32")]
-    r = subprocess.run([exe, str(tmp_path / "l.bgr"), str(tmp_path / "r.bgr"), str(W), str(H), str(D),
-                        outs[0], outs[1], str(tmp_path / "im0.acrt"), outs[2], outs[3]],
-                       capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr
-    single = np.fromfile(outs[2], np.float32).reshape(H, W)
-    lr = np.fromfile(outs[3], np.float32).reshape(H, W)
-
+    out = _run_driver(tmp_path, s, W, H, D, src)
     ctx = E.Context(0)
     try:
-        cuda = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-        n = H * W
-        f = lambda k=1: torch.zeros(k * n, dtype=torch.float32, device="cuda")
         nv = E.volume_f32_bytes(W, H, D) // 4
-        vol, volR = (torch.zeros(nv, dtype=torch.float32, device="cuda") for _ in range(2))
-        wta, wtaR = f(), f()
-        ctx.cost_f32_d(cuda(src), W, H, D, 0.5, vol, wta, volR, wtaR)
-        prm = E.default_params(alpha=1.3)
-        dL, pL, dR, pR = f(), f(3), f(), f(3)
-        ctx.segment_d(cuda(s.left), W, H)
-        ctx.infer_f32_d(vol, wta, D, 0.5, prm, dL, pL)
-        want1 = dL.clone()
-        ctx.driver_median_d(want1, W, H)
-        ctx.segment_d(cuda(s.right), W, H)
-        ctx.infer_f32_d(volR, wtaR, D, 0.5, prm, dR, pR)
-        fail = torch.zeros(n, dtype=torch.uint8, device="cuda")
-        dout = f()
-        ctx.lr_check_d(dL, dR, pL, fail, dout, W, H)
-        ctx.weighted_median_d(cuda(s.left), fail, pL, dout, W, H)
-        torch.cuda.synchronize()
-        want1 = want1.cpu().numpy().reshape(H, W)
-        want2 = dout.cpu().numpy().reshape(H, W)
+        vols = [torch.zeros(k, dtype=torch.float32, device="cuda") for k in (nv, W * H, nv, W * H)]
+        ctx.cost_f32_d(torch.from_numpy(src).cuda(), W, H, D, 0.5, *vols)
+        want1, want2 = _flows_via_stages(E, ctx, torch, s, D, vols, 0.5, 1.3)
     finally:
         ctx.close()
-    assert np.array_equal(single.view(np.uint32), want1.view(np.uint32))
-    assert np.array_equal(lr.view(np.uint32), want2.view(np.uint32))
+    assert _same(out("mccnn_single"), want1) and _same(out("mccnn_lr"), want2)
