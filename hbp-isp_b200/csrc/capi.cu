@@ -600,6 +600,45 @@ hbp_status hbp_infer_f32_d(hbp_ctx *c, const float *vol, const float *wta, int D
     });
 }
 
+hbp_status hbp_infer_levels_d(hbp_ctx *c, const uint8_t *vol, const float *volf, const float *wta, int D, float tau,
+                              const hbp_params *prm, int max_levels, float *disp_levels, float *plane_levels,
+                              int *num_levels, void *stream)
+{
+    if (!c || !wta || !disp_levels || !c->have_pyr || (vol == nullptr) == (volf == nullptr))
+        return fail(HBP_ERR_INVALID_ARG, "bad arguments (one of vol, volf), or no pyramid");
+    if (volf && !(tau > 0.0f))
+        return fail(HBP_ERR_INVALID_ARG, "tau <= 0");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        check_dims(c->pyr.W, c->pyr.H, D);
+        cudaStream_t st = pick(c, stream);
+        HbpParams q = to_params(prm, c->prof.on ? &c->prof : nullptr);
+        const int n = c->pyr.L - q.min_level;
+        if (q.min_level < 0 || n < 1)
+            throw StatusError{HBP_ERR_INVALID_ARG, "min_level must lie in [0, levels-1]"};
+        if (n > max_levels)
+            throw StatusError{HBP_ERR_INVALID_ARG, "the output holds fewer levels than levels - min_level"};
+        q.level_disp = disp_levels;
+        q.level_plane = plane_levels;
+        Slot *sl = slot_at(c, 0);
+        const long HW = (long)c->pyr.W * c->pyr.H;
+        ensure_slot(sl, HW, D);
+        sl->mem.reset();
+        c->tmp.reset();
+        CostVolume cv;
+        cv.u8 = vol;
+        cv.f32 = volf;
+        cv.tau = volf ? tau : CENSUS_TAU;
+        float *disp = sl->mem.alloc<float>((size_t)HW);
+        hbp_prepare(c->pyr, cv, wta, D, q, disp, nullptr, sl->mem, c->tmp, st, sl->plan);
+        c->tmp.reset();
+        std::vector<ViewPlan *> views{&sl->plan};
+        hbp_run_views(views, q, c->tmp, st);
+        if (num_levels)
+            *num_levels = n;
+    });
+}
+
 hbp_status hbp_lr_check_d(hbp_ctx *c, const float *dispL, const float *dispR, float *planeL,
                           uint8_t *fail_mask, float *disp_out, int W, int H, void *stream)
 {

@@ -215,6 +215,9 @@ struct HbpParams
     int msg_fp16 = 0;
     int bp_streams = 0; // BP scheduler streams of a batch (0: automatic)
     KernelProf *prof = nullptr;
+    // run_ms_vis: every level's map, top level L-1 first, down to min_level
+    // (HW floats and HW x 3 floats per level; level_plane may be null)
+    float *level_disp = nullptr, *level_plane = nullptr;
 };
 
 
@@ -225,6 +228,7 @@ struct ViewPlan
     struct Impl;
     Impl *impl;
     int L = 0, min_level = 0, D = 0, HW = 0;
+    bool levels = false;                     // every level's map is kept (run_ms_vis)
     std::vector<int> levelN, levelE, levelC; // nodes, edges, data-cost chunks per level
     ViewPlan();
     ~ViewPlan();

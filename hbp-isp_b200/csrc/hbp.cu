@@ -256,6 +256,7 @@ struct ViewDev
     const LevelDev *lv; // [L]
     ViewBufs b;
     float *disp, *plane_out;
+    float *lvl_disp, *lvl_plane; // per-level maps (run_ms_vis), index L-1-li; null if not kept
     int L;
 };
 
@@ -1123,7 +1124,10 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
     store_msg(v.b, t.mb, (size_t)e, out);
 }
 
-// map_msg (hbp_isp.cu:783-841), one warp per node of the finest level
+// map_msg (hbp_isp.cu:783-841), one warp per node of the task's level; into
+// the view's disparity/planes, or (MAP_LEVEL) into the per-level maps of
+// run_ms_vis (hbp_isp.cu:1348-1383)
+constexpr int MAP_LEVEL = 1;
 __global__ void __launch_bounds__(128) k_map(const ViewDev *__restrict__ V, StepDesc d)
 {
     const int lane = threadIdx.x & 31;
@@ -1148,6 +1152,13 @@ __global__ void __launch_bounds__(128) k_map(const ViewDev *__restrict__ V, Step
             break;
         }
     float4 pl = l.plane[(size_t)n * K + mp];
+    float *disp = v.disp, *plane_out = v.plane_out;
+    if (t.mode == MAP_LEVEL)
+    {
+        const size_t off = (size_t)(v.L - 1 - t.li) * c.W * c.H;
+        disp = v.lvl_disp + off;
+        plane_out = v.lvl_plane ? v.lvl_plane + 3 * off : nullptr;
+    }
     for (int j = l.pix_off[n] + lane; j < l.pix_off[n + 1]; j += 32)
     {
         uint32_t xy = l.pix[j];
@@ -1155,12 +1166,12 @@ __global__ void __launch_bounds__(128) k_map(const ViewDev *__restrict__ V, Step
         float dd = pl.x * (float)x + pl.y * (float)y + pl.z;
         dd = fminf(fmaxf(dd, 0.f), (float)(c.D - 1));
         size_t id = (size_t)y * c.W + x;
-        v.disp[id] = dd;
-        if (v.plane_out)
+        disp[id] = dd;
+        if (plane_out)
         {
-            v.plane_out[3 * id] = pl.x;
-            v.plane_out[3 * id + 1] = pl.y;
-            v.plane_out[3 * id + 2] = pl.z;
+            plane_out[3 * id] = pl.x;
+            plane_out[3 * id + 1] = pl.y;
+            plane_out[3 * id + 2] = pl.z;
         }
     }
 }
@@ -1322,6 +1333,9 @@ void hbp_prepare(const Pyramid &pyr, const CostVolume &cv, const float *wta, int
     vd.b.buf = persist.alloc<float4>((size_t)Nmax * P);
     vd.disp = disp;
     vd.plane_out = plane_out;
+    vd.lvl_disp = prm.level_disp;
+    vd.lvl_plane = prm.level_disp ? prm.level_plane : nullptr;
+    vp.levels = prm.level_disp != nullptr;
     vp.impl->vd_dev = persist.alloc<ViewDev>(1);
     HBP_CUDA(cudaMemcpyAsync(vp.impl->vd_dev, &vd, sizeof(ViewDev), cudaMemcpyHostToDevice, st));
     HBP_CUDA(cudaStreamSynchronize(st)); // lv and vd (host) feed the copies above
@@ -1341,6 +1355,7 @@ enum Phase
     PH_INIT,  // level setup: priors, their costs, beliefs, seeds (init_bp)
     PH_STEP,  // one candidate step + data cost + BP sweep
     PH_FINAL, // the level's last select
+    PH_MAP_LEVEL, // map_msg of level li into the per-level maps (run_ms_vis)
     PH_MAP,   // map_msg at min_level
     PH_DONE
 };
@@ -1470,7 +1485,15 @@ void BpScheduler::add(ViewPlan *vp, void *user)
     v.vp = vp;
     v.user = user;
     if (vp->L - 2 >= vp->min_level)
-        v.enter_level(vp->L - 2);
+    {
+        if (vp->levels)
+        {
+            v.li = vp->L - 1; // run_ms_vis maps the top level before any BP
+            v.phase = PH_MAP_LEVEL;
+        }
+        else
+            v.enter_level(vp->L - 2);
+    }
     else
     {
         v.li = vp->min_level;
@@ -1540,9 +1563,18 @@ void BpScheduler::tick(std::vector<void *> &finished)
             vn.push_back(&v);
             tn.push_back(I.task_of(v, false, pb, NODE_SELECT));
             break;
+        case PH_MAP_LEVEL:
+            vm.push_back(&v);
+            tm.push_back(I.task_of(v, false, pb, MAP_LEVEL));
+            break;
         case PH_MAP:
             vm.push_back(&v);
             tm.push_back(I.task_of(v, false, pb, NODE_SELECT));
+            if (v.vp->levels)
+            {
+                vm.push_back(&v);
+                tm.push_back(I.task_of(v, false, pb, MAP_LEVEL));
+            }
             break;
         }
     }
@@ -1659,9 +1691,17 @@ void BpScheduler::tick(std::vector<void *> &finished)
         }
         case PH_FINAL:
             if (v.li > v.vp->min_level)
-                v.enter_level(v.li - 1);
+            {
+                if (v.vp->levels)
+                    v.phase = PH_MAP_LEVEL;
+                else
+                    v.enter_level(v.li - 1);
+            }
             else
                 v.phase = PH_MAP;
+            break;
+        case PH_MAP_LEVEL:
+            v.enter_level(v.li - 1);
             break;
         case PH_MAP:
             v.phase = PH_DONE;

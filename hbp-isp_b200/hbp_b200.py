@@ -182,6 +182,14 @@ class Context:
         _check(lib().hbp_infer_f32_d(self.h, _p(vol), _p(wta), D, C.c_float(tau), C.byref(prm), _p(disp),
                                      _p(plane), None))
 
+    def infer_levels_d(self, vol, volf, wta, D, tau, params: Params | None, max_levels, disp_levels,
+                       plane_levels=None) -> int:
+        prm = params or default_params()
+        n = C.c_int(0)
+        _check(lib().hbp_infer_levels_d(self.h, _p(vol), _p(volf), _p(wta), D, C.c_float(tau), C.byref(prm),
+                                        max_levels, _p(disp_levels), _p(plane_levels), C.byref(n), None))
+        return n.value
+
     def lab_d(self, bgr, n, lab4):
         _check(lib().hbp_lab_d(self.h, _p(bgr), n, _p(lab4), None))
 

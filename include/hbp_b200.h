@@ -140,6 +140,20 @@ hbp_status hbp_infer_d(hbp_ctx *ctx, const uint8_t *vol, const float *wta, int D
 hbp_status hbp_infer_f32_d(hbp_ctx *ctx, const float *vol, const float *wta, int D, float tau,
                            const hbp_params *prm, float *disp, float *plane, void *stream);
 
+/* HBP_ISP::run_ms_vis (hbp_isp.cu:1348-1383) without its superpixel drawing
+ * (cvtColor, circles, lines: visualisation): every level's map from the top
+ * level L-1 down to min_level. disp_levels receives (L - min_level) H x W
+ * float disparities, top level first; plane_levels (may be NULL) the H x W x 3
+ * planes in the same order; *num_levels (may be NULL) their count. Give
+ * exactly one of vol (uint8, from hbp_cost_census_d) or volf (float, from
+ * hbp_cost_f32_d / hbp_cost_ad_d, with its tau; tau is ignored for vol).
+ * HBP_ERR_INVALID_ARG when L - min_level > max_levels. The last map equals
+ * hbp_infer_d's result; the top level's is 0 everywhere (its planes are
+ * never written; the reference maps uninitialised memory there). */
+hbp_status hbp_infer_levels_d(hbp_ctx *ctx, const uint8_t *vol, const float *volf, const float *wta, int D,
+                              float tau, const hbp_params *prm, int max_levels, float *disp_levels,
+                              float *plane_levels, int *num_levels, void *stream);
+
 /* PostProcess::left_right_check + plane_label_to_disp (post_process.cu:4-110,
  * :373-390): updates planeL in place, writes the failure mask (0/255) and the
  * disparity of the updated planes. */

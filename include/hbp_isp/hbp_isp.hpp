@@ -6,6 +6,8 @@
 // Extension: set_msg_fp16() stores the BP messages as FP16.
 #pragma once
 
+#include <tuple>
+
 #include "segment.hpp"
 #include "stereo_cost.hpp"
 
@@ -115,6 +117,41 @@ class HBP_ISP
         detail::download(disp, d);
         detail::download(plane, pl);
         return {disp, plane};
+    }
+
+    // run_ms_vis (hbp_isp.cu:1348-1383): (disparity, planes, superpixel
+    // image) of every level from the top level down to min_level. The
+    // superpixel image is visualisation (cvtColor, circles, lines) and is
+    // left empty here.
+    std::vector<std::tuple<Mat, Mat, Mat>> run_ms_vis(const int min_level)
+    {
+        const size_t n = (size_t)isp->width * isp->height;
+        const int levels = (int)isp->g_num_clus_isp().size() - min_level;
+        if (min_level < 0 || levels < 1)
+            throw std::invalid_argument("HBP_ISP: min_level must lie in [0, levels-1]");
+        hbp_params p;
+        hbp_default_params(&p);
+        p.alpha = m_alpha;
+        p.tau_smooth = m_tau_smooth;
+        p.min_level = min_level;
+        p.msg_fp16 = fp16 ? 1 : 0;
+        p.post = 0;
+        detail::Buf d = std::make_shared<detail::DevBuf>(4 * n * levels);
+        detail::Buf pl = std::make_shared<detail::DevBuf>(12 * n * levels);
+        int got = 0;
+        detail::check(hbp_infer_levels_d(isp->ctx->h, sd->f32 ? nullptr : sd->vol->as<uint8_t>(),
+                                         sd->f32 ? sd->vol->as<float>() : nullptr, sd->wta->as<float>(),
+                                         sd->m_labels, sd->m_tau, &p, levels, d->as<float>(), pl->as<float>(), &got,
+                                         nullptr));
+        std::vector<std::tuple<Mat, Mat, Mat>> out;
+        for (int k = 0; k < got; ++k)
+        {
+            Mat disp(isp->height, isp->width, MAT_32FC1), plane(isp->height, isp->width, MAT_32FC3);
+            detail::check(hbp_copy(disp.data, d->as<float>() + k * n, disp.bytes()));
+            detail::check(hbp_copy(plane.data, pl->as<float>() + 3 * k * n, plane.bytes()));
+            out.emplace_back(disp, plane, Mat());
+        }
+        return out;
     }
 
   private:

@@ -33,6 +33,10 @@ int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, c
             const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
             float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
             float *plane, float *state_belief, float *state_plane);
+int orc_hbp_levels(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+                   const int *bdl, const uint8_t *vol, const float *volf, const float *wta, int W, int H, int D,
+                   float data_tau, float alpha, float tau_smooth, int min_level, int mode, float *disp_levels,
+                   float *plane_levels);
 int orc_hbp_f32(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
                 const int *bdl, const float *volf, const float *wta, int W, int H, int D, float data_tau,
                 float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,

@@ -590,7 +590,7 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
         const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
         float tau_smooth, int min_level, long max_steps, float *disp, float *plane_out,
         float *state_belief, float *state_plane, bool fp16_msg = false, const float *volf = nullptr,
-        float data_tau = 25.0f)
+        float data_tau = 25.0f, float *disp_levels = nullptr, float *plane_levels = nullptr)
 {
     if (L < 1 || min_level < 0 || min_level > L - 1)
         return -1;
@@ -608,8 +608,53 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
     eng.max_steps = max_steps;
     eng.fp16_msg = fp16_msg;
     eng.setup(level_sizes, clus, mean, bd, bdl);
+    // map_msg (hbp_isp.cu:1081-1105) of level li: first slot among 0..3
+    // holding the minimum belief; per pixel d = clamp(a*x + b*y + c, 0, D-1).
+    auto map_level = [&](int li, float *d_out, float *p_out) {
+        const Level<R> &l = eng.lv[li];
+        std::vector<P4<R>> best(l.N);
+        for (int n = 0; n < l.N; ++n)
+        {
+            R mn = l.belief[n];
+            for (int p = 1; p < P; ++p)
+                mn = std::min(mn, l.belief[(size_t)p * l.N + n]);
+            int mp = 0;
+            for (int p = 0; p < P; ++p)
+                if (l.belief[(size_t)p * l.N + n] == mn)
+                {
+                    mp = p;
+                    break;
+                }
+            best[n] = l.plane[(size_t)mp * l.N + n];
+        }
+        for (int k = 0; k < l.N; ++k)
+            for (int j = l.pix_off[k]; j < l.pix_off[k + 1]; ++j)
+            {
+                int px = l.pix[j];
+                const P4<R> &pl = best[k];
+                R x = (R)(px % W), y = (R)(px / W);
+                R d = pl.x * x + pl.y * y + pl.z;
+                d = std::fmin(std::fmax(d, (R)0), (R)(D - 1));
+                d_out[px] = (float)d;
+                if (p_out)
+                {
+                    p_out[3 * (size_t)px] = (float)pl.x;
+                    p_out[3 * (size_t)px + 1] = (float)pl.y;
+                    p_out[3 * (size_t)px + 2] = (float)pl.z;
+                }
+            }
+    };
+    // HBP_ISP::run_ms_vis (hbp_isp.cu:1348-1383) keeps every level's map,
+    // from the top level L-1 down to min_level, at index L-1-li
+    const size_t HW = (size_t)W * H;
+    auto keep_level = [&](int li) {
+        if (disp_levels)
+            map_level(li, disp_levels + (size_t)(L - 1 - li) * HW,
+                      plane_levels ? plane_levels + (size_t)(L - 1 - li) * HW * 3 : nullptr);
+    };
     // top level: messages and beliefs zero, planes zero (never written by the
     // reference, hbp_isp.cu:1333-1337)
+    keep_level(L - 1);
     int lm = min_level;
     for (int li = L - 2; li >= min_level; --li)
     {
@@ -619,6 +664,7 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
             lm = li;
             break;
         }
+        keep_level(li);
     }
     Level<R> &l = eng.lv[lm];
     if (state_belief)
@@ -632,39 +678,7 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
             state_plane[4 * i + 2] = (float)l.plane[i].z;
             state_plane[4 * i + 3] = (float)l.plane[i].w;
         }
-    // map_msg (hbp_isp.cu:1081-1105): first slot among 0..3 holding the
-    // minimum belief; per pixel d = clamp(a*x + b*y + c, 0, D-1).
-    std::vector<P4<R>> best(l.N);
-    for (int n = 0; n < l.N; ++n)
-    {
-        R mn = l.belief[n];
-        for (int p = 1; p < P; ++p)
-            mn = std::min(mn, l.belief[(size_t)p * l.N + n]);
-        int mp = 0;
-        for (int p = 0; p < P; ++p)
-            if (l.belief[(size_t)p * l.N + n] == mn)
-            {
-                mp = p;
-                break;
-            }
-        best[n] = l.plane[(size_t)mp * l.N + n];
-    }
-    for (int k = 0; k < l.N; ++k)
-        for (int j = l.pix_off[k]; j < l.pix_off[k + 1]; ++j)
-        {
-            int px = l.pix[j];
-            const P4<R> &pl = best[k];
-            R x = (R)(px % W), y = (R)(px / W);
-            R d = pl.x * x + pl.y * y + pl.z;
-            d = std::fmin(std::fmax(d, (R)0), (R)(D - 1));
-            disp[px] = (float)d;
-            if (plane_out)
-            {
-                plane_out[3 * (size_t)px] = (float)pl.x;
-                plane_out[3 * (size_t)px + 1] = (float)pl.y;
-                plane_out[3 * (size_t)px + 2] = (float)pl.z;
-            }
-        }
+    map_level(lm, disp, plane_out);
     return (int)eng.steps;
 }
 } // namespace
@@ -720,6 +734,27 @@ int orc_hbp_f32(const int *level_sizes, int L, const int *clus, const float *mea
                            data_tau);
     return run<float>(level_sizes, L, clus, mean, bd, bdl, nullptr, wta, W, H, D, alpha, tau_smooth, min_level,
                       max_steps, disp, plane, state_belief, state_plane, mode == 2, volf, data_tau);
+}
+
+// HBP_ISP::run_ms_vis (hbp_isp.cu:1348-1383) without its superpixel image:
+// the disparity (HW) and planes (HW x 3) of every level from the top level
+// L-1 down to min_level, at index L-1-li of disp_levels / plane_levels
+// (plane_levels may be null). vol (uint8) or volf (float, with data_tau)
+// gives the data term. Modes as orc_hbp. Returns the number of BP steps.
+int orc_hbp_levels(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+                   const int *bdl, const uint8_t *vol, const float *volf, const float *wta, int W, int H, int D,
+                   float data_tau, float alpha, float tau_smooth, int min_level, int mode, float *disp_levels,
+                   float *plane_levels)
+{
+    if ((vol == nullptr) == (volf == nullptr) || !disp_levels || L < 1 || min_level < 0 || min_level > L - 1)
+        return -1;
+    std::vector<float> disp((size_t)W * H);
+    if (mode == 1)
+        return run<double>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth, min_level, -1,
+                           disp.data(), nullptr, nullptr, nullptr, false, volf, data_tau, disp_levels,
+                           plane_levels);
+    return run<float>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth, min_level, -1,
+                      disp.data(), nullptr, nullptr, nullptr, mode == 2, volf, data_tau, disp_levels, plane_levels);
 }
 
 } // extern "C"

@@ -44,6 +44,9 @@ def lib():
         _lib.orc_hbp_f32.restype = C.c_int
         _lib.orc_hbp_f32.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
                                      C.c_float, C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
+        _lib.orc_hbp_levels.restype = C.c_int
+        _lib.orc_hbp_levels.argtypes = [P, C.c_int, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
+                                        C.c_float, C.c_float, C.c_int, C.c_int, P, P]
         _lib.orc_cost_f32.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
         _lib.orc_cost_f32_right.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, P]
         _lib.orc_grey_f32.argtypes = [P, C.c_int, P]
@@ -213,6 +216,29 @@ def cost_f32(src, tau=0.5, right=False):
     f = lib().orc_cost_f32_right if right else lib().orc_cost_f32
     f(_p(src), W, H, D, tau, _p(vol), _p(wta))
     return vol, wta
+
+
+def hbp_levels(seg, vol, wta, W, H, D, volf=None, tau=25.0, alpha=1000.1, tau_smooth=0.6, min_level=2,
+               fp16_msg=False):
+    """HBP_ISP::run_ms_vis without its superpixel image: (disp [L-m][H][W],
+    plane [L-m][H][W][3]) from the top level down to min_level. vol is the
+    uint8 volume [D][H*W], or None with volf the float one."""
+    sizes = np.ascontiguousarray(seg["level_sizes"], np.int32)
+    L = sizes.shape[0]
+    n = L - min_level
+    disp = np.zeros((n, H, W), np.float32)
+    plane = np.zeros((n, H, W, 3), np.float32)
+    vb = None if vol is None else np.ascontiguousarray(vol, np.uint8)
+    vf = None if volf is None else np.ascontiguousarray(volf, np.float32)
+    steps = lib().orc_hbp_levels(_p(sizes), L, _p(np.ascontiguousarray(seg["clus"], np.int32)),
+                                 _p(np.ascontiguousarray(seg["mean"], np.float32)),
+                                 _p(np.ascontiguousarray(seg["bd"], np.int32)),
+                                 _p(np.ascontiguousarray(seg["bdl"], np.int32)), _p(vb), _p(vf),
+                                 _p(np.ascontiguousarray(wta, np.float32)), W, H, D, tau, alpha, tau_smooth,
+                                 min_level, 2 if fp16_msg else 0, _p(disp), _p(plane))
+    if steps < 0:
+        raise ValueError("orc_hbp_levels rejected its input")
+    return disp, plane
 
 
 def grey_f32(bgr):

@@ -6,7 +6,8 @@
 //           weighted median, plane -> disparity)
 // with the Census and AD costs (alpha 1000.1) and, given an im0.acrt-style
 // volume file, the MC-CNN cost (alpha 1.3, bench_MiddV3_train.sh:6). Writes
-// <out_prefix>{census,ad,mccnn}_{single,lr}.f32.
+// <out_prefix>{census,ad,mccnn}_{single,lr,levels}.f32 (levels: every level's
+// disparity from HBP_ISP::run_ms_vis, top level first).
 // usage: compat_pipeline left.bgr right.bgr W H D out_prefix [vol.acrt]
 #include <cstdio>
 #include <cstdlib>
@@ -33,7 +34,7 @@ static void write_f32(const char *path, const Mat &m)
 }
 
 static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, const std::string &vol_dir,
-                  float alpha, const char *out_single, const char *out_lr)
+                  float alpha, const std::string &out)
 {
     const float tau_smooth = 0.6f;
     const int min_level = 2;
@@ -51,7 +52,13 @@ static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, co
     auto results_left = hbp->run_ms(min_level);
     Mat disp = results_left.first.clone();
     medianFilter(disp);
-    write_f32(out_single, disp);
+    write_f32((out + "_single.f32").c_str(), disp);
+    {
+        // every level's map (run_ms_vis), top level first, concatenated
+        std::ofstream f(out + "_levels.f32", std::ios::binary);
+        for (const auto &lv : hbp->run_ms_vis(min_level))
+            f.write(reinterpret_cast<const char *>(std::get<0>(lv).data), (std::streamsize)std::get<0>(lv).bytes());
+    }
 
     // MidV3_LR: the right view, then LR check, fill and weighted median
     SegHAC *seg_r = new SegHAC(R, CentoridLink, 4, 0, LabelISPFormat, 1, false);
@@ -70,7 +77,7 @@ static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, co
     post->plane_label_to_disp(results_left, results_right);
     post->median_filter(results_left, results_right);
     post->plane_label_to_disp(results_left, results_right);
-    write_f32(out_lr, results_left.first);
+    write_f32((out + "_lr.f32").c_str(), results_left.first);
 
     delete post;
     delete hbp_r;
@@ -93,11 +100,10 @@ int main(int argc, char **argv)
     try
     {
         Mat L = read_bgr(argv[1], W, H), R = read_bgr(argv[2], W, H);
-        flows(L, R, D, "Census", "", 1000.1f, (out + "census_single.f32").c_str(), (out + "census_lr.f32").c_str());
-        flows(L, R, D, "AD", "", 1000.1f, (out + "ad_single.f32").c_str(), (out + "ad_lr.f32").c_str());
+        flows(L, R, D, "Census", "", 1000.1f, out + "census");
+        flows(L, R, D, "AD", "", 1000.1f, out + "ad");
         if (argc == 8)
-            flows(L, R, D, "MC-CNN", argv[7], 1.3f, (out + "mccnn_single.f32").c_str(),
-                  (out + "mccnn_lr.f32").c_str());
+            flows(L, R, D, "MC-CNN", argv[7], 1.3f, out + "mccnn");
     }
     catch (const std::exception &e)
     {

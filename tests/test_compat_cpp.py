@@ -38,7 +38,11 @@ def _run_driver(tmp_path, s, W, H, D, src=None):
         args.append(str(tmp_path / "im0.acrt"))
     r = subprocess.run(args, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
-    return lambda name: np.fromfile(tmp_path / f"o_{name}.f32", np.float32).reshape(H, W)
+
+    def read(name):  # one H x W map, or [levels][H][W] for "*_levels"
+        a = np.fromfile(tmp_path / f"o_{name}.f32", np.float32).reshape(-1, H, W)
+        return a if name.endswith("levels") else a[0]
+    return read
 
 
 def _flows_via_stages(E, ctx, torch, s, D, vols, tau, alpha):
@@ -91,9 +95,19 @@ def test_driver_flows_match_the_engine(tmp_path):
         gL, gR = (torch.zeros(W * H, dtype=torch.float32, device="cuda") for _ in range(2))
         ctx.cost_ad_d(cuda(s.left), cuda(s.right), W, H, D, gL, gR, *vols)
         ad1, ad2 = _flows_via_stages(E, ctx, torch, s, D, vols, 30.0, 1000.1)
+        # run_ms_vis of the Census flow against the engine's per-level entry point
+        cL, cR = (torch.zeros(W * H, dtype=torch.int32, device="cuda") for _ in range(2))
+        vol = torch.zeros(E.volume_bytes(W, H, D), dtype=torch.uint8, device="cuda")
+        wta = torch.zeros(W * H, device="cuda")
+        ctx.cost_census_d(cuda(s.left), cuda(s.right), W, H, D, cL, cR, vol, wta, None, None)
+        L = ctx.segment_d(cuda(s.left), W, H)
+        lv = torch.zeros((L - 2) * W * H, device="cuda")
+        n = ctx.infer_levels_d(vol, None, wta, D, 25.0, E.default_params(), L - 2, lv)
+        levels = lv.cpu().numpy().reshape(n, H, W)
     finally:
         ctx.close()
     assert _same(out("census_single"), want1) and _same(out("census_lr"), want2)
+    assert _same(out("census_levels"), levels)
     assert _same(out("ad_single"), ad1) and _same(out("ad_lr"), ad2)
 
 

@@ -231,3 +231,18 @@ def test_ad_path_agrees_with_reference(golden_dir, name):
         res = O.pipeline_ad(s.left, s.right, D, right_view=right)
         diff = np.abs(res["disp"] - z[dk])
         assert np.mean(diff == 0) >= 0.95 and np.mean(diff < 1.0) >= 0.985, (np.mean(diff == 0), np.mean(diff < 1))
+
+
+def test_levels_end_with_the_ordinary_result():
+    """The oracle's per-level maps (run_ms_vis) end with run_ms's result and
+    start with the all-zero top level."""
+    from scenes import make_scene
+    s = make_scene(96, 64, 32, 7)
+    cs = O.cost_stage(s.left, s.right, 32)
+    seg = O.segment(O.lab(s.left))
+    d, p = O.hbp_levels(seg, cs["vol"], cs["wta"], 96, 64, 32)
+    od, op, _, _, _ = O.hbp(seg, cs["vol"], cs["wta"], 96, 64, 32)
+    assert d.shape[0] == len(seg["level_sizes"]) - 2
+    assert np.array_equal(d[-1].view(np.uint32), od.view(np.uint32))
+    assert np.array_equal(p[-1].view(np.uint32), op.view(np.uint32))
+    assert not d[0].any() and not p[0].any()
