@@ -145,11 +145,22 @@ hbp_status guarded(F &&f)
     }
 }
 
+// per pixel: the volume(s), the pyramid (room for the 8-neighbour grid's
+// edges) and the BP data; temporaries of the segmentation and the BP setup
 size_t slab_bytes(long pixels, int D)
 {
-    return (size_t)pixels * (size_t)(2 * (D + 16) + 1200) + ((size_t)96 << 20);
+    return (size_t)pixels * (size_t)(2 * (D + 16) + 1296) + ((size_t)96 << 20);
 }
-size_t tmp_bytes(long pixels) { return (size_t)pixels * 480 + ((size_t)64 << 20); }
+size_t tmp_bytes(long pixels) { return (size_t)pixels * 560 + ((size_t)64 << 20); }
+
+SegConfig seg_config(const hbp_params &p)
+{
+    SegConfig s;
+    s.link = p.linkage;
+    s.num_nb = p.num_nb;
+    s.sigma = p.sigma;
+    return s;
+}
 
 void ensure_capacity(Lane *c, long pixels, int D)
 {
@@ -237,9 +248,10 @@ void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint
         launch_cost(dL, dR, W, H, D, cL, cR, vol, wta, volR, wtaR, st);
     }
     HbpParams q = to_params(&p);
+    const SegConfig seg = seg_config(p);
     {
         NvtxRange r("segmentation");
-        segment_image(dL, W, H, sl->pyr, a, L->tmp, L->err_dev, st);
+        segment_image(dL, W, H, sl->pyr, a, L->tmp, L->err_dev, st, seg);
         check_device_error(L);
     }
     L->tmp.reset();
@@ -252,7 +264,7 @@ void prepare_pair(hbp_ctx *ctx, Lane *L, Slot *sl, const uint8_t *dL, const uint
         sl->dispR = a.alloc<float>(n);
         sl->planeR = a.alloc<float>(3 * n);
         L->tmp.reset();
-        segment_image(dR, W, H, sl->pyrR, a, L->tmp, L->err_dev, st);
+        segment_image(dR, W, H, sl->pyrR, a, L->tmp, L->err_dev, st, seg);
         check_device_error(L);
         L->tmp.reset();
         hbp_prepare(sl->pyrR, volR, wtaR, D, q, sl->dispR, sl->planeR, a, L->tmp, st, sl->planR);
@@ -343,6 +355,9 @@ void hbp_default_params(hbp_params *p)
     p->min_level = 2;
     p->msg_fp16 = 0;
     p->post = 1;
+    p->linkage = 2; // CentoridLink, 4-neighbour grid, no blur (test_stereo_hbp_isp.sh:4)
+    p->num_nb = 4;
+    p->sigma = 0.0;
 }
 
 const char *hbp_status_string(hbp_status s)
@@ -469,9 +484,44 @@ hbp_status hbp_crtrees_d(hbp_ctx *c, const int *nn, int N, int *clus, int *num_c
 
 hbp_status hbp_segment_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int *levels, void *stream)
 {
+    return hbp_segment_cfg_d(c, bgr, W, H, 2, 4, 0.0, levels, stream);
+}
+
+hbp_status hbp_lab_sigma_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, double sigma, float *lab4, void *stream)
+{
+    if (!c || !bgr || !lab4)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 16);
+        SegConfig cfg;
+        cfg.sigma = sigma;
+        check_seg_config(cfg);
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        if (sigma > 1.1754943508222875e-38) // FLT_MIN, as segment.cu:805
+        {
+            c->tmp.reset();
+            float4 *blur = c->tmp.alloc<float4>((size_t)W * H);
+            launch_lab_blur(bgr, W, H, sigma, blur, (float4 *)lab4, st);
+        }
+        else
+            launch_lab(bgr, W * H, (float4 *)lab4, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_segment_cfg_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int linkage, int num_nb, double sigma,
+                             int *levels, void *stream)
+{
     if (!c || !bgr || !levels)
         return fail(HBP_ERR_INVALID_ARG, "null pointer");
     return guarded([&] {
+        SegConfig cfg;
+        cfg.link = linkage;
+        cfg.num_nb = num_nb;
+        cfg.sigma = sigma;
+        check_seg_config(cfg);
         check_dims(W, H, 16);
         HBP_CUDA(cudaSetDevice(c->device));
         ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
@@ -480,7 +530,7 @@ hbp_status hbp_segment_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int *leve
         c->tmp.reset();
         HBP_CUDA(cudaMemsetAsync(c->err_dev, 0, sizeof(int), st));
         c->have_pyr = false;
-        segment_image(bgr, W, H, c->pyr, c->arena, c->tmp, c->err_dev, st);
+        segment_image(bgr, W, H, c->pyr, c->arena, c->tmp, c->err_dev, st, cfg);
         check_device_error(c);
         c->have_pyr = true;
         *levels = c->pyr.L;
@@ -850,6 +900,7 @@ hbp_status hbp_run_pair(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *bgrR, in
     if (p.post < 0 || p.post > 2)
         return fail(HBP_ERR_INVALID_ARG, "post must be 0, 1 or 2");
     return guarded([&] {
+        check_seg_config(seg_config(p));
         check_dims(W, H, D);
         HBP_CUDA(cudaSetDevice(c->device));
         const long n = (long)W * H;
@@ -893,6 +944,11 @@ hbp_status hbp_run_batch_d(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, c
     const hbp_params &p = prm ? *prm : def;
     if (p.post < 0 || p.post > 2)
         return fail(HBP_ERR_INVALID_ARG, "post must be 0, 1 or 2");
+    {
+        hbp_status st = guarded([&] { check_seg_config(seg_config(p)); });
+        if (st != HBP_OK)
+            return st;
+    }
     for (int i = 0; i < npairs; ++i)
         if (!bgrL[i] || !bgrR[i] || !disp[i])
             return fail(HBP_ERR_INVALID_ARG, "null pair pointer");
@@ -1282,6 +1338,12 @@ hbp_status hbp_server_create(int device, size_t budget_bytes, int prep_lanes, co
         return fail(HBP_ERR_INVALID_ARG, "need a budget > 0 and 1..64 preparation lanes");
     if (prm && (prm->post < 0 || prm->post > 1))
         return fail(HBP_ERR_INVALID_ARG, "the server runs post = 0 or 1 (driver median)");
+    if (prm)
+    {
+        hbp_status st = guarded([&] { check_seg_config(seg_config(*prm)); });
+        if (st != HBP_OK)
+            return st;
+    }
     *out = nullptr;
     auto s = std::make_unique<hbp_server>();
     s->device = device;

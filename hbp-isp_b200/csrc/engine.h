@@ -84,6 +84,10 @@ void launch_cost_ad(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int 
 
 // lab.cu
 void launch_lab(const uint8_t *bgr, int n, float4 *lab, cudaStream_t st);
+// LAB of the image blurred with sigma > 0 (tmp4: W*H float4 scratch)
+constexpr int BLUR_MAX_S = 7; // the reference's filter buffer: 15 x 15 (segment.hpp:303-306)
+int blur_radius(double sigma);
+void launch_lab_blur(const uint8_t *bgr, int W, int H, double sigma, float4 *tmp4, float4 *lab, cudaStream_t st);
 
 // scan_sort.cu
 size_t scan_scratch_bytes(long n);
@@ -120,11 +124,29 @@ struct Pyramid
     int *nb_off = nullptr;     // per level N_l + 1 at nb_base[l]
 };
 
-// segment.cu: SegHAC::run_ms with CentroidLink / 4-grid / sigma 0. Uses `a`
-// for the pyramid and `tmp` for temporaries; the host learns each level's size
+// SegHAC's configuration (segment.hpp:248): linkage (segment.hpp:8-16),
+// pixel neighbourhood and pre-blur. The path's default is CentroidLink, 4, 0.
+enum SegLinkage
+{
+    LINK_MIN = 0,
+    LINK_MAX = 1,
+    LINK_CENTROID = 2,
+    LINK_WARD = 3
+};
+struct SegConfig
+{
+    int link = LINK_CENTROID;
+    int num_nb = 4;
+    double sigma = 0.0;
+};
+// Rejects configurations the reference cannot run (HBP_ERR_INVALID_ARG).
+void check_seg_config(const SegConfig &cfg);
+
+// segment.cu: SegHAC::run_ms with LabelISPFormat and target 1. Uses `a` for
+// the pyramid and `tmp` for temporaries; the host learns each level's size
 // (one small device-to-host read per level).
 void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
-                   int *err_dev, cudaStream_t st);
+                   int *err_dev, cudaStream_t st, const SegConfig &cfg = SegConfig{});
 
 // ---------------------------------------------------------------------------
 // hbp.cu

@@ -1,5 +1,7 @@
-// Image segmentation pyramid (SegHAC with CentroidLink, 4-neighbour grid,
-// sigma = 0, LabelISPFormat, target 1): reference segment.cu:1279-1321.
+// Image segmentation pyramid (SegHAC with LabelISPFormat, target 1):
+// reference segment.cu:1279-1321. The path runs CentroidLink, 4-neighbour
+// grid, sigma = 0; Min / Max / Ward linkage, the 8-neighbour grid and the
+// Gaussian pre-blur are the reference's other configurations.
 //
 // Level l holds N_l nodes and E_l directed edges. Per level the loop runs
 // CRTrees on the 1-NN successor array, records the level in the reference's
@@ -12,7 +14,9 @@
 //   * child sums of (L, a, b, x, y, count), added in increasing child index
 //     (the reference uses float atomics, segment.cu:472-486);
 //   * centroid distance with the hinge on L, fused as the reference's device
-//     code fuses it, plus the penalty d += max(d - maxinner[t], 0)
+//     code fuses it (Ward: times w_s w_t / (w_s + w_t), :559-577), or for
+//     Min / Max linkage the min / max of the merged edges' distances
+//     (reduce_dist, :336-366), plus the penalty d += max(d - maxinner[t], 0)
 //     (segment.cu:508-534, :582-612);
 //   * per node the minimum over its out-edges, ties to the largest target
 //     (segment.cu:403-422, :1211-1231).
@@ -31,12 +35,15 @@ __device__ __forceinline__ float pix_dist(float4 s, float4 t)
     return __fadd_rn(d, dx > 0.f ? dx : 0.f);
 }
 
-// compute_1nn_grid_k (segment.cu:57-195), num_nb = 4: neighbours up, down,
-// left, right; first strict minimum. Also writes the level-0 edge list
-// bd[4i+k] = (i, neighbour or i) and the level-0 sums (L, a, b, x, y, 1).
+// compute_1nn_grid_k (segment.cu:57-195), NB = 4 or 8: neighbours up, down,
+// left, right, then up-left, up-right, down-right, down-left; first strict
+// minimum. Also writes the level-0 edge list bd[NB*i+k] = (i, neighbour or i),
+// the edge distances (edist, Min / Max linkage only; 0 on self-edges) and the
+// level-0 sums (L, a, b, x, y, w).
+template <int NB>
 __global__ void nn_grid_kernel(const float4 *__restrict__ lab, int W, int H, int *__restrict__ nn,
                                float *__restrict__ dist_min, int2 *__restrict__ bd,
-                               int *__restrict__ bdl, float *__restrict__ sums)
+                               int *__restrict__ bdl, float *__restrict__ sums, float *__restrict__ edist)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = W * H;
@@ -44,19 +51,25 @@ __global__ void nn_grid_kernel(const float4 *__restrict__ lab, int W, int H, int
         return;
     int y = i / W, x = i - y * W;
     float4 s = lab[i];
-    int nb[4] = {y > 0 ? i - W : -1, y < H - 1 ? i + W : -1, x > 0 ? i - 1 : -1,
-                 x < W - 1 ? i + 1 : -1};
+    const bool up = y > 0, dn = y < H - 1, lf = x > 0, rt = x < W - 1;
+    int nb[8] = {up ? i - W : -1,           dn ? i + W : -1,           lf ? i - 1 : -1,
+                 rt ? i + 1 : -1,           up && lf ? i - W - 1 : -1, up && rt ? i - W + 1 : -1,
+                 dn && rt ? i + W + 1 : -1, dn && lf ? i + W - 1 : -1};
     float best = 3.402823466e+38f;
     int arg = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < NB; ++k)
     {
         int t = nb[k];
-        bd[4 * i + k] = make_int2(i, t < 0 ? i : t);
-        bdl[4 * i + k] = 1;
+        bd[NB * i + k] = make_int2(i, t < 0 ? i : t);
+        bdl[NB * i + k] = 1;
+        if (edist)
+            edist[NB * i + k] = 0.0f;
         if (t < 0)
             continue;
         float d = pix_dist(s, lab[t]);
+        if (edist)
+            edist[NB * i + k] = d;
         if (d < best)
         {
             best = d;
@@ -164,6 +177,47 @@ __global__ void parent_sums(const uint32_t *__restrict__ child, const int *__res
     dmax_p[p] = mx;
 }
 
+// reduce_dist (segment.cu:336-366) for Min / Max linkage: every merged edge
+// (s, t), s != t, folds its distance into the new edge (s, t) with min / max.
+// The new edges are sorted by (s, t), so t is found by binary search in s's
+// out-edge range. Distances are >= 0, so their bit patterns order as ints.
+__global__ void reduce_edge_dist(const int2 *__restrict__ bd_c, const float *__restrict__ edist_c,
+                                 const int *__restrict__ clus, long E, const int2 *__restrict__ bd_p,
+                                 const int *__restrict__ off_p, int use_max, float *__restrict__ edist_p)
+{
+    long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E)
+        return;
+    const int2 v = bd_c[e];
+    const int s = clus[v.x], t = clus[v.y];
+    if (s == t)
+        return;
+    int lo = off_p[s], hi = off_p[s + 1] - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (bd_p[mid].y < t)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    if (lo > hi || bd_p[lo].y != t)
+        return; // cannot happen: every merged pair is a new edge
+    int *dst = reinterpret_cast<int *>(edist_p + lo);
+    const int bits = __float_as_int(edist_c[e]);
+    if (use_max)
+        atomicMax(dst, bits);
+    else
+        atomicMin(dst, bits);
+}
+
+__global__ void fill_f32(float *p, long n, float v)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        p[i] = v;
+}
+
 __global__ void edge_src_count(const int2 *__restrict__ bd, int E, int *__restrict__ count)
 {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,10 +226,14 @@ __global__ void edge_src_count(const int2 *__restrict__ bd, int E, int *__restri
 }
 
 // One thread per node walks its out-edges (contiguous, targets ascending):
-// centroid distance + penalty, minimum, and the largest target among minima.
+// the edge distance (centroid from the means, times the Ward weight from the
+// weight sums wsum; or the reduced distance in edist for Min / Max, where the
+// penalised value is written back for the next level) + penalty, minimum, and
+// the largest target among minima.
 __global__ void node_1nn(const int2 *__restrict__ bd, const int *__restrict__ off, int N,
                          const float *__restrict__ mean, const float *__restrict__ dmax,
-                         int *__restrict__ nn, float *__restrict__ dist_min)
+                         int *__restrict__ nn, float *__restrict__ dist_min, int link,
+                         const float *__restrict__ wsum, float *__restrict__ edist)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= N)
@@ -186,12 +244,25 @@ __global__ void node_1nn(const int2 *__restrict__ bd, const int *__restrict__ of
     for (int e = off[s]; e < off[s + 1]; ++e)
     {
         int t = bd[e].y;
-        float e0 = __fsub_rn(ls, mean[t]), e1 = __fsub_rn(as, mean[N + t]), e2 = __fsub_rn(bs, mean[2 * N + t]);
-        float h = e0 > 0.f ? e0 : 0.f;
-        float d = __fmaf_rn(e2, e2, __fmaf_rn(e1, e1, __fmaf_rn(e0, e0, h)));
+        float d;
+        if (link == LINK_MIN || link == LINK_MAX)
+            d = edist[e];
+        else
+        {
+            float e0 = __fsub_rn(ls, mean[t]), e1 = __fsub_rn(as, mean[N + t]), e2 = __fsub_rn(bs, mean[2 * N + t]);
+            float h = e0 > 0.f ? e0 : 0.f;
+            d = __fmaf_rn(e2, e2, __fmaf_rn(e1, e1, __fmaf_rn(e0, e0, h)));
+            if (link == LINK_WARD)
+            {
+                const float sw = wsum[s], tw = wsum[t];
+                d = __fmul_rn(__fdiv_rn(__fmul_rn(sw, tw), __fadd_rn(sw, tw)), d);
+            }
+        }
         float delta = __fsub_rn(d, dmax[t]);
         if (delta > 0)
             d = __fadd_rn(d, delta);
+        if (edist)
+            edist[e] = d;
         if (d < best)
         {
             best = d;
@@ -221,10 +292,22 @@ int read_int(const int *dev, cudaStream_t st)
 }
 } // namespace
 
-void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
-                   int *err_dev, cudaStream_t st)
+void check_seg_config(const SegConfig &cfg)
 {
-    const int N0 = W * H;
+    if (cfg.link < LINK_MIN || cfg.link > LINK_WARD)
+        throw StatusError{HBP_ERR_INVALID_ARG, "linkage must be 0 (Min), 1 (Max), 2 (Centroid) or 3 (Ward)"};
+    if (cfg.num_nb != 4 && cfg.num_nb != 8)
+        throw StatusError{HBP_ERR_INVALID_ARG, "num_nb must be 4 or 8"};
+    if (!(cfg.sigma >= 0.0) || blur_radius(cfg.sigma) > BLUR_MAX_S)
+        throw StatusError{HBP_ERR_INVALID_ARG, "sigma must lie in [0, 2.5): the blur radius round(3 sigma) <= 7"};
+}
+
+void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
+                   int *err_dev, cudaStream_t st, const SegConfig &cfg)
+{
+    check_seg_config(cfg);
+    const int N0 = W * H, NB = cfg.num_nb;
+    const bool use_mean = cfg.link == LINK_CENTROID || cfg.link == LINK_WARD;
     pyr.W = W;
     pyr.H = H;
     pyr.L = 0;
@@ -237,8 +320,8 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
     // capacities of the concatenated ISP arrays (segment.hpp:276-283)
     pyr.clus = a.alloc<int>(2 * (size_t)N0);
     pyr.sums = a.alloc<float>(12 * (size_t)N0);
-    pyr.bd = a.alloc<int2>(8 * (size_t)N0);
-    pyr.bdl = a.alloc<int>(8 * (size_t)N0);
+    pyr.bd = a.alloc<int2>(2 * (size_t)NB * N0);
+    pyr.bdl = a.alloc<int>(2 * (size_t)NB * N0);
     pyr.child = a.alloc<uint32_t>(2 * (size_t)N0);
     pyr.child_off = a.alloc<int>(2 * (size_t)N0 + 64);
     pyr.nb_off = a.alloc<int>(2 * (size_t)N0 + 64);
@@ -251,18 +334,32 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
     float *dmax = tmp.alloc<float>(N0);
     int *count = tmp.alloc<int>(N0 + 1);
     int *num_dev = tmp.alloc<int>(2);
-    uint64_t *keys = tmp.alloc<uint64_t>(4 * (size_t)N0), *keys_alt = tmp.alloc<uint64_t>(4 * (size_t)N0);
-    int *keep = tmp.alloc<int>(4 * (size_t)N0), *slot = tmp.alloc<int>(4 * (size_t)N0);
+    uint64_t *keys = tmp.alloc<uint64_t>((size_t)NB * N0), *keys_alt = tmp.alloc<uint64_t>((size_t)NB * N0);
+    int *keep = tmp.alloc<int>((size_t)NB * N0), *slot = tmp.alloc<int>((size_t)NB * N0);
     uint32_t *ck = tmp.alloc<uint32_t>(N0), *ck_alt = tmp.alloc<uint32_t>(N0),
              *cv_alt = tmp.alloc<uint32_t>(N0);
+    // edge distances of the current and the next level (Min / Max linkage)
+    float *edist = use_mean ? nullptr : tmp.alloc<float>((size_t)NB * N0);
+    float *edist2 = use_mean ? nullptr : tmp.alloc<float>((size_t)NB * N0);
 
-    launch_lab(bgr, N0, lab, st);
-    nn_grid_kernel<<<ceil_div(N0, 256), 256, 0, st>>>(lab, W, H, nn, dmin, pyr.bd, pyr.bdl, pyr.sums);
+    if (cfg.sigma > 1.1754943508222875e-38) // FLT_MIN, as segment.cu:805
+    {
+        size_t mb = tmp.mark();
+        float4 *blur = tmp.alloc<float4>(N0);
+        launch_lab_blur(bgr, W, H, cfg.sigma, blur, lab, st);
+        tmp.rewind(mb); // later users of the scratch run after the blur (same stream)
+    }
+    else
+        launch_lab(bgr, N0, lab, st);
+    if (NB == 8)
+        nn_grid_kernel<8><<<ceil_div(N0, 256), 256, 0, st>>>(lab, W, H, nn, dmin, pyr.bd, pyr.bdl, pyr.sums, edist);
+    else
+        nn_grid_kernel<4><<<ceil_div(N0, 256), 256, 0, st>>>(lab, W, H, nn, dmin, pyr.bd, pyr.bdl, pyr.sums, edist);
     note_launch();
     HBP_LAUNCH_CHECK();
 
     int N = N0;
-    long E = 4l * N0;
+    long E = (long)NB * N0;
     size_t oc = 0, ob = 0, och = 0, onb = 0;
     for (;;)
     {
@@ -321,7 +418,7 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         HBP_LAUNCH_CHECK();
         exclusive_scan(keep, slot, E, num_dev + 1, tmp, st);
         int E2 = read_int(num_dev + 1, st);
-        if ((size_t)(ob + E + E2) > 8 * (size_t)N0 || E2 < 1)
+        if ((size_t)(ob + E + E2) > 2 * (size_t)NB * N0 || E2 < 1)
             throw StatusError{HBP_ERR_INTERNAL, "edge capacity exceeded"};
         HBP_CUDA(cudaMemsetAsync(bdl_p, 0, sizeof(int) * E2, st));
         emit_edges<<<ceil_div(E, 256), 256, 0, st>>>(keys, keep, slot, bdl_c, E, bits, bd_p, bdl_p);
@@ -338,11 +435,22 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         note_launch();
         HBP_LAUNCH_CHECK();
         exclusive_scan(count, slot, Nn + 1, nullptr, tmp, st);
-        node_1nn<<<ceil_div(Nn, 128), 128, 0, st>>>(bd_p, slot, Nn, mean, dmax, nn2, dmin2);
+        if (!use_mean)
+        {
+            fill_f32<<<ceil_div(E2, 256), 256, 0, st>>>(edist2, E2, cfg.link == LINK_MIN ? 3.402823466e+38f : 0.0f);
+            note_launch();
+            reduce_edge_dist<<<ceil_div(E, 256), 256, 0, st>>>(bd_c, edist, clus, E, bd_p, slot,
+                                                               cfg.link == LINK_MAX ? 1 : 0, edist2);
+            note_launch();
+            HBP_LAUNCH_CHECK();
+        }
+        node_1nn<<<ceil_div(Nn, 128), 128, 0, st>>>(bd_p, slot, Nn, mean, dmax, nn2, dmin2, cfg.link,
+                                                     sums_p + 5 * (size_t)Nn, edist2);
         note_launch();
         HBP_LAUNCH_CHECK();
         std::swap(nn, nn2);
         std::swap(dmin, dmin2);
+        std::swap(edist, edist2);
         oc += N;
         ob += E;
         N = Nn;

@@ -33,7 +33,8 @@ class HbpError(RuntimeError):
 
 class Params(C.Structure):
     _fields_ = [("alpha", C.c_float), ("tau_smooth", C.c_float), ("min_level", C.c_int),
-                ("msg_fp16", C.c_int), ("post", C.c_int)]
+                ("msg_fp16", C.c_int), ("post", C.c_int), ("linkage", C.c_int), ("num_nb", C.c_int),
+                ("sigma", C.c_double)]
 
 
 _lib = None
@@ -197,6 +198,15 @@ class Context:
         k = C.c_int(0)
         _check(lib().hbp_crtrees_d(self.h, _p(nn), N, _p(clus), C.byref(k), None))
         return k.value
+
+    def segment_cfg_d(self, bgr, W, H, linkage, num_nb, sigma) -> int:
+        L = C.c_int(0)
+        _check(lib().hbp_segment_cfg_d(self.h, _p(bgr), W, H, linkage, num_nb, C.c_double(sigma), C.byref(L),
+                                       None))
+        return L.value
+
+    def lab_sigma_d(self, bgr, W, H, sigma, lab4):
+        _check(lib().hbp_lab_sigma_d(self.h, _p(bgr), W, H, C.c_double(sigma), _p(lab4), None))
 
     def segment_d(self, bgr, W, H) -> int:
         L = C.c_int(0)

@@ -54,6 +54,11 @@ typedef struct hbp_params
     int post;         /* 0: none; 1: driver 7-tap median (main_stereo_hbp_isp.cu:75);
                          2: right view + LR check/fill + weighted median + plane->disp
                             (main_bench_middv3.cu:189-219) */
+    /* the segmentation's configuration, the drivers' argv link, num_nb, sigma
+     * (main_stereo_hbp_isp.cu:15-29; SegHAC, segment.hpp:248) */
+    int linkage;      /* 0 MinLink, 1 MaxLink, 2 CentoridLink (default), 3 WardLink */
+    int num_nb;       /* pixel grid neighbours: 4 (default) or 8 */
+    double sigma;     /* Gaussian pre-blur, 0 (default) or round(3 sigma) <= 7 */
 } hbp_params;
 
 void hbp_default_params(hbp_params *p);
@@ -125,6 +130,19 @@ hbp_status hbp_crtrees_d(hbp_ctx *ctx, const int *nn, int N, int *clus, int *num
  * (clus, mean sums [6][N_l], bd pairs, bdl, concatenated over levels) to host
  * buffers of at least the summed sizes. */
 hbp_status hbp_segment_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int *levels, void *stream);
+/* The same for any SegHAC configuration of the reference's drivers (segment.hpp:
+ * 248, segment.cu:1279-1321): linkage 0 MinLink, 1 MaxLink, 2 CentoridLink,
+ * 3 WardLink; num_nb 4 or 8 (compute_1nn_grid_k, segment.cu:57-195); sigma >= 0
+ * the Gaussian pre-blur (img_gauss_blur, imutil.cu:397-497; round(3 sigma)
+ * <= 7, the reference's 15 x 15 filter buffer). hbp_segment_d is
+ * (2, 4, 0.0). */
+hbp_status hbp_segment_cfg_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int linkage, int num_nb,
+                             double sigma, int *levels, void *stream);
+/* SegHAC::img_CPU_to_GPU with sigma (segment.cu:795-809): CIELAB float4 of
+ * the blurred image (the fourth channel is the blurred constant 1), into
+ * lab4 (W*H float4). sigma = 0 gives hbp_lab_d's result. */
+hbp_status hbp_lab_sigma_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, double sigma, float *lab4,
+                           void *stream);
 hbp_status hbp_pyramid_levels(hbp_ctx *ctx, int *sizes, int max_levels);
 hbp_status hbp_pyramid_copy(hbp_ctx *ctx, int *clus, float *mean, int *bd, int *bdl);
 

@@ -20,12 +20,16 @@ void orc_cost_ad(const float *gL, const float *gR, int W, int H, int D, float ta
 void orc_lab_set_overrides(const uint32_t *keys, const float *vals, int n);
 void orc_lab(const uint8_t *bgr, int n, float *lab4);
 void orc_nn_grid(const float *lab4, int W, int H, int *nn, float *dist_min, int *bd);
+void orc_nn_grid_nb(const float *lab4, int W, int H, int num_nb, int *nn, float *dist_min, int *bd, float *edist);
+void orc_lab_sigma(const uint8_t *bgr, int W, int H, double sigma, float *lab4);
 
 // segmentation (oracle_seg.cpp)
 int orc_crtrees(const int *nn, int N, int *clus);
 int orc_crtrees_literal(const int *nn, int N, int *clus);
 int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_sizes, int *clus,
                 float *mean, int *bd, int *bdl);
+int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int max_levels, int *level_sizes,
+                    int *clus, float *mean, int *bd, int *bdl);
 
 // belief propagation (oracle_hbp.cpp)
 void orc_round_fp16(const float *in, float *out, long n);

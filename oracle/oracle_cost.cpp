@@ -232,9 +232,9 @@ void orc_lab_set_overrides(const uint32_t *keys, const float *vals, int n)
     g_lab_override_vals.assign(vals, vals + 3 * (size_t)n);
 }
 
-static inline void lab_one(uint8_t B, uint8_t G, uint8_t R, float *o)
+static inline void lab_of(float B, float G, float R, float W, float *o)
 {
-    double b = (float)B / 255.0, g = (float)G / 255.0, r = (float)R / 255.0;
+    double b = B / 255.0, g = G / 255.0, r = R / 255.0;
     r = (r > 0.04045) ? std::pow((r + 0.055) / 1.055, 2.4) : r / 12.92;
     g = (g > 0.04045) ? std::pow((g + 0.055) / 1.055, 2.4) : g / 12.92;
     b = (b > 0.04045) ? std::pow((b + 0.055) / 1.055, 2.4) : b / 12.92;
@@ -248,8 +248,10 @@ static inline void lab_one(uint8_t B, uint8_t G, uint8_t R, float *o)
     o[0] = (float)std::fma(116.0, y, -16.0);
     o[1] = (float)(500 * (x - y));
     o[2] = (float)(200 * (y - z));
-    o[3] = 1.0f;
+    o[3] = W;
 }
+
+static inline void lab_one(uint8_t B, uint8_t G, uint8_t R, float *o) { lab_of(B, G, R, 1.0f, o); }
 
 void orc_lab(const uint8_t *bgr, int n, float *lab4)
 {
@@ -286,6 +288,120 @@ static inline float pix_dist(const float *s, const float *t)
 // compute_1nn_grid_k (segment.cu:57-195), 4-neighbour grid: neighbours in the
 // order up, down, left, right; the first strict minimum wins. Also writes the
 // level-0 directed edge list bd[4i+k] = (i, neighbour or i).
+// SegHAC::img_CPU_to_GPU with sigma (segment.cu:795-809): the float4 image
+// (B, G, R, 1), blurred when sigma > FLT_MIN by img_gauss_blur (imutil.cu:
+// 397-497), then BGR -> LAB (which keeps the fourth channel). The blur: S =
+// round(3 sigma); weights exp(-(r^2 + c^2) / (2 sigma^2)) in double, scaled by
+// the reciprocal of their sum, stored as float; coordinates clamped to the
+// image; per pixel the taps accumulate row by row (r outer, c inner) from 0 as
+// sum = fma(pixel, weight, sum) per channel, the fused form of the
+// reference's sum += pixel * weight. Pixels are those of a thread whose
+// output position lies inside the image; the reference's edge blocks also let
+// threads beyond a ragged right or bottom edge write the clamped last
+// column/row, so only sizes that are multiples of 16 are deterministic there.
+void orc_lab_sigma(const uint8_t *bgr, int W, int H, double sigma, float *lab4)
+{
+    const size_t n = (size_t)W * H;
+    std::vector<float> img(4 * n);
+    for (size_t i = 0; i < n; ++i)
+    {
+        img[4 * i] = bgr[3 * i];
+        img[4 * i + 1] = bgr[3 * i + 1];
+        img[4 * i + 2] = bgr[3 * i + 2];
+        img[4 * i + 3] = 1.0f;
+    }
+    if (sigma > FLT_MIN)
+    {
+        const int S = (int)std::round(3 * sigma), F = 2 * S + 1;
+        std::vector<double> w64((size_t)F * F);
+        double sum = 0;
+        for (int r = -S; r <= S; ++r)
+            for (int c = -S; c <= S; ++c)
+            {
+                double v = std::exp(-(double)(r * r + c * c) / (2 * sigma * sigma));
+                w64[(size_t)(r + S) * F + c + S] = v;
+                sum += v;
+            }
+        sum = 1. / sum;
+        std::vector<float> w((size_t)F * F);
+        for (size_t k = 0; k < w.size(); ++k)
+            w[k] = (float)(w64[k] * sum);
+        std::vector<float> out(4 * n);
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x)
+            {
+                float acc[4] = {0, 0, 0, 0};
+                for (int r = -S; r <= S; ++r)
+                {
+                    const int yy = std::min(std::max(y + r, 0), H - 1);
+                    for (int c = -S; c <= S; ++c)
+                    {
+                        const int xx = std::min(std::max(x + c, 0), W - 1);
+                        const float wt = w[(size_t)(r + S) * F + c + S];
+                        const float *p = &img[4 * ((size_t)yy * W + xx)];
+                        for (int ch = 0; ch < 4; ++ch)
+                            acc[ch] = std::fma(p[ch], wt, acc[ch]);
+                    }
+                }
+                for (int ch = 0; ch < 4; ++ch)
+                    out[4 * ((size_t)y * W + x) + ch] = acc[ch];
+            }
+        img.swap(out);
+    }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)n; ++i)
+        lab_of(img[4 * i], img[4 * i + 1], img[4 * i + 2], img[4 * i + 3], lab4 + 4 * i);
+}
+
+// compute_1nn_grid_k (segment.cu:57-195) with num_nb = 4 or 8: neighbours up,
+// down, left, right, then up-left, up-right, down-right, down-left; first
+// strict minimum. bd (2 ints per edge) and edist (the distance of each
+// existing edge; missing neighbours give the self-edge (i, i)) are optional.
+void orc_nn_grid_nb(const float *lab4, int W, int H, int num_nb, int *nn, float *dist_min, int *bd, float *edist)
+{
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+        {
+            int i = y * W + x;
+            const float *s = lab4 + 4 * (size_t)i;
+            float best = FLT_MAX;
+            int arg = 0;
+            const int nb[8] = {y > 0 ? i - W : -1,
+                               y < H - 1 ? i + W : -1,
+                               x > 0 ? i - 1 : -1,
+                               x < W - 1 ? i + 1 : -1,
+                               y > 0 && x > 0 ? i - W - 1 : -1,
+                               y > 0 && x < W - 1 ? i - W + 1 : -1,
+                               y < H - 1 && x < W - 1 ? i + W + 1 : -1,
+                               y < H - 1 && x > 0 ? i + W - 1 : -1};
+            for (int k = 0; k < num_nb; ++k)
+            {
+                const size_t e = (size_t)num_nb * i + k;
+                if (bd)
+                {
+                    bd[2 * e] = i;
+                    bd[2 * e + 1] = nb[k] < 0 ? i : nb[k];
+                }
+                if (edist)
+                    edist[e] = 0.0f;
+                if (nb[k] < 0)
+                    continue;
+                float d = pix_dist(s, lab4 + 4 * (size_t)nb[k]);
+                if (edist)
+                    edist[e] = d;
+                if (d < best)
+                {
+                    best = d;
+                    arg = nb[k];
+                }
+            }
+            nn[i] = arg;
+            dist_min[i] = best;
+        }
+}
+
 void orc_nn_grid(const float *lab4, int W, int H, int *nn, float *dist_min, int *bd)
 {
 #pragma omp parallel for schedule(static)

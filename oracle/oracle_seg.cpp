@@ -250,25 +250,30 @@ int orc_crtrees_literal(const int *nn_in, int N, int *clus_out)
     return k;
 }
 
-// SegHAC::run_ms with CentroidLink, 4-grid, sigma 0, LabelISPFormat, target 1
-// (segment.cu:1279-1321). Input: LAB float4 image. Output: the image
-// segmentation pyramid in the reference's ISP layout (segment.cu:884-905):
-// per level l, num_clus N_l and num_bd E_l (level_sizes[2l], [2l+1]); clus
-// (N_l ints: node -> parent), mean (6 x N_l floats, channel-major: sums of L,
-// a, b, x, y and the pixel count), bd (E_l int pairs), bdl (E_l ints),
-// concatenated over levels. Capacities: clus 2*HW, mean 12*HW, bd 16*HW ints,
-// bdl 8*HW. Returns the number of levels.
+// SegHAC::run_ms with LabelISPFormat and target 1 (segment.cu:1279-1321), for
+// the linkages of segment.hpp:8-16 (0 Min, 1 Max, 2 Centroid, 3 Ward) and a
+// 4- or 8-neighbour pixel grid. Input: LAB float4 image (its fourth channel is
+// the pixel weight). Output: the image segmentation pyramid in the reference's
+// ISP layout (segment.cu:884-905): per level l, num_clus N_l and num_bd E_l
+// (level_sizes[2l], [2l+1]); clus (N_l ints: node -> parent), mean (6 x N_l
+// floats, channel-major: sums of L, a, b, x, y and the weight), bd (E_l int
+// pairs), bdl (E_l ints), concatenated over levels. Capacities: clus 2*HW,
+// mean 12*HW, bd 4*num_nb*HW ints, bdl 2*num_nb*HW. Returns the number of
+// levels.
 //
 // Child sums are added in increasing child index starting from 0.0f (the
 // reference adds them with float atomics in an unspecified order,
 // segment.cu:472-486).
-int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_sizes, int *clus_out,
-                float *mean_out, int *bd_out, int *bdl_out)
+int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int max_levels, int *level_sizes,
+                    int *clus_out, float *mean_out, int *bd_out, int *bdl_out)
 {
+    if (link < 0 || link > 3 || (num_nb != 4 && num_nb != 8))
+        return -1;
+    const bool use_mean = link == 2 || link == 3; // segment.hpp:248
     const int N0 = W * H;
-    std::vector<int> nn(N0), bd(8 * (size_t)N0), bdl(4 * (size_t)N0, 1);
-    std::vector<float> dist_min(N0), sums(6 * (size_t)N0);
-    orc_nn_grid(lab4, W, H, nn.data(), dist_min.data(), bd.data());
+    std::vector<int> nn(N0), bd(2 * (size_t)num_nb * N0), bdl((size_t)num_nb * N0, 1);
+    std::vector<float> dist_min(N0), sums(6 * (size_t)N0), edist((size_t)num_nb * N0);
+    orc_nn_grid_nb(lab4, W, H, num_nb, nn.data(), dist_min.data(), bd.data(), edist.data());
     for (int i = 0; i < N0; ++i)
     {
         sums[i] = lab4[4 * (size_t)i];
@@ -278,7 +283,7 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
         sums[4 * (size_t)N0 + i] = (float)(i / W);
         sums[5 * (size_t)N0 + i] = lab4[4 * (size_t)i + 3];
     }
-    int num = N0, E = 4 * N0, levels = 0;
+    int num = N0, E = num_nb * N0, levels = 0;
     size_t oc = 0, ob = 0;
     std::vector<int> clus;
     for (;;)
@@ -302,25 +307,34 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
             break;
 
         // reduce_boundary_dist (segment.cu:1050-1091): map edges to parents,
-        // sort the (s, t) pairs alone, keep the last of each run unless it is
-        // a self-loop; boundary lengths are summed by POSITION in the sorted
-        // order (the bdl array is not permuted with the pairs, :1061, :368-386).
-        std::vector<uint64_t> key(E);
+        // sort the (s, t) pairs, keep the last of each run unless it is a
+        // self-loop; boundary lengths are summed by POSITION in the sorted
+        // order (the bdl array is not permuted with the pairs, :1061,
+        // :368-386). Min / Max linkage carry each edge's distance through the
+        // sort and reduce each run with min / max (reduce_dist, :336-366),
+        // which no order changes.
+        std::vector<std::pair<uint64_t, float>> key(E);
         for (int e = 0; e < E; ++e)
         {
             uint32_t s = (uint32_t)clus[bd[2 * (size_t)e]], t = (uint32_t)clus[bd[2 * (size_t)e + 1]];
-            key[e] = ((uint64_t)s << 32) | t;
+            key[e] = {((uint64_t)s << 32) | t, edist[e]};
         }
-        std::sort(key.begin(), key.end());
+        std::sort(key.begin(), key.end(),
+                  [](const std::pair<uint64_t, float> &a, const std::pair<uint64_t, float> &b) { return a.first < b.first; });
         std::vector<int> bd2, bdl2;
+        std::vector<float> edist2;
         bd2.reserve(2 * (size_t)E);
         int run_sum = 0;
+        float run_d = link == 0 ? FLT_MAX : 0.0f;
         for (int e = 0; e < E; ++e)
         {
-            uint32_t s = (uint32_t)(key[e] >> 32), t = (uint32_t)key[e];
+            uint32_t s = (uint32_t)(key[e].first >> 32), t = (uint32_t)key[e].first;
             if (s != t)
+            {
                 run_sum += bdl[e];
-            bool last = (e == E - 1) || key[e + 1] != key[e];
+                run_d = link == 0 ? std::min(run_d, key[e].second) : std::max(run_d, key[e].second);
+            }
+            bool last = (e == E - 1) || key[e + 1].first != key[e].first;
             if (last)
             {
                 if (s != t)
@@ -328,8 +342,10 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
                     bd2.push_back((int)s);
                     bd2.push_back((int)t);
                     bdl2.push_back(run_sum);
+                    edist2.push_back(run_d);
                 }
                 run_sum = 0;
+                run_d = link == 0 ? FLT_MAX : 0.0f;
             }
         }
         int E2 = (int)bdl2.size();
@@ -338,7 +354,8 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
         std::vector<float> dmax(num_new, 0.0f);
         for (int c = 0; c < num; ++c)
             dmax[clus[c]] = std::max(dmax[clus[c]], dist_min[c]);
-        // reduce_data_mean (segment.cu:1134-1153): child sums in child order
+        // reduce_data_mean (segment.cu:1134-1153): child sums in child order;
+        // means of channels 0-4, the weight sum stays (sum_to_mean, :492-503)
         std::vector<float> sums2(6 * (size_t)num_new, 0.0f);
         for (int ch = 0; ch < 6; ++ch)
             for (int c = 0; c < num; ++c)
@@ -347,30 +364,41 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
         for (int ch = 0; ch < 5; ++ch)
             for (int p = 0; p < num_new; ++p)
                 mean2[(size_t)ch * num_new + p] = sums2[(size_t)ch * num_new + p] / sums2[5 * (size_t)num_new + p];
-        // compute_dist_mean_k + pernalize_dist_k + compute_1nn
-        // (segment.cu:508-534, :582-612, :1211-1231, :403-422); the centroid
-        // distance is fused the way the reference's device code fuses it.
-        std::vector<float> dist(E2);
+        // compute_dist_mean_k (+ ward_weight, :559-577) or the reduced
+        // distance, then pernalize_dist_k and compute_1nn (segment.cu:508-534,
+        // :582-612, :1211-1231, :403-422); the centroid distance is fused the
+        // way the reference's device code fuses it.
         std::vector<float> dmin2(num_new, FLT_MAX);
         for (int e = 0; e < E2; ++e)
         {
             int s = bd2[2 * (size_t)e], t = bd2[2 * (size_t)e + 1];
-            float e0 = mean2[s] - mean2[t];
-            float e1 = mean2[(size_t)num_new + s] - mean2[(size_t)num_new + t];
-            float e2 = mean2[2 * (size_t)num_new + s] - mean2[2 * (size_t)num_new + t];
-            float h = e0 > 0.f ? e0 : 0.f;
-            float d = std::fma(e2, e2, std::fma(e1, e1, std::fma(e0, e0, h)));
+            float d;
+            if (use_mean)
+            {
+                float e0 = mean2[s] - mean2[t];
+                float e1 = mean2[(size_t)num_new + s] - mean2[(size_t)num_new + t];
+                float e2 = mean2[2 * (size_t)num_new + s] - mean2[2 * (size_t)num_new + t];
+                float h = e0 > 0.f ? e0 : 0.f;
+                d = std::fma(e2, e2, std::fma(e1, e1, std::fma(e0, e0, h)));
+                if (link == 3)
+                {
+                    const float sw = sums2[5 * (size_t)num_new + s], tw = sums2[5 * (size_t)num_new + t];
+                    d = sw * tw / (sw + tw) * d;
+                }
+            }
+            else
+                d = edist2[e];
             float delta = d - dmax[t];
             if (delta > 0)
                 d += delta;
-            dist[e] = d;
+            edist2[e] = d;
             dmin2[s] = std::min(dmin2[s], d);
         }
         std::vector<int> nn2(num_new, 0);
         for (int e = 0; e < E2; ++e)
         {
             int s = bd2[2 * (size_t)e], t = bd2[2 * (size_t)e + 1];
-            if (dist[e] == dmin2[s])
+            if (edist2[e] == dmin2[s])
                 nn2[s] = std::max(nn2[s], t);
         }
         num = num_new;
@@ -380,8 +408,17 @@ int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_size
         sums.swap(sums2);
         bd.swap(bd2);
         bdl.swap(bdl2);
+        edist.swap(edist2);
     }
     return levels;
+}
+
+// SegHAC::run_ms with CentroidLink and the 4-neighbour grid (the path's
+// configuration); see orc_segment_cfg.
+int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_sizes, int *clus_out,
+                float *mean_out, int *bd_out, int *bdl_out)
+{
+    return orc_segment_cfg(lab4, W, H, 2, 4, max_levels, level_sizes, clus_out, mean_out, bd_out, bdl_out);
 }
 
 } // extern "C"

@@ -38,6 +38,8 @@ def lib():
         _lib.orc_crtrees.restype = C.c_int
         _lib.orc_crtrees_literal.restype = C.c_int
         _lib.orc_segment.restype = C.c_int
+        _lib.orc_segment_cfg.restype = C.c_int
+        _lib.orc_lab_sigma.argtypes = [P, C.c_int, C.c_int, C.c_double, P]
         _lib.orc_hbp.restype = C.c_int
         _lib.orc_hbp.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
                                  C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
@@ -120,16 +122,28 @@ def crtrees(nn: np.ndarray, literal: bool = False):
     return out, n
 
 
-def segment(lab4: np.ndarray) -> dict:
+def lab_sigma(bgr: np.ndarray, sigma: float) -> np.ndarray:
+    """LAB of the image blurred with sigma (SegHAC::img_CPU_to_GPU)."""
+    bgr = np.ascontiguousarray(bgr, np.uint8)
+    H, W = bgr.shape[:2]
+    out = np.zeros((H, W, 4), np.float32)
+    lib().orc_lab_sigma(_p(bgr), W, H, float(sigma), _p(out))
+    return out
+
+
+def segment(lab4: np.ndarray, link: int = 2, num_nb: int = 4) -> dict:
+    """SegHAC pyramid of a LAB image; link 0 Min, 1 Max, 2 Centroid, 3 Ward."""
     lab4 = np.ascontiguousarray(lab4, np.float32)
     H, W = lab4.shape[:2]
     n = H * W
     sizes = np.zeros(2 * 64, np.int32)
     clus = np.zeros(2 * n, np.int32)
     mean = np.zeros(12 * n, np.float32)
-    bd = np.zeros(16 * n, np.int32)
-    bdl = np.zeros(8 * n, np.int32)
-    L = lib().orc_segment(_p(lab4), W, H, 64, _p(sizes), _p(clus), _p(mean), _p(bd), _p(bdl))
+    bd = np.zeros(4 * num_nb * n, np.int32)
+    bdl = np.zeros(2 * num_nb * n, np.int32)
+    L = lib().orc_segment_cfg(_p(lab4), W, H, link, num_nb, 64, _p(sizes), _p(clus), _p(mean), _p(bd), _p(bdl))
+    if L < 1:
+        raise ValueError("orc_segment_cfg rejected its input")
     sizes = sizes[: 2 * L].reshape(L, 2)
     tc, tb = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
     return dict(level_sizes=sizes, clus=clus[:tc], mean=mean[: 6 * tc], bd=bd[: 2 * tb].reshape(tb, 2), bdl=bdl[:tb])
@@ -299,15 +313,20 @@ def pipeline_f32(L, src, tau=0.5, alpha=1.3, tau_smooth=0.6, min_level=2, R=None
 
 
 def pipeline(L, R, D, alpha=1000.1, tau_smooth=0.6, min_level=2, fp64=False, right_view=False,
-             fp16_msg=False):
+             fp16_msg=False, link=2, num_nb=4, sigma=0.0, lab_image=None):
     """The single-pair path of main_stereo_hbp_isp.cu:33-72 (without the driver
-    median); right_view selects the right-view path of main_bench_middv3.cu:189-203."""
+    median); right_view selects the right-view path of main_bench_middv3.cu:189-203.
+    link / num_nb / sigma: the SegHAC configuration; lab_image replaces the
+    oracle's LAB of the segmented view (e.g. the engine's blurred LAB)."""
     H, W = L.shape[:2]
     cs = cost_stage(L, R, D)
     vol, wta = cs["vol"], cs["wta"]
     if right_view:
         vol, wta = cost_to_right(vol, W, H, D)
-    seg = segment(lab(R if right_view else L))
+    img = R if right_view else L
+    if lab_image is None:
+        lab_image = lab(img) if sigma == 0 else lab_sigma(img, sigma)
+    seg = segment(lab_image, link, num_nb)
     disp, plane, steps, _, _ = hbp(seg, vol, wta, W, H, D, alpha, tau_smooth, min_level, fp64,
                                    fp16_msg=fp16_msg)
     return dict(disp=disp, plane=plane, steps=steps, seg=seg, wta=wta, vol=vol)

@@ -24,6 +24,7 @@ __global__ void img_BGR_to_grey(const uchar3 *, float *, const int, const int);
 __global__ void img_float1_to_uchar1(const float *, uint8_t *, const int, const int);
 __global__ void img_uchar3_to_float4(const uchar3 *, float4 *, const int, const int);
 __global__ void img_BGR_to_LAB(float4 *, const int, const int);
+void img_gauss_blur(float4 *&, float4 *&, float *const, const double, const int, const int);
 __global__ void compute_1nn_grid_k(const float4 *, int *, int2 *, float *, float *, const int,
                                    const int, const int);
 
@@ -109,6 +110,71 @@ int ref_lab(const uint8_t *bgr, int W, int H, float *lab4)
     cudaFree(in_d);
     cudaFree(f_d);
     return rc;
+}
+
+// SegHAC::img_CPU_to_GPU (segment.cu:795-809) with sigma: the float4 BGR
+// image, the Gaussian blur img_gauss_blur (imutil.cu:397-497) when
+// sigma > FLT_MIN, then BGR -> LAB.
+int ref_lab_sigma(const uint8_t *bgr, int W, int H, double sigma, float *lab4)
+{
+    size_t n = (size_t)W * H;
+    uchar3 *in_d;
+    float4 *f_d, *buf_d;
+    float *filter_d;
+    cudaMalloc(&in_d, n * 3);
+    cudaMalloc(&f_d, n * 16);
+    cudaMalloc(&buf_d, n * 16);
+    cudaMalloc(&filter_d, sizeof(float) * 64 * 64);
+    cudaMemcpy(in_d, bgr, n * 3, cudaMemcpyHostToDevice);
+    dim3 blk(32, 2), grd((W + 31) / 32, (H + 1) / 2);
+    img_uchar3_to_float4<<<grd, blk>>>(in_d, f_d, W, H);
+    float4 *img = f_d, *buf = buf_d;
+    if (sigma > FLT_MIN)
+        img_gauss_blur(img, buf, filter_d, sigma, W, H);
+    img_BGR_to_LAB<<<grd, blk>>>(img, W, H);
+    int rc = last_error();
+    d2h(lab4, (const float *)img, n * 4);
+    cudaFree(in_d);
+    cudaFree(f_d);
+    cudaFree(buf_d);
+    cudaFree(filter_d);
+    return rc;
+}
+
+// SegHAC(link, num_nb, sigma, LabelISPFormat, 1).run_ms() (segment.cu:
+// 1279-1321), outputs as ref_segment (bd capacity 2 * num_nb * HW pairs,
+// bdl num_nb * 2 * HW). Returns the number of levels.
+int ref_segment_cfg(const uint8_t *bgr, int W, int H, int link, int num_nb, double sigma, int max_levels,
+                    int *level_sizes, int *clus, float *mean, int *bd, int *bdl)
+{
+    int levels = 0;
+    int rc;
+    {
+        SegHAC seg(wrap_bgr(bgr, W, H), (Linkage)link, num_nb, sigma, LabelISPFormat, 1, false);
+        seg.run_ms();
+        rc = last_error();
+        std::vector<int> nc = seg.g_num_clus_isp(), nb = seg.g_num_bd_isp();
+        levels = (int)nc.size();
+        size_t tc = 0, tb = 0;
+        for (int i = 0; i < levels; ++i)
+        {
+            if (i < max_levels)
+            {
+                level_sizes[2 * i] = nc[i];
+                level_sizes[2 * i + 1] = nb[i];
+            }
+            tc += nc[i];
+            tb += nb[i];
+        }
+        d2h(clus, seg.g_isp_clus_d(), tc);
+        d2h(mean, seg.g_isp_mean_d(), tc * 6);
+        d2h(bd, (const int *)seg.g_isp_bd_d(), tb * 2);
+        d2h(bdl, seg.g_isp_bdl_d(), tb);
+    }
+    int rc2 = last_error();
+    if (rc || rc2)
+        return rc ? rc : rc2;
+    return levels;
 }
 
 // Pixel 1-NN on the 4-grid (segment.cu:57-195): nn, dist_min and the four

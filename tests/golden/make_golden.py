@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad]
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -38,10 +38,14 @@ class RefLib:
         path = path or os.path.join(ROOT, "oracle", "_ref", "libhbpref.so")
         self.lib = C.CDLL(path)
         for name in ("ref_grey", "ref_lab", "ref_1nn_grid", "ref_crtrees", "ref_cost",
-                     "ref_segment", "ref_hbp_pair", "ref_post", "ref_hbp_f32", "ref_hbp_ad"):
+                     "ref_segment", "ref_hbp_pair", "ref_post", "ref_hbp_f32", "ref_hbp_ad", "ref_lab_sigma",
+                     "ref_segment_cfg"):
             getattr(self.lib, name).restype = C.c_int
         self.lib.ref_hbp_pair.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_int, C.c_int, P, P]
+        self.lib.ref_lab_sigma.argtypes = [P, C.c_int, C.c_int, C.c_double, P]
+        self.lib.ref_segment_cfg.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, P, P, P,
+                                             P, P]
         self.lib.ref_hbp_ad.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int,
                                         P, P, P, P, P, P]
         self.lib.ref_hbp_f32.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
@@ -138,6 +142,29 @@ class RefLib:
         assert levels > 0, levels
         out["levels"] = levels
         return out
+
+    def lab_sigma(self, bgr, sigma):
+        H, W, _ = bgr.shape
+        out = np.zeros((H, W, 4), np.float32)
+        rc = self.lib.ref_lab_sigma(ptr(bgr), W, H, sigma, ptr(out))
+        assert rc == 0, rc
+        return out
+
+    def segment_cfg(self, bgr, link, num_nb, sigma):
+        H, W, _ = bgr.shape
+        n = H * W
+        sizes = np.zeros(2 * 64, np.int32)
+        clus = np.zeros(2 * n, np.int32)
+        mean = np.zeros(12 * n, np.float32)
+        bd = np.zeros(4 * num_nb * n, np.int32)
+        bdl = np.zeros(2 * num_nb * n, np.int32)
+        L = self.lib.ref_segment_cfg(ptr(bgr), W, H, link, num_nb, sigma, 64, ptr(sizes), ptr(clus), ptr(mean),
+                                     ptr(bd), ptr(bdl))
+        assert L > 0, L
+        sizes = sizes[: 2 * L].reshape(L, 2)
+        tc, tb = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
+        return dict(level_sizes=sizes, clus=clus[:tc], mean=mean[: 6 * tc], bd=bd[: 2 * tb].reshape(tb, 2),
+                    bdl=bdl[:tb])
 
     def post(self, L, R, dispL, planeL, dispR, planeR, median=True):
         H, W, _ = L.shape
@@ -265,11 +292,30 @@ def ad_record(ref: RefLib, W, H, D, seed):
                 levels=a["levels"], levels_right=b["levels"])
 
 
+# (linkage, num_nb, sigma) of the segmentation variants; 0 Min, 1 Max,
+# 2 Centroid, 3 Ward (segment.hpp:8-16)
+SEG_CFGS = [(0, 4, 0.0), (1, 4, 0.0), (3, 4, 0.0), (2, 8, 0.0), (0, 8, 0.0), (2, 4, 1.0), (3, 8, 0.7)]
+
+
+def seg_record(ref: RefLib, W, H, seed):
+    """The segmentation variants on one seeded scene: every configuration's
+    pyramid (full arrays) and the blurred LAB images."""
+    s = make_scene(W, H, 32, seed)
+    rec = dict(W=W, H=H, seed=seed, left=s.left, cfgs=np.array(SEG_CFGS, np.float64))
+    for i, (link, nb, sigma) in enumerate(SEG_CFGS):
+        seg = ref.segment_cfg(s.left, link, nb, sigma)
+        for k, v in seg.items():
+            rec[f"c{i}_{k}"] = v
+    for sigma in sorted({c[2] for c in SEG_CFGS if c[2] > 0}):
+        rec[f"lab_sigma_{sigma:g}"] = ref.lab_sigma(s.left, sigma)
+    return rec
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
-    ap.add_argument("--only", choices=["census", "mccnn", "ad"], default=None)
+    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     ref = RefLib(args.lib)
@@ -284,7 +330,13 @@ def main():
             rec = ad_record(ref, W, H, D, seed)
             np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
             print(name, "levels", rec["levels"])
-    if args.only in ("mccnn", "ad"):
+    if args.only in (None, "seg"):
+        # sizes a multiple of 16: the reference's blur races at a ragged edge
+        for (W, H, seed, name) in [(96, 64, 7, "seg_96x64_s7"), (160, 112, 11, "seg_160x112_s11")]:
+            rec = seg_record(ref, W, H, seed)
+            np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
+            print(name, [int(rec[f"c{i}_level_sizes"].shape[0]) for i in range(len(SEG_CFGS))])
+    if args.only in ("mccnn", "ad", "seg"):
         return
 
     for (W, H, D, seed, full, name) in [

@@ -1,0 +1,81 @@
+"""The reference's other SegHAC configurations (segment.hpp:8-16, :248):
+Min / Max / Ward linkage, the 8-neighbour grid and the Gaussian pre-blur.
+The engine's pyramid equals the oracle's bit for bit on the same LAB image;
+the blurred LAB image equals the reference build's (golden fixtures); a whole
+pair with a variant configuration equals the oracle's pipeline. Requires a
+GPU."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CFGS = [(0, 4, 0.0), (1, 4, 0.0), (3, 4, 0.0), (2, 8, 0.0), (0, 8, 0.0), (2, 4, 1.0), (3, 8, 0.7)]
+
+
+@pytest.fixture(scope="module")
+def eng():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import hbp_b200 as E
+    ctx = E.Context(0)
+    yield E, ctx, torch
+    ctx.close()
+
+
+def _lab(E, ctx, torch, img, sigma):
+    H, W = img.shape[:2]
+    out = torch.zeros(H * W * 4, device="cuda")
+    ctx.lab_sigma_d(torch.from_numpy(np.ascontiguousarray(img)).cuda(), W, H, sigma, out)
+    return out.cpu().numpy().reshape(H, W, 4)
+
+
+@pytest.mark.parametrize("name", ["seg_96x64_s7", "seg_160x112_s11"])
+def test_blurred_lab_matches_reference(eng, golden_dir, name):
+    E, ctx, torch = eng
+    z = dict(np.load(os.path.join(golden_dir, name + ".npz")))
+    for key in [k for k in z if k.startswith("lab_sigma_")]:
+        sigma = float(key[len("lab_sigma_"):])
+        got = _lab(E, ctx, torch, z["left"], sigma)
+        assert np.array_equal(got.view(np.uint32), z[key].view(np.uint32)), (key, float(np.mean(got != z[key])))
+
+
+@pytest.mark.parametrize("cfg", CFGS)
+def test_pyramid_variants_bit_exact(eng, golden_dir, cfg):
+    """Every ISP array of every level equals the oracle's on the engine's LAB
+    image; labels, edges and lengths also equal the reference build's."""
+    import pyoracle as O
+    E, ctx, torch = eng
+    link, nb, sigma = cfg
+    z = dict(np.load(os.path.join(golden_dir, "seg_160x112_s11.npz")))
+    i = [tuple(c) for c in z["cfgs"].tolist()].index((float(link), float(nb), float(sigma)))
+    L = z["left"]
+    H, W = L.shape[:2]
+    ctx.segment_cfg_d(torch.from_numpy(np.ascontiguousarray(L)).cuda(), W, H, link, nb, sigma)
+    g = ctx.pyramid()
+    o = O.segment(_lab(E, ctx, torch, L, sigma), link, nb)
+    assert np.array_equal(g["level_sizes"], o["level_sizes"])
+    for k in ("clus", "bd", "bdl"):
+        assert np.array_equal(g[k], o[k]), k
+    assert np.array_equal(g["mean"].view(np.uint32), o["mean"].view(np.uint32))
+    assert np.array_equal(g["level_sizes"], z[f"c{i}_level_sizes"])
+    for k in ("clus", "bd", "bdl"):
+        assert np.array_equal(g[k], z[f"c{i}_{k}"]), k
+
+
+@pytest.mark.parametrize("cfg", [(0, 8, 0.0), (3, 4, 0.7)])
+def test_pair_with_variant_segmentation(eng, cfg):
+    """hbp_run_pair with the configuration in hbp_params equals the oracle's
+    pipeline (driver median included) bit for bit."""
+    import pyoracle as O
+    from scenes import make_scene
+    E, ctx, torch = eng
+    link, nb, sigma = cfg
+    s = make_scene(160, 112, 48, 5)
+    prm = E.default_params(post=1, linkage=link, num_nb=nb, sigma=sigma)
+    got = ctx.run_pair(s.left, s.right, 48, prm)
+    lab = _lab(E, ctx, torch, s.left, sigma)
+    ref = O.driver_median(O.pipeline(s.left, s.right, 48, link=link, num_nb=nb, lab_image=lab)["disp"])
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), float(np.mean(got != ref))

@@ -246,3 +246,26 @@ def test_levels_end_with_the_ordinary_result():
     assert np.array_equal(d[-1].view(np.uint32), od.view(np.uint32))
     assert np.array_equal(p[-1].view(np.uint32), op.view(np.uint32))
     assert not d[0].any() and not p[0].any()
+
+
+@pytest.mark.parametrize("name", ["seg_96x64_s7", "seg_160x112_s11"])
+def test_seg_variants_match_reference(golden_dir, name):
+    """The reference's other SegHAC configurations (Min / Max / Ward linkage,
+    8 neighbours, pre-blur): labels, edges and boundary lengths agree with the
+    reference build at every level; node sums to float rounding (the
+    reference adds them with float atomics; with the blur's fractional pixel
+    weights the sums round more, hence 5e-5 relative). The blurred LAB images
+    agree bit for bit; the pyramid starts from the reference's own LAB image."""
+    z = load(golden_dir, name)
+    L = z["left"]
+    for key in [k for k in z if k.startswith("lab_sigma_")]:
+        sigma = float(key[len("lab_sigma_"):])
+        assert np.array_equal(O.lab_sigma(L, sigma).view(np.uint32), z[key].view(np.uint32)), key
+    for i, (link, nb, sigma) in enumerate(z["cfgs"].tolist()):
+        lab = O.lab(L) if sigma == 0 else z[f"lab_sigma_{sigma:g}"]
+        seg = O.segment(lab, int(link), int(nb))
+        assert np.array_equal(seg["level_sizes"], z[f"c{i}_level_sizes"]), (i, link, nb, sigma)
+        for k in ("clus", "bd", "bdl"):
+            assert np.array_equal(seg[k], z[f"c{i}_{k}"]), (i, k)
+        m, r = seg["mean"], z[f"c{i}_mean"]
+        assert np.max(np.abs(m - r) / np.maximum(1.0, np.abs(r))) < 5e-5, i
