@@ -81,6 +81,10 @@ __device__ __forceinline__ float byte_to_float(uint32_t v)
 // read_plane_cost (hbp_isp.cu:205-227) for one pixel (xf, yf = its
 // coordinates as floats, base = vol_tile_base) and one plane. For d in
 // [0, D-1), (float)(d + 1) == (float)d + 1 exactly.
+// F32: the float volume of the MC-CNN / AD paths (c.volf), else the uint8
+// Census volume (c.vol); a template parameter, so the Census loop carries no
+// branch on the volume's type.
+template <bool F32>
 __device__ __forceinline__ float pixel_cost(const Common &c, float xf, float yf, size_t base, float4 pl)
 {
     float d_f = __fmaf_rn(pl.x, xf, __fmaf_rn(pl.y, yf, pl.z));
@@ -91,7 +95,7 @@ __device__ __forceinline__ float pixel_cost(const Common &c, float xf, float yf,
     else
     {
         float v0, v1;
-        if (c.volf)
+        if constexpr (F32)
         {
             const float *pv = c.volf + base + (size_t)d * VT_BYTES;
             v0 = pv[0];
@@ -765,12 +769,9 @@ __device__ __forceinline__ void emit_chunk(const LevelDev &l, float4 *pc, int n,
     pc[l.chunk_off[n] + win - l.pix_off[n] / PC_CHUNK] = v;
 }
 
-__global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
+template <bool F32>
+__device__ __forceinline__ void cost_window(const StepDesc &d, int mode, int item, int lane)
 {
-    const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (item >= d.pre[d.nt]) // warp-uniform
-        return;
     const int ti = find_task(d, item);
     const Task &t = d.t[ti];
     const ViewDev &v = *t.vd;
@@ -822,7 +823,7 @@ __global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, 
 #pragma unroll
                 for (int p = 0; p < 4; ++p)
                 {
-                    const float cv = pixel_cost(c, xf, yf, base, pl[p]);
+                    const float cv = pixel_cost<F32>(c, xf, yf, base, pl[p]);
                     a[p] = k == 0 ? cv : a[p] + cv;
                 }
             }
@@ -897,7 +898,7 @@ __global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, 
             const size_t base = vol_tile_base(x, y, c.TX, c.D);
 #pragma unroll
             for (int p = 0; p < 4; ++p)
-                cc[p] = pixel_cost(c, xf, yf, base, pl[p]);
+                cc[p] = pixel_cost<F32>(c, xf, yf, base, pl[p]);
         }
         // S1
 #pragma unroll
@@ -928,6 +929,18 @@ __global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, 
     }
     if (lane == 0 && carry_n >= 0 && carry_n < N)
         emit_chunk(l, pc, carry_n, win, carry);
+}
+
+__global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
+{
+    const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (item >= d.pre[d.nt]) // warp-uniform
+        return;
+    if (d.t[find_task(d, item)].vd->c.volf) // uniform per view
+        cost_window<true>(d, mode, item, lane);
+    else
+        cost_window<false>(d, mode, item, lane);
 }
 
 // init_bp, continued: costs of the prior slots, belief = cost, child seeds.

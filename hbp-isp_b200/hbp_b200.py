@@ -79,7 +79,12 @@ def _p(a):
         return None
     if isinstance(a, np.ndarray):
         return a.ctypes.data_as(P)
-    return P(a.data_ptr())  # torch tensor on the device
+    # a torch tensor on the device: the engine runs on its own non-blocking
+    # stream, so torch's pending work on the tensor (a fill, a copy) must
+    # finish first
+    import torch
+    torch.cuda.current_stream(a.device).synchronize()
+    return P(a.data_ptr())
 
 
 def default_params(**kw) -> Params:
