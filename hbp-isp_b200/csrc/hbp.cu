@@ -780,15 +780,27 @@ __device__ __forceinline__ void cost_window(const StepDesc &d, int mode, int ite
     const int HW = c.W * c.H, N = l.N;
     const int win = item - d.pre[ti];
     float4 *pc = v.b.pc[t.pb];
-    // S0: a window that one node fills entirely
+    // S0: a window that one node fills entirely. The window's list entries and
+    // (for a step) the node's candidate planes are loaded before the test, so
+    // that their latency overlaps the node-range loads.
     if ((win + 1) * PC_CHUNK <= HW)
     {
         const int q0 = win * PC_CHUNK;
+        uint32_t xy[PC_CHUNK / 32];
+#pragma unroll
+        for (int k = 0; k < PC_CHUNK / 32; ++k)
+            xy[k] = l.pix[q0 + lane + 32 * k];
         const int n0 = l.pnode[q0];
+        float4 pl[4];
+        if (mode != COST_INIT)
+        {
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                pl[p] = l.plane[(size_t)n0 * K + 2 * P + p];
+        }
         const int b0 = l.pix_off[n0];
         if (b0 <= q0 && l.pix_off[n0 + 1] >= q0 + PC_CHUNK) // warp-uniform
         {
-            float4 pl[4];
             if (mode == COST_INIT)
             {
                 const int pn = l.clus[n0];
@@ -803,16 +815,6 @@ __device__ __forceinline__ void cost_window(const StepDesc &d, int mode, int ite
                     v.b.s_ransac[t.rb][n0] = (uint32_t)q0;
                 }
             }
-            else
-            {
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-                    pl[p] = l.plane[(size_t)n0 * K + 2 * P + p];
-            }
-            uint32_t xy[PC_CHUNK / 32];
-#pragma unroll
-            for (int k = 0; k < PC_CHUNK / 32; ++k)
-                xy[k] = l.pix[q0 + lane + 32 * k];
             float a[4];
 #pragma unroll
             for (int k = 0; k < PC_CHUNK / 32; ++k)
