@@ -63,10 +63,12 @@ def parse():
     ap.add_argument("--fp16", type=int, default=1, help="store BP messages as FP16 (1) or FP32 (0)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="batch", choices=["batch", "uneven", "precision", "serve"],
+    ap.add_argument("--config", default="batch", choices=["batch", "uneven", "precision", "serve", "mccnn"],
                     help="batch: the contract line (16 pairs 720x496 D128); uneven: 32 pairs of mixed "
                          "sizes and disparity ranges in flight together; precision: 8 pairs 1440x992 D256, "
-                         "FP16 vs FP32 messages; serve: Poisson arrivals of a size mix")
+                         "FP16 vs FP32 messages; serve: Poisson arrivals of a size mix; mccnn: the "
+                         "reference's published benchmark flow (MC-CNN volume, one view, runtime against "
+                         "min_level) at a Middlebury half-resolution size")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
     ap.add_argument("--profile-run", action="store_true",
@@ -258,6 +260,72 @@ def run_reference(args, rank):
     print(json.dumps(out))
 
 
+# runtime.png of the reference (README.md:17-18): Adirondack at trainingH, seconds per view
+# on a Titan Xp for min_level 9, 8, ..., 1 (read from the plot, about +-0.03 s)
+PUBLISHED_ADIRONDACK_S = {9: 0.42, 8: 0.80, 7: 1.18, 6: 1.61, 5: 2.00, 4: 2.42, 3: 3.05, 2: 4.12, 1: 5.36}
+
+
+def run_mccnn(args, E, torch, local, bad):
+    """The flow the reference publishes runtimes for (main_bench_middv3.cu:73-108 with
+    cost "MC-CNN", bench_MiddV3_train.sh: alpha 1.3, tau_smooth 0.6): SegHAC on the left
+    image, the MC-CNN volume, HBP_ISP::run_ms(min_level), for min_level 9 down to 1. The
+    scene and its float volume are synthetic stand-ins (1440x992, D 144, Adirondack's
+    half-resolution size; the volume is the 5x5 mean of the grey difference / 48 plus noise,
+    built on the device). Each time is the median of 3 runs of segmentation + volume ingest +
+    HBP, device-resident inputs."""
+    from scenes import make_scene
+    W, H, D = 1440, 992, 144
+    s = make_scene(W, H, D, 8000)
+    w = torch.tensor([0.114, 0.587, 0.299], device="cuda")
+    gl = torch.from_numpy(s.left).cuda().float() @ w
+    gr = torch.from_numpy(s.right).cuda().float() @ w
+    xs = torch.arange(W, device="cuda")
+    src = torch.empty((D, H, W), device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(8001)
+    for d in range(D):
+        diff = (gl - gr[:, (xs - d).clamp(min=0)]).abs()[None, None]
+        src[d] = torch.nn.functional.avg_pool2d(diff, 5, 1, 2, count_include_pad=False)[0, 0] / 48.0
+    src += 0.02 * torch.randn(src.shape, device="cuda", generator=gen)
+    src.clamp_(0.0, 1.0)
+    torch.cuda.synchronize()
+    ctx = E.Context(local, W * H, D)
+    vol = torch.empty(E.volume_f32_bytes(W, H, D) // 4, device="cuda")
+    wta = torch.empty(H * W, device="cuda")
+    disp = torch.empty(H * W, device="cuda")
+    dl = torch.from_numpy(s.left).cuda()
+    out = {}
+    try:
+        L = ctx.segment_d(dl, W, H)
+        for m in sorted(PUBLISHED_ADIRONDACK_S, reverse=True):
+            if m > L - 1:
+                continue
+            row = {}
+            for name, f16 in (("fp32", 0), ("fp16", 1)):
+                prm = E.default_params(alpha=1.3, min_level=m, msg_fp16=f16, post=0)
+                ts = []
+                for rep in range(4):
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    ctx.segment_d(dl, W, H)
+                    ctx.cost_f32_d(src, W, H, D, 0.5, vol, wta)
+                    ctx.infer_f32_d(vol, wta, D, 0.5, prm, disp)
+                    torch.cuda.synchronize()
+                    if rep:
+                        ts.append((time.perf_counter() - t0) * 1e3)
+                d = disp.cpu().numpy().reshape(H, W)
+                row[name] = {"ms": sorted(ts)[1], "bad2_pct": bad(d, s, 2.0)}
+            row["published_titan_xp_ms"] = PUBLISHED_ADIRONDACK_S[m] * 1e3
+            row["speedup_fp32_vs_published"] = row["published_titan_xp_ms"] / row["fp32"]["ms"]
+            out[str(m)] = row
+    finally:
+        ctx.close()
+    return {"config": "mccnn", "workload": f"1 synthetic view {W}x{H} D{D} with a synthetic MC-CNN-like "
+                                           "float volume; segmentation + ingest + HBP per min_level",
+            "levels": L, "by_min_level": out,
+            "published": "runtime.png (README.md:17-18), Adirondack trainingH, Titan Xp; not the same "
+                         "image: a size-matched comparison, not a like-for-like one"}
+
+
 def run_config(args, E, torch):
     """The other workloads (one JSON line each, not the contract line)."""
     from scenes import make_scene
@@ -319,6 +387,8 @@ def run_config(args, E, torch):
                                                    "hbp_run_batch_d", "fp32": res["fp32"], "fp16": res["fp16"],
                 "fp16_vs_fp32_identical_mean": float(np.mean(same)),
                 "fp16_vs_fp32_identical_min": float(np.min(same))}
+    if args.config == "mccnn":
+        return run_mccnn(args, E, torch, local, bad)
     # serve: Poisson arrivals of the size mix, FP16 messages, 120 GB budget
     rng = np.random.default_rng(11)
     mix = [((450, 375, 64), 0.4), ((720, 496, 128), 0.3), ((1440, 992, 256), 0.2), ((2880, 1984, 384), 0.1)]
