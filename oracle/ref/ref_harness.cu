@@ -7,6 +7,7 @@
 // Every entry point takes host buffers, returns 0 on success and a negative
 // code on a CUDA error, and runs synchronously on the legacy default stream
 // exactly as the reference drivers do (main_stereo_hbp_isp.cu:31-76).
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -369,6 +370,12 @@ int ref_post(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, float *disp
 // right view of main_bench_middv3.cu:189-203 instead (SegHAC on the right
 // image, cost_to_right). vol_f32 ([D][HW]) and wta receive the stored volume
 // and WTA (optional). Returns the number of levels.
+static double g_last_hbp_ms = 0.0;
+
+// Milliseconds of the last ref_hbp_f32's HBP_ISP construction + run_ms, the
+// scope main_bench_middv3.cu:97-104 times.
+double ref_last_hbp_ms() { return g_last_hbp_ms; }
+
 int ref_hbp_f32(const uint8_t *bgrL, const uint8_t *bgrR, const float *src, int W, int H, int D,
                 float alpha, float tau_smooth, int min_level, int right_view, float *vol_f32, float *wta,
                 float *disp, float *plane)
@@ -402,8 +409,12 @@ int ref_hbp_f32(const uint8_t *bgrL, const uint8_t *bgrR, const float *src, int 
         d2h(wta, sc->g_img_D_d(), n);
         StereoData *sd = new StereoData(sc, true);
         delete sc;
+        cudaDeviceSynchronize();
+        auto c0 = std::chrono::steady_clock::now();
         HBP_ISP *hbp = new HBP_ISP(isp, sd, alpha, tau_smooth);
         std::pair<cv::Mat, cv::Mat> res = hbp->run_ms(min_level);
+        auto c1 = std::chrono::steady_clock::now();
+        g_last_hbp_ms = std::chrono::duration<double, std::milli>(c1 - c0).count();
         rc = last_error();
         std::memcpy(disp, res.first.data, sizeof(float) * n);
         std::memcpy(plane, res.second.data, sizeof(float) * n * 3);
