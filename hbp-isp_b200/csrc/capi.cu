@@ -728,6 +728,40 @@ hbp_status hbp_weighted_median_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t 
     });
 }
 
+hbp_status hbp_weighted_median_gpu_d(hbp_ctx *c, const uint8_t *bgrL, const uint8_t *fail_mask, float *plane,
+                                     float *disp_out, int W, int H, void *stream)
+{
+    if (!c || !bgrL || !fail_mask || !plane)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        check_dims(W, H, 2);
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
+        cudaStream_t st = pick(c, stream);
+        c->tmp.reset();
+        float *copy = c->tmp.alloc<float>(3 * (size_t)W * H);
+        float *wtab = c->tmp.alloc<float>(766);
+        HBP_CUDA(cudaMemcpyAsync(copy, plane, sizeof(float) * 3 * W * H, cudaMemcpyDeviceToDevice, st));
+        launch_patch_weights(wtab, st);
+        launch_weighted_median_gpu(bgrL, fail_mask, copy, plane, W, H, wtab, c->tmp, st);
+        if (disp_out)
+            launch_plane_to_disp(plane, disp_out, W, H, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+hbp_status hbp_patch_weights_d(hbp_ctx *c, float *wtab766, void *stream)
+{
+    if (!c || !wtab766)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = pick(c, stream);
+        launch_patch_weights(wtab766, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
 hbp_status hbp_plane_to_disp_d(hbp_ctx *c, const float *plane, float *disp, int W, int H, void *stream)
 {
     if (!c || !plane || !disp)

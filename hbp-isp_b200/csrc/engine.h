@@ -349,6 +349,12 @@ void launch_weighted_median(const uint8_t *bgr, const uint8_t *fail, const float
                             float *plane_out, int W, int H, const float *wtab, Arena &tmp,
                             cudaStream_t st);
 void launch_driver_median(float *disp, float *tmp, int W, int H, cudaStream_t st);
+// median_filter_gpu: the reference's GPU variant of the weighted median
+// (device patch weights from launch_patch_weights, in lab.cu)
+void launch_patch_weights(float *wtab766, cudaStream_t st);
+void launch_weighted_median_gpu(const uint8_t *bgr, const uint8_t *fail, const float *plane_in,
+                                float *plane_out, int W, int H, const float *wtab766, Arena &tmp,
+                                cudaStream_t st);
 // same filter with the file-scope static scratch of noalloc.cu (allocates nothing)
 void launch_driver_median_noalloc(float *disp, int W, int H, cudaStream_t st);
 

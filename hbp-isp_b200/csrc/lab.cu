@@ -99,7 +99,28 @@ __global__ void blur_kernel(const uint8_t *__restrict__ bgr, int W, int H, BlurT
     }
     out[(size_t)y * W + x] = make_float4(a0, a1, a2, a3);
 }
+
+// compute_patch_weight of median_filter_gpu (post_process.cu:199-213) for
+// every colour distance k = 0..765: expf(-k / 10.0f), CUDA's expf as the
+// reference's device code calls it (this file keeps the default contraction
+// setting, so the library function is compiled as it is there).
+__global__ void patch_weight_kernel(float *wtab)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 766)
+    {
+        const float absdiff = (float)k;
+        wtab[k] = expf(-absdiff / 10.0f);
+    }
+}
 } // namespace
+
+void launch_patch_weights(float *wtab766, cudaStream_t st)
+{
+    patch_weight_kernel<<<ceil_div(766, 128), 128, 0, st>>>(wtab766);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+}
 
 int blur_radius(double sigma) { return (int)std::round(3 * sigma); }
 

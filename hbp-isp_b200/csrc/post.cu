@@ -219,6 +219,200 @@ __global__ void __launch_bounds__(WM_T)
     }
 }
 
+// PostProcess::median_filter_gpu (post_process.cu:188-371), the reference's
+// GPU variant of the weighted median: one block per failed pixel. Window
+// samples in row-major order get the device patch weight wtab[sum|dBGR|]
+// (expf(-k / 10), launch_patch_weights) and z = fma(a, x, b * y) + c, the
+// reference device code's evaluation of a * x + b * y + c; the total weight
+// is a float sum in window order. The reference orders the samples with
+// bubble_sort (:216-229): step i swaps into position i, in scan order, every
+// later sample smaller than the current one there. Its effect is a rotation
+// along the chain of strict running minima of [i, n): position i takes the
+// last of the chain, each chain member the previous one's sample, the first
+// member the old sample at i; position i is then final. Each step finds the
+// chain in parallel (per-thread chunk minima, an ordered scan of them, a walk
+// of each chunk) and applies the rotation; the running weight in float stops
+// the sort at the first sample past half the total, whose plane is taken.
+// NaN disparities never enter a chain, as NaN compares false there.
+constexpr int WG_T = 256, WG_MAXN = (2 * WM_R + 1) * (2 * WM_R + 1);
+constexpr int WG_MAXC = (WG_MAXN - 1 + WG_T - 1) / WG_T; // chunk length bound (7)
+
+// the earlier of two (z, pos) candidates unless the later is strictly smaller;
+// pos < 0: none
+__device__ __forceinline__ void first_min(float &z, int &p, float z2, int p2)
+{
+    if (p2 >= 0 && (p < 0 || z2 < z))
+    {
+        z = z2;
+        p = p2;
+    }
+}
+
+__global__ void __launch_bounds__(WG_T)
+    weighted_median_gpu_kernel(const uint8_t *__restrict__ bgr, const int *__restrict__ list, int W, int H,
+                               const float *__restrict__ plane_in, float *__restrict__ plane_out,
+                               const float *__restrict__ wtab)
+{
+    __shared__ float zs[WG_MAXN], ws[WG_MAXN];
+    __shared__ int ids[WG_MAXN];
+    __shared__ float warp_z[WG_T / 32];
+    __shared__ int warp_p[WG_T / 32];
+    __shared__ float s_center;
+    __shared__ int s_pick;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int p = list[blockIdx.x];
+    const int y = p / W, x = p - y * W;
+    const int y0 = max(y - WM_R, 0), y1 = min(y + WM_R, H - 1);
+    const int x0 = max(x - WM_R, 0), x1 = min(x + WM_R, W - 1);
+    const int ww = x1 - x0 + 1, n = ww * (y1 - y0 + 1);
+    const uint8_t *s = bgr + 3 * (size_t)p;
+    const float fx = (float)x, fy = (float)y;
+    for (int j = tid; j < n; j += WG_T)
+    {
+        const int q = (y0 + j / ww) * W + x0 + j % ww;
+        const uint8_t *t = bgr + 3 * (size_t)q;
+        const int d = abs((int)s[0] - (int)t[0]) + abs((int)s[1] - (int)t[1]) + abs((int)s[2] - (int)t[2]);
+        ws[j] = wtab[d];
+        const float *pl = plane_in + 3 * (size_t)q;
+        zs[j] = __fadd_rn(__fmaf_rn(pl[0], fx, __fmul_rn(pl[1], fy)), pl[2]);
+        ids[j] = j;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        float sum = 0.f;
+        for (int j = 0; j < n; ++j)
+            sum = __fadd_rn(sum, ws[j]);
+        s_center = __fdiv_rn(sum, 2.0f);
+        s_pick = -1;
+    }
+    float run = 0.f; // thread 0's running weight in sorted order
+    __syncthreads();
+    for (int i = 0; i < n; ++i)
+    {
+        const float zi = zs[i];
+        const bool chain = zi == zi; // a NaN at i is never displaced
+        const int m = n - i - 1;
+        const int c = (m + WG_T - 1) / WG_T;
+        const int lo = i + 1 + tid * c, hi = min(lo + c, n);
+        // the chunk's first minimum (NaN samples never qualify)
+        float cz = 0.f;
+        int cp = -1;
+        for (int j = lo; j < hi; ++j)
+        {
+            const float zj = zs[j];
+            if (zj == zj)
+                first_min(cz, cp, zj, j);
+        }
+        // ordered inclusive scan of the chunk minima: within the warp, then
+        // across warps through shared memory
+        float sz = cz;
+        int sp = cp;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const float oz = __shfl_up_sync(0xffffffffu, sz, off);
+            const int op = __shfl_up_sync(0xffffffffu, sp, off);
+            if (lane >= off)
+            {
+                float nz = oz;
+                int np = op;
+                first_min(nz, np, sz, sp);
+                sz = nz;
+                sp = np;
+            }
+        }
+        if (lane == 31)
+        {
+            warp_z[wid] = sz;
+            warp_p[wid] = sp;
+        }
+        // exclusive prefix within the warp
+        float ez = __shfl_up_sync(0xffffffffu, sz, 1);
+        int ep = __shfl_up_sync(0xffffffffu, sp, 1);
+        if (lane == 0)
+            ep = -1;
+        __syncthreads();
+        // the sample at i, then the earlier warps, then the earlier lanes
+        float pz = zi;
+        int pp = i;
+        for (int k = 0; k < wid; ++k)
+            first_min(pz, pp, warp_z[k], warp_p[k]);
+        first_min(pz, pp, ez, ep);
+        float tz = zi; // the chain's end over the whole range
+        int tp = i;
+        for (int k = 0; k < WG_T / 32; ++k)
+            first_min(tz, tp, warp_z[k], warp_p[k]);
+        // walk the chunk: records j (z[j] below the running minimum) take the
+        // previous record's sample
+        int rj[WG_MAXC], rp[WG_MAXC];
+        int nr = 0;
+        if (chain)
+        {
+            for (int j = lo; j < hi; ++j)
+            {
+                const float zj = zs[j];
+                if (zj < pz)
+                {
+                    rj[nr] = j;
+                    rp[nr] = pp;
+                    ++nr;
+                    pz = zj;
+                    pp = j;
+                }
+            }
+        }
+        float vz[WG_MAXC], vw[WG_MAXC];
+        int vi[WG_MAXC];
+#pragma unroll
+        for (int k = 0; k < WG_MAXC; ++k)
+            if (k < nr)
+            {
+                vz[k] = zs[rp[k]];
+                vw[k] = ws[rp[k]];
+                vi[k] = ids[rp[k]];
+            }
+        float nz = 0.f, nw = 0.f;
+        int ni = 0;
+        const bool moved = chain && tp != i;
+        if (tid == 0)
+        {
+            const int src = moved ? tp : i; // the sample that ends at position i
+            nz = zs[src];
+            nw = ws[src];
+            ni = ids[src];
+            run = __fadd_rn(run, nw);
+            if (run > s_center)
+                s_pick = ni;
+        }
+        __syncthreads();
+        if (s_pick >= 0)
+            break;
+#pragma unroll
+        for (int k = 0; k < WG_MAXC; ++k)
+            if (k < nr)
+            {
+                zs[rj[k]] = vz[k];
+                ws[rj[k]] = vw[k];
+                ids[rj[k]] = vi[k];
+            }
+        if (tid == 0 && moved)
+        {
+            zs[i] = nz;
+            ws[i] = nw;
+            ids[i] = ni;
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && s_pick >= 0)
+    {
+        const int q = (y0 + s_pick / ww) * W + x0 + s_pick % ww;
+        plane_out[3 * (size_t)p] = plane_in[3 * (size_t)q];
+        plane_out[3 * (size_t)p + 1] = plane_in[3 * (size_t)q + 1];
+        plane_out[3 * (size_t)p + 2] = plane_in[3 * (size_t)q + 2];
+    }
+}
+
 __device__ __forceinline__ float median7(float *v)
 {
     for (int j = 1; j < 7; ++j)
@@ -292,6 +486,30 @@ void launch_plane_to_disp(const float *plane, float *disp, int W, int H, cudaStr
     plane_to_disp_kernel<<<ceil_div(W * H, 256), 256, 0, st>>>(plane, W, H, disp);
     note_launch();
     HBP_LAUNCH_CHECK();
+}
+
+void launch_weighted_median_gpu(const uint8_t *bgr, const uint8_t *fail, const float *plane_in,
+                                float *plane_out, int W, int H, const float *wtab766, Arena &tmp,
+                                cudaStream_t st)
+{
+    int n = W * H;
+    size_t m = tmp.mark();
+    int *list = tmp.alloc<int>(n), *count = tmp.alloc<int>(1);
+    HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int), st));
+    HBP_CUDA(cudaMemcpyAsync(plane_out, plane_in, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    compact_fail<<<ceil_div(n, 256), 256, 0, st>>>(fail, n, list, count);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    int nf = 0;
+    HBP_CUDA(cudaMemcpyAsync(&nf, count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HBP_CUDA(cudaStreamSynchronize(st));
+    if (nf > 0)
+    {
+        weighted_median_gpu_kernel<<<nf, WG_T, 0, st>>>(bgr, list, W, H, plane_in, plane_out, wtab766);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+    }
+    tmp.rewind(m);
 }
 
 void median_weight_table(float *host766)

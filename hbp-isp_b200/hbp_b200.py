@@ -243,6 +243,12 @@ class Context:
     def weighted_median_d(self, bgrL, fail, plane, disp_out, W, H):
         _check(lib().hbp_weighted_median_d(self.h, _p(bgrL), _p(fail), _p(plane), _p(disp_out), W, H, None))
 
+    def weighted_median_gpu_d(self, bgrL, fail, plane, disp_out, W, H):
+        _check(lib().hbp_weighted_median_gpu_d(self.h, _p(bgrL), _p(fail), _p(plane), _p(disp_out), W, H, None))
+
+    def patch_weights_d(self, wtab766):
+        _check(lib().hbp_patch_weights_d(self.h, _p(wtab766), None))
+
     def driver_median_d(self, disp, W, H):
         _check(lib().hbp_driver_median_d(self.h, _p(disp), W, H, None))
 

@@ -180,6 +180,16 @@ hbp_status hbp_lr_check_d(hbp_ctx *ctx, const float *dispL, const float *dispR, 
 /* PostProcess::median_filter + plane_label_to_disp (post_process.cu:112-185). */
 hbp_status hbp_weighted_median_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *fail,
                                  float *plane, float *disp_out, int W, int H, void *stream);
+/* PostProcess::median_filter_gpu (post_process.cu:188-371), the reference's
+ * GPU variant: as hbp_weighted_median_d, but with the device's expf weights,
+ * float weight sums, the disparity evaluated as fma(a, x, b * y) + c, and the
+ * samples in bubble_sort's order (post_process.cu:216-229), whose ties can
+ * differ from the CPU variant's. */
+hbp_status hbp_weighted_median_gpu_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *fail,
+                                     float *plane, float *disp_out, int W, int H, void *stream);
+/* The GPU variant's 766 patch weights expf(-k / 10), k = 0..765 (device
+ * memory), as compute_patch_weight evaluates them (post_process.cu:199-213). */
+hbp_status hbp_patch_weights_d(hbp_ctx *ctx, float *wtab766, void *stream);
 /* PostProcess::plane_label_to_disp for one view (post_process.cu:373-390):
  * disp = a*x + b*y + c of each pixel's plane. */
 hbp_status hbp_plane_to_disp_d(hbp_ctx *ctx, const float *plane, float *disp, int W, int H, void *stream);

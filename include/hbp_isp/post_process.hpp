@@ -42,7 +42,17 @@ class PostProcess
                                             pL->as<float>(), nullptr, width, height, nullptr));
         detail::download(results_left.second, pL);
     }
-    void median_filter_gpu(Result &l, Result &r) { median_filter(l, r); }
+    // median_filter_gpu (post_process.cu:245-371): the reference's GPU variant
+    // (device expf weights, float sums, bubble-sort tie order)
+    void median_filter_gpu(Result &results_left, Result &)
+    {
+        if (!fail)
+            throw std::logic_error("PostProcess: left_right_check() comes before median_filter_gpu()");
+        detail::Buf pL = detail::upload(results_left.second);
+        detail::check(hbp_weighted_median_gpu_d(detail::shared_ctx()->h, left->as<uint8_t>(), fail->as<uint8_t>(),
+                                                pL->as<float>(), nullptr, width, height, nullptr));
+        detail::download(results_left.second, pL);
+    }
 
     // plane_label_to_disp (post_process.cu:373-390)
     void plane_label_to_disp(Result &results_left, Result &)

@@ -53,4 +53,6 @@ void orc_plane_to_disp(const float *plane, int W, int H, float *disp);
 void orc_weighted_median(const uint8_t *bgr, const uint8_t *fail, float *plane, int W, int H,
                          int stable);
 void orc_driver_median(float *D, int W, int H);
+void orc_weighted_median_gpu(const uint8_t *bgr, const uint8_t *fail, float *plane, int W, int H,
+                             const float *wtab, int z_mode);
 }

@@ -145,6 +145,83 @@ void orc_weighted_median(const uint8_t *bgr, const uint8_t *fail, float *plane, 
     }
 }
 
+// PostProcess::median_filter_gpu (post_process.cu:188-371), the reference's
+// GPU variant of the weighted median, restated literally: per failed pixel the
+// clipped 41x41 window in row-major order gives (window index, weight, z),
+// the weight being compute_patch_weight's expf(-sum|dBGR| / 10) (wtab[k] for
+// the integer colour distance k: the device's expf values, passed in), and
+// z the plane's disparity at the pixel as the device evaluates
+// a * x + b * y + c (z_mode 0: fma(a, x, b * y) + c; 1: unfused; 2:
+// fma(a, x, fma(b, y, c))). The total weight is a float sum in window order;
+// the samples are ordered by bubble_sort (:216-229: for each i, every later j
+// with a smaller z is swapped into i), and the first sample whose float
+// running weight exceeds half the total gives the plane. Position i is final
+// once step i ends, so the scan runs alongside the sort and stops there.
+void orc_weighted_median_gpu(const uint8_t *bgr, const uint8_t *fail, float *plane, int W, int H,
+                             const float *wtab, int z_mode)
+{
+    std::vector<float> copy(plane, plane + 3 * (size_t)W * H);
+    const int R = 20;
+    struct S
+    {
+        float i, w, z;
+    };
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int y = 0; y < H; ++y)
+    {
+        std::vector<S> m;
+        for (int x = 0; x < W; ++x)
+        {
+            if (!fail[y * W + x])
+                continue;
+            m.clear();
+            const int y0 = std::max(y - R, 0), y1 = std::min(y + R, H - 1);
+            const int x0 = std::max(x - R, 0), x1 = std::min(x + R, W - 1);
+            const uint8_t *s = bgr + 3 * (size_t)(y * W + x);
+            float sumw = 0.f;
+            int k = 0;
+            for (int yy = y0; yy <= y1; ++yy)
+                for (int xx = x0; xx <= x1; ++xx, ++k)
+                {
+                    const uint8_t *t = bgr + 3 * (size_t)(yy * W + xx);
+                    const int d = std::abs((int)s[0] - (int)t[0]) + std::abs((int)s[1] - (int)t[1]) +
+                                  std::abs((int)s[2] - (int)t[2]);
+                    const float w = wtab[d];
+                    sumw += w;
+                    const float *pl = copy.data() + 3 * (size_t)(yy * W + xx);
+                    const float fx = (float)x, fy = (float)y;
+                    float z;
+                    if (z_mode == 0)
+                        z = std::fma(pl[0], fx, pl[1] * fy) + pl[2];
+                    else if (z_mode == 1)
+                        z = (pl[0] * fx + pl[1] * fy) + pl[2];
+                    else
+                        z = std::fma(pl[0], fx, std::fma(pl[1], fy, pl[2]));
+                    m.push_back({(float)k, w, z});
+                }
+            const int n = (int)m.size();
+            const float center = sumw / 2;
+            float run = 0.f;
+            int pick = -1;
+            for (int i = 0; i < n && pick < 0; ++i)
+            {
+                for (int j = i + 1; j < n; ++j)
+                    if (m[j].z < m[i].z)
+                        std::swap(m[i], m[j]);
+                run += m[i].w;
+                if (run > center)
+                    pick = (int)m[i].i;
+            }
+            if (pick >= 0)
+            {
+                const int ww = x1 - x0 + 1;
+                const int q = (y0 + pick / ww) * W + x0 + pick % ww;
+                std::memcpy(plane + 3 * (size_t)(y * W + x), copy.data() + 3 * (size_t)q, 12);
+            }
+        }
+    }
+}
+
 // medianFilter of the single-pair driver (main_stereo_hbp_isp.cu:120-192):
 // a 7-tap horizontal median into a zero-initialised buffer over the interior
 // (3-pixel border), then a 7-tap vertical median of that buffer back into D;

@@ -205,6 +205,16 @@ def weighted_median(bgr, fail, plane, stable=True):
     return pl
 
 
+def weighted_median_gpu(bgr, fail, plane, wtab, z_mode=0):
+    """PostProcess::median_filter_gpu (the reference's GPU variant); wtab holds the
+    766 device patch weights expf(-k / 10)."""
+    H, W = fail.shape
+    pl = np.ascontiguousarray(plane, np.float32).copy()
+    lib().orc_weighted_median_gpu(_p(np.ascontiguousarray(bgr, np.uint8)), _p(np.ascontiguousarray(fail, np.uint8)),
+                                  _p(pl), W, H, _p(np.ascontiguousarray(wtab, np.float32)), int(z_mode))
+    return pl
+
+
 def driver_median(disp):
     d = np.ascontiguousarray(disp, np.float32).copy()
     H, W = d.shape

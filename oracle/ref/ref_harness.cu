@@ -60,6 +60,16 @@ struct StereoCostView : public StereoCost
     const float *greyR_f() const { return imgR_f1_d; }
 };
 
+__global__ void ref_patch_weight_k(float *out, float omega)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 766)
+    {
+        float absdiff = (float)k;
+        out[k] = expf(-absdiff / omega);
+    }
+}
+
 template <typename T>
 void d2h(T *dst, const T *src, size_t n)
 {
@@ -335,9 +345,9 @@ int ref_hbp_pair(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D, 
 }
 
 // PostProcess::left_right_check + plane_label_to_disp (post_process.cu:47-110,
-// :373-390) and, with do_median != 0, median_filter + plane_label_to_disp
-// (:127-185). CPU only. dispL/planeL are updated in place; dispR/planeR are
-// read.
+// :373-390) and, with do_median == 1, median_filter + plane_label_to_disp
+// (:127-185, CPU); with do_median == 2, median_filter_gpu (:245-371) instead.
+// dispL/planeL are updated in place; dispR/planeR are read.
 int ref_post(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, float *dispL, float *planeL,
              float *dispR, float *planeR, int do_median)
 {
@@ -352,7 +362,12 @@ int ref_post(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, float *disp
     PostProcess pp(L, R);
     pp.left_right_check(left, right);
     pp.plane_label_to_disp(left, right);
-    if (do_median)
+    if (do_median == 2)
+    {
+        pp.median_filter_gpu(left, right);
+        pp.plane_label_to_disp(left, right);
+    }
+    else if (do_median)
     {
         pp.median_filter(left, right);
         pp.plane_label_to_disp(left, right);
@@ -360,6 +375,20 @@ int ref_post(const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, float *disp
     std::memcpy(dispL, left.first.data, n * 4);
     std::memcpy(planeL, left.second.data, n * 12);
     return 0;
+}
+
+// compute_patch_weight's expression (post_process.cu:199-213) for every
+// colour distance k = 0..765 (the distance of two BGR8 pixels is an integer):
+// expf(-k / 10.0f) on the device, as median_filter_gpu evaluates it.
+int ref_patch_weights(float *out766)
+{
+    float *d;
+    cudaMalloc(&d, sizeof(float) * 766);
+    ref_patch_weight_k<<<(766 + 127) / 128, 128>>>(d, 10.0f);
+    int rc = last_error();
+    d2h(out766, d, 766);
+    cudaFree(d);
+    return rc;
 }
 
 // The MC-CNN single-view path (main_bench_middv3.cu:73-108 with cost

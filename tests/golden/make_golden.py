@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg]
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|post_gpu]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -167,6 +167,8 @@ class RefLib:
                     bdl=bdl[:tb])
 
     def post(self, L, R, dispL, planeL, dispR, planeR, median=True):
+        """LR check + fill; median: False none, True (1) the CPU weighted median,
+        2 the GPU variant (median_filter_gpu)."""
         H, W, _ = L.shape
         dL, pL = dispL.copy(), planeL.copy()
         rc = self.lib.ref_post(ptr(L), ptr(R), W, H, ptr(dL), ptr(pL), ptr(np.ascontiguousarray(dispR)),
@@ -311,11 +313,26 @@ def seg_record(ref: RefLib, W, H, seed):
     return rec
 
 
+def post_gpu_record(ref: RefLib, golden_dir: str):
+    """median_filter_gpu on the reference's own HBP results stored in the small
+    fixtures (both views' disparities and planes), and the device patch weights."""
+    w = np.zeros(766, np.float32)
+    assert ref.lib.ref_patch_weights(ptr(w)) == 0
+    rec = dict(patch_weights=w)
+    for name in ("tiny_96x64_d32_s7", "small_160x120_d48_s11"):
+        z = np.load(os.path.join(golden_dir, name + ".npz"))
+        d, p = ref.post(z["left"], z["right"], z["disp"], z["plane"].astype(np.float32), z["disp_right"],
+                        z["plane_right"].astype(np.float32), median=2)
+        rec[name + "_disp"] = d
+        rec[name + "_plane"] = p
+    return rec
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
-    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg"], default=None)
+    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "post_gpu"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     ref = RefLib(args.lib)
@@ -336,7 +353,12 @@ def main():
             rec = seg_record(ref, W, H, seed)
             np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
             print(name, [int(rec[f"c{i}_level_sizes"].shape[0]) for i in range(len(SEG_CFGS))])
-    if args.only in ("mccnn", "ad", "seg"):
+    if args.only in (None, "post_gpu"):
+        # inputs: the reference's HBP results in the committed census fixtures
+        src = os.path.dirname(os.path.abspath(__file__))
+        np.savez_compressed(os.path.join(args.out, "post_gpu.npz"), **post_gpu_record(ref, src))
+        print("post_gpu")
+    if args.only in ("mccnn", "ad", "seg", "post_gpu"):
         return
 
     for (W, H, D, seed, full, name) in [

@@ -239,3 +239,27 @@ def test_fp16_messages_agree_with_fp32(eng):
         bad = lambda d: 100.0 * float(np.mean(np.abs(d - s.gt)[s.nonocc] > 2.0))
         assert abs(bad(d16) - bad(d32)) <= 0.1
     assert min(same) >= 0.998 and np.mean(same) >= 0.999, same
+
+
+@pytest.mark.parametrize("name", SCENES[:2])
+def test_weighted_median_gpu_variant_vs_reference(eng, golden_dir, name):
+    """hbp_weighted_median_gpu_d (PostProcess::median_filter_gpu) on the
+    reference's own HBP results equals the reference build's planes and
+    disparity bit for bit; the device patch weights equal the reference's."""
+    import pyoracle as O
+    E, ctx, torch = eng
+    z = load(golden_dir, name)
+    f = load(golden_dir, "post_gpu")
+    wt = torch.zeros(766, device="cuda")
+    ctx.patch_weights_d(wt)
+    torch.cuda.synchronize()
+    assert np.array_equal(wt.cpu().numpy().view(np.uint32), f["patch_weights"].view(np.uint32))
+    H, W = z["disp"].shape
+    pl, fail = O.lr_check(z["disp"], z["disp_right"], z["plane"].astype(np.float32))
+    plane = dev(torch, pl.reshape(-1))
+    dout = torch.zeros(H * W, dtype=torch.float32, device="cuda")
+    ctx.weighted_median_gpu_d(dev(torch, z["left"]), dev(torch, fail.reshape(-1)), plane, dout, W, H)
+    torch.cuda.synchronize()
+    got = plane.cpu().numpy().reshape(H, W, 3)
+    assert np.array_equal(got.view(np.uint32), f[name + "_plane"].view(np.uint32))
+    assert np.array_equal(dout.cpu().numpy().reshape(H, W).view(np.uint32), f[name + "_disp"].view(np.uint32))

@@ -269,3 +269,21 @@ def test_seg_variants_match_reference(golden_dir, name):
             assert np.array_equal(seg[k], z[f"c{i}_{k}"]), (i, k)
         m, r = seg["mean"], z[f"c{i}_mean"]
         assert np.max(np.abs(m - r) / np.maximum(1.0, np.abs(r))) < 5e-5, i
+
+
+@pytest.mark.parametrize("name", ["tiny_96x64_d32_s7", "small_160x120_d48_s11"])
+def test_weighted_median_gpu_variant_bit_exact(golden_dir, name):
+    """PostProcess::median_filter_gpu on the reference's own HBP results: the
+    oracle's restatement (device patch weights from the fixture, float sums,
+    bubble-sort order) equals the reference build's planes bit for bit, with
+    the disparity evaluated as fma(a, x, b * y) + c; the unfused and the
+    other fused forms do not (the form is pinned, not assumed)."""
+    z = load(golden_dir, name)
+    f = load(golden_dir, "post_gpu")
+    pl, fail = O.lr_check(z["disp"], z["disp_right"], z["plane"].astype(np.float32))
+    want = f[name + "_plane"]
+    got = O.weighted_median_gpu(z["left"], fail, pl, f["patch_weights"], z_mode=0)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(O.plane_to_disp(got).view(np.uint32), f[name + "_disp"].view(np.uint32))
+    other = [O.weighted_median_gpu(z["left"], fail, pl, f["patch_weights"], z_mode=m) for m in (1, 2)]
+    assert not any(np.array_equal(o, want) for o in other)
