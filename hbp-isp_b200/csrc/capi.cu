@@ -549,6 +549,21 @@ hbp_status hbp_pyramid_levels(hbp_ctx *c, int *sizes, int max_levels)
     return HBP_OK;
 }
 
+hbp_status hbp_pyramid_device(hbp_ctx *c, const int **clus, const float **mean, const int **bd, const int **bdl)
+{
+    if (!c || !c->have_pyr)
+        return fail(HBP_ERR_INVALID_ARG, "no pyramid");
+    if (clus)
+        *clus = c->pyr.clus;
+    if (mean)
+        *mean = c->pyr.sums;
+    if (bd)
+        *bd = reinterpret_cast<const int *>(c->pyr.bd);
+    if (bdl)
+        *bdl = c->pyr.bdl;
+    return HBP_OK;
+}
+
 hbp_status hbp_pyramid_copy(hbp_ctx *c, int *clus, float *mean, int *bd, int *bdl)
 {
     if (!c || !c->have_pyr)

@@ -145,6 +145,11 @@ hbp_status hbp_lab_sigma_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, doubl
                            void *stream);
 hbp_status hbp_pyramid_levels(hbp_ctx *ctx, int *sizes, int max_levels);
 hbp_status hbp_pyramid_copy(hbp_ctx *ctx, int *clus, float *mean, int *bd, int *bdl);
+/* The same arrays in place on the device (SegHAC / ISPData g_isp_clus_d,
+ * g_isp_mean_d, g_isp_bd_d (int pairs), g_isp_bdl_d; segment.hpp:131-150,
+ * hbp_isp.hpp:18-21). Valid until the context's next segmentation. */
+hbp_status hbp_pyramid_device(hbp_ctx *ctx, const int **clus, const float **mean, const int **bd,
+                              const int **bdl);
 
 /* HBP_ISP(ISPData, StereoData, alpha, tau_smooth).run_ms(min_level)
  * (hbp_isp.hpp:288-386, hbp_isp.cu:1313-1346) on the context's pyramid and a

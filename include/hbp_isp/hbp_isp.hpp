@@ -33,8 +33,15 @@ class ISPData
     int g_mean_channels() const { return 6; }
     std::vector<int> g_num_clus_isp() const { return num_clus_isp; }
     std::vector<int> g_num_bd_isp() const { return num_bd_isp; }
-    // the ISP arrays on the host: clus, mean sums [6][N_l], bd pairs, bdl,
-    // concatenated over levels (the reference's device getters)
+    // the ISP arrays in place on the device (hbp_isp.hpp:18-21; bd as int
+    // pairs); they belong to the SegHAC's context, so a later run_ms of that
+    // SegHAC replaces them (the reference's ISPData holds a copy)
+    const int *g_isp_clus_d() const { return device_arrays(0).c; }
+    const float *g_isp_mean_d() const { return device_arrays(1).m; }
+    const int *g_isp_bd_d() const { return device_arrays(2).c; }
+    const int *g_isp_bdl_d() const { return device_arrays(3).c; }
+    // the same on the host: clus, mean sums [6][N_l], bd pairs, bdl,
+    // concatenated over levels
     void copy_isp(std::vector<int> &clus, std::vector<float> &mean, std::vector<int> &bd,
                   std::vector<int> &bdl) const
     {
@@ -54,6 +61,25 @@ class ISPData
     int width, height;
     detail::CtxPtr ctx;
     std::vector<int> num_clus_isp, num_bd_isp;
+
+  private:
+    struct Ptr
+    {
+        const int *c = nullptr;
+        const float *m = nullptr;
+    };
+    Ptr device_arrays(int which) const
+    {
+        const int *clus = nullptr, *bd = nullptr, *bdl = nullptr;
+        const float *mean = nullptr;
+        detail::check(hbp_pyramid_device(ctx->h, &clus, &mean, &bd, &bdl));
+        Ptr p;
+        p.c = which == 0 ? clus : which == 2 ? bd : bdl;
+        p.m = mean;
+        return p;
+    }
+
+  public:
 };
 
 class StereoData

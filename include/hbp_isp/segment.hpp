@@ -48,22 +48,76 @@ class SegHAC
         ctx = std::make_shared<detail::Ctx>();
     }
 
-    // run_ms (segment.cu:1279-1321); per-level images are not produced
+    // run_ms (segment.cu:1279-1321). With LabelISPFormat the reference leaves
+    // segs untouched (save_output, :1099-1113), and so does this. Each run
+    // builds the pyramid from the current image anew.
     void run_ms(std::vector<Mat> *segs = nullptr)
     {
-        if (segs)
-            throw std::invalid_argument("SegHAC: per-level label images are not produced");
+        (void)segs;
         detail::check(hbp_segment_cfg_d(ctx->h, img->as<uint8_t>(), width, height, (int)m_link, m_num_nb, m_sigma,
                                         &levels, nullptr));
+    }
+
+    // set_frame (segment.hpp:87-91): the next image of a video stream, same size
+    void set_frame(const Mat &frame)
+    {
+        detail::need_bgr(frame, "SegHAC::set_frame");
+        if (frame.cols != width || frame.rows != height)
+            throw std::invalid_argument("SegHAC::set_frame: the frame size differs");
+        img = detail::upload(frame);
+    }
+    // set_seq_img (segment.hpp:95-107): the next image of a sequence, same size
+    // or transposed
+    void set_seq_img(const Mat &frame)
+    {
+        detail::need_bgr(frame, "SegHAC::set_seq_img");
+        if (frame.cols != width)
+        {
+            if (frame.cols != height || frame.rows != width)
+                throw std::invalid_argument("SegHAC::set_seq_img: the image is neither the same size nor transposed");
+            width = frame.cols;
+            height = frame.rows;
+        }
+        img = detail::upload(frame);
     }
 
     int g_width() const { return width; }
     int g_height() const { return height; }
     int g_levels() const { return levels; }
+    int g_mean_channels() const { return 6; }
+    // the level sizes and the ISP arrays in place on the device (segment.hpp:
+    // 118-150); the pointers stay valid until the next run_ms
+    std::vector<int> g_num_clus_isp() const { return level_column(0); }
+    std::vector<int> g_num_bd_isp() const { return level_column(1); }
+    const int *g_isp_clus_d() const { return device_arrays().clus; }
+    const float *g_isp_mean_d() const { return device_arrays().mean; }
+    const int *g_isp_bd_d() const { return device_arrays().bd; }
+    const int *g_isp_bdl_d() const { return device_arrays().bdl; }
 
     detail::CtxPtr ctx; // holds the pyramid after run_ms
 
   private:
+    std::vector<int> level_column(int k) const
+    {
+        std::vector<int> sizes(2 * 64), out;
+        detail::check(hbp_pyramid_levels(ctx->h, sizes.data(), 64));
+        for (int l = 0; l < 64 && sizes[2 * l] > 0; ++l)
+            out.push_back(sizes[2 * l + k]);
+        return out;
+    }
+    struct DeviceArrays
+    {
+        const int *clus = nullptr;
+        const float *mean = nullptr;
+        const int *bd = nullptr, *bdl = nullptr;
+    };
+    DeviceArrays device_arrays() const
+    {
+        DeviceArrays a;
+        detail::check(hbp_pyramid_device(ctx->h, &a.clus, &a.mean, &a.bd, &a.bdl));
+        return a;
+    }
+
     int width, height;
     Linkage m_link;
     int m_num_nb;

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <tuple>
 
 #include "hbp_isp/hbp_isp_all.hpp"
 
@@ -88,6 +89,36 @@ static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, co
     delete isp;
 }
 
+// SegHAC on a stream (segment.hpp:87-107): after set_frame / set_seq_img and
+// run_ms, the pyramid equals a fresh SegHAC's on the same image, and the
+// device getters point at it.
+static void stream_check(const Mat &L, const Mat &R)
+{
+    auto isp_of = [](SegHAC &s) {
+        ISPData isp(&s);
+        std::vector<int> clus, bd, bdl;
+        std::vector<float> mean;
+        isp.copy_isp(clus, mean, bd, bdl);
+        if (!isp.g_isp_clus_d() || !isp.g_isp_mean_d() || !isp.g_isp_bd_d() || !isp.g_isp_bdl_d())
+            throw std::runtime_error("ISPData device getters returned null");
+        return std::make_tuple(clus, mean, bd, bdl, isp.g_num_clus_isp());
+    };
+    SegHAC video(L, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+    video.run_ms();
+    video.set_frame(R);
+    video.run_ms();
+    SegHAC fresh(R, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+    fresh.run_ms();
+    if (isp_of(video) != isp_of(fresh) || video.g_num_clus_isp() != fresh.g_num_clus_isp())
+        throw std::runtime_error("set_frame + run_ms differs from a fresh SegHAC");
+    video.set_seq_img(L);
+    video.run_ms();
+    SegHAC fresh_l(L, CentoridLink, 4, 0, LabelISPFormat, 1, false);
+    fresh_l.run_ms();
+    if (isp_of(video) != isp_of(fresh_l))
+        throw std::runtime_error("set_seq_img + run_ms differs from a fresh SegHAC");
+}
+
 int main(int argc, char **argv)
 {
     if (argc != 7 && argc != 8)
@@ -100,6 +131,7 @@ int main(int argc, char **argv)
     try
     {
         Mat L = read_bgr(argv[1], W, H), R = read_bgr(argv[2], W, H);
+        stream_check(L, R);
         flows(L, R, D, "Census", "", 1000.1f, out + "census");
         flows(L, R, D, "AD", "", 1000.1f, out + "ad");
         if (argc == 8)
