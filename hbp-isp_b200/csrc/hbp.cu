@@ -1065,9 +1065,11 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
         cswap(1, 3);
         cswap(1, 2);
     }
-    // Lower bound of q = (phi / 3) / dist_pos from one multiply by rounded
-    // reciprocals: qa is within 4 ulp of q, so qa * (1 - 2^-20) <= q (tiny
-    // or NaN qa -> bound 0). Rounding is monotone, so with the bound qlb:
+    // Lower bound of q = (phi / 3) / dist_pos from one multiply: scale =
+    // (1/3)(1/dist_pos)(1 - 2^-20) in rounded steps, so phi * scale is within
+    // (1 - 2^-20)(1 + 2^-24)^5 of phi / (3 dist_pos), below q, which is within
+    // (1 - 2^-24)^2 of it, for normal values (tiny or NaN bound -> 0).
+    // Rounding is monotone, so with the bound qlb:
     // qlb >= tau_smooth means min(q, tau_smooth) == tau_smooth exactly, and
     // fma(c0, qlb, mp) >= the running minimum means the label cannot lower it.
     // Only the remaining labels need the exact divisions. Every label's phi
@@ -1076,6 +1078,7 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
     const float tau = c.tau_smooth;
     const float inv_dp = 1.0f / dist_pos;
     const float inv3 = 1.0f / 3.0f;
+    const float scale = inv3 * inv_dp * 0.99999905f; // 1 - 2^-20
     __shared__ float s_out[K][128];
     float sum = 0.f;
 #pragma unroll 1
@@ -1097,8 +1100,8 @@ __global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, St
 #pragma unroll
                 for (int i = 1; i < 6; ++i)
                     phi = phi + fabsf(__fmaf_rn(dx, X[i], __fmaf_rn(dy, Y[i], dz)));
-                const float qa = phi * inv3 * inv_dp;
-                const float qlb = qa >= 1e-30f ? qa * 0.99999905f : 0.0f; // 1 - 2^-20
+                const float qs = phi * scale;
+                const float qlb = qs >= 1e-30f ? qs : 0.0f;
                 float m;
                 if (qlb >= tau)
                     m = __fmaf_rn(c0, tau, mp[q]);
