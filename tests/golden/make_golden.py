@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|post_gpu]
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|post_gpu|lab_sweep]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -328,11 +328,31 @@ def post_gpu_record(ref: RefLib, golden_dir: str):
     return rec
 
 
+def all_colours() -> np.ndarray:
+    """A 4096x4096 BGR image holding every 24-bit colour once (key = B | G << 8 | R << 16)."""
+    c = np.arange(1 << 24, dtype=np.uint32)
+    return np.stack([c & 255, (c >> 8) & 255, c >> 16], axis=1).astype(np.uint8).reshape(4096, 4096, 3)
+
+
+def lab_sweep_record(ref: RefLib):
+    """The reference build's LAB of all 2^24 colours: its hash, and the colours where
+    the CPU oracle's LAB (the host's pow) differs, with the reference's values there
+    (the oracle takes them as overrides)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    O.set_lab_overrides(np.zeros(0, np.uint32), np.zeros((0, 3), np.float32))  # the plain host pow
+    img = all_colours()
+    lab = ref.lab(img)
+    mine = O.lab(img)
+    diff = np.nonzero(np.any(lab.view(np.uint32) != mine.view(np.uint32), axis=2).ravel())[0]
+    return dict(sha_lab_all=sha(lab), keys=diff.astype(np.uint32), vals=lab.reshape(-1, 4)[diff, :3].copy())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
-    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "post_gpu"], default=None)
+    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "post_gpu", "lab_sweep"], default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     ref = RefLib(args.lib)
@@ -358,7 +378,11 @@ def main():
         src = os.path.dirname(os.path.abspath(__file__))
         np.savez_compressed(os.path.join(args.out, "post_gpu.npz"), **post_gpu_record(ref, src))
         print("post_gpu")
-    if args.only in ("mccnn", "ad", "seg", "post_gpu"):
+    if args.only in (None, "lab_sweep"):
+        rec = lab_sweep_record(ref)
+        np.savez_compressed(os.path.join(args.out, "lab_overrides.npz"), **rec)
+        print("lab_sweep: colours where the host pow differs:", len(rec["keys"]))
+    if args.only in ("mccnn", "ad", "seg", "post_gpu", "lab_sweep"):
         return
 
     for (W, H, D, seed, full, name) in [

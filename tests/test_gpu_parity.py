@@ -263,3 +263,18 @@ def test_weighted_median_gpu_variant_vs_reference(eng, golden_dir, name):
     got = plane.cpu().numpy().reshape(H, W, 3)
     assert np.array_equal(got.view(np.uint32), f[name + "_plane"].view(np.uint32))
     assert np.array_equal(dout.cpu().numpy().reshape(H, W).view(np.uint32), f[name + "_disp"].view(np.uint32))
+
+
+def test_lab_every_colour(eng, golden_dir):
+    """The engine's LAB of all 2^24 colours equals the oracle's (with its pow
+    overrides) bit for bit, and hashes to the reference build's."""
+    import pyoracle as O
+    from make_golden import all_colours
+    E, ctx, torch = eng
+    img = all_colours()
+    out = torch.zeros(img.shape[0] * img.shape[1] * 4, dtype=torch.float32, device="cuda")
+    ctx.lab_d(dev(torch, img), img.shape[0] * img.shape[1], out)
+    torch.cuda.synchronize()
+    g = out.cpu().numpy().reshape(img.shape[0], img.shape[1], 4)
+    assert np.array_equal(g.view(np.uint32), O.lab(img).view(np.uint32))
+    assert sha(g) == str(load(golden_dir, "lab_overrides")["sha_lab_all"])
