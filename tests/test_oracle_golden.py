@@ -297,3 +297,14 @@ def test_lab_every_colour_matches_reference(golden_dir):
     z = load(golden_dir, "lab_overrides")
     assert len(z["keys"]) < 1000  # a handful of pow roundings, not a systematic difference
     assert sha(O.lab(all_colours())) == str(z["sha_lab_all"])
+
+
+def test_grey_u8_every_colour():
+    """The census grey (the reference's double sum stored as float, then
+    truncated, imutil.cu:116-168) equals the integer (114B + 587G + 299R) // 1000
+    for all 2^24 colours, the form the engine computes."""
+    from make_golden import all_colours
+    img = all_colours()
+    b = img.reshape(-1, 3).astype(np.int64)
+    want = np.minimum((114 * b[:, 0] + 587 * b[:, 1] + 299 * b[:, 2]) // 1000, 255).astype(np.uint8)
+    assert np.array_equal(O.grey_u8(img).ravel(), want)
