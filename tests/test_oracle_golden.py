@@ -308,3 +308,18 @@ def test_grey_u8_every_colour():
     b = img.reshape(-1, 3).astype(np.int64)
     want = np.minimum((114 * b[:, 0] + 587 * b[:, 1] + 299 * b[:, 2]) // 1000, 255).astype(np.uint8)
     assert np.array_equal(O.grey_u8(img).ravel(), want)
+
+
+def test_float_path_against_fp64():
+    """The float path (the engine's arithmetic, FP32 and FP16 messages)
+    against the FP64 oracle on a 160x120 scene: >= 99% of pixels within 1 px
+    and bad-2.0 within 0.1 percentage point. The residue is near-ties between
+    candidate planes that the two precisions resolve differently."""
+    from scenes import make_scene
+    s = make_scene(160, 120, 48, 11)
+    d64 = O.pipeline(s.left, s.right, 48, fp64=True)["disp"]
+    bad = lambda d: 100.0 * float(np.mean(np.abs(d - s.gt)[s.nonocc] > 2.0))
+    for kw in ({}, {"fp16_msg": True}):
+        d = O.pipeline(s.left, s.right, 48, **kw)["disp"]
+        assert np.mean(np.abs(d - d64) < 1.0) >= 0.99, kw
+        assert abs(bad(d) - bad(d64)) <= 0.1, kw
