@@ -40,3 +40,31 @@ def test_noalloc_rejects_before_touching_the_device(lib):
         E.driver_median_noalloc_d(None, 720, 496)
     assert L.hbp_driver_median_noalloc_d(C.c_void_p(16), 0, 10, None) == 1
     assert L.hbp_driver_median_noalloc_d(C.c_void_p(16), 2049, 1024, None) == 1
+
+
+def test_new_entry_points_reject_bad_arguments_on_the_host(lib):
+    """The MC-CNN, AD, segmentation-variant, per-level, median and pyramid entry
+    points check their arguments before any device work (no GPU needed)."""
+    E, L = lib
+    P = C.c_void_p
+    p16 = P(16)
+    INVALID = 1
+    f = C.c_float
+    assert L.hbp_volume_f32_bytes(720, 496, 128) == 4 * 720 * 496 * 128
+    assert L.hbp_volume_f32_bytes(0, 496, 128) == 0
+    # null context / pointers, tau <= 0, no output pair
+    assert L.hbp_cost_f32_d(None, p16, 64, 64, 16, f(0.5), p16, p16, None, None, None) == INVALID
+    assert L.hbp_cost_f32_d(p16, None, 64, 64, 16, f(0.5), p16, p16, None, None, None) == INVALID
+    assert L.hbp_cost_f32_d(p16, p16, 64, 64, 16, f(0.0), p16, p16, None, None, None) == INVALID
+    assert L.hbp_cost_f32_d(p16, p16, 64, 64, 16, f(0.5), None, None, None, None, None) == INVALID
+    assert L.hbp_cost_f32_d(p16, p16, 64, 64, 16, f(0.5), p16, None, None, None, None) == INVALID
+    assert L.hbp_cost_ad_d(None, p16, p16, 64, 64, 16, p16, p16, p16, p16, None, None, None) == INVALID
+    assert L.hbp_cost_ad_d(p16, p16, p16, 64, 64, 16, None, p16, p16, p16, None, None, None) == INVALID
+    assert L.hbp_infer_f32_d(None, p16, p16, 16, f(0.5), None, p16, None, None) == INVALID
+    assert L.hbp_infer_levels_d(None, p16, None, p16, 16, f(25.0), None, 8, p16, None, None, None) == INVALID
+    assert L.hbp_segment_cfg_d(None, p16, 64, 64, 2, 4, C.c_double(0.0), P(16), None) == INVALID
+    assert L.hbp_lab_sigma_d(None, p16, 64, 64, C.c_double(1.0), p16, None) == INVALID
+    assert L.hbp_weighted_median_gpu_d(None, p16, p16, p16, None, 64, 64, None) == INVALID
+    assert L.hbp_patch_weights_d(None, p16, None) == INVALID
+    ptrs = (P * 4)()
+    assert L.hbp_pyramid_device(None, ptrs, None, None, None) == INVALID
