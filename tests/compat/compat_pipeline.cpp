@@ -6,8 +6,9 @@
 //           weighted median, plane -> disparity)
 // with the Census and AD costs (alpha 1000.1) and, given an im0.acrt-style
 // volume file, the MC-CNN cost (alpha 1.3, bench_MiddV3_train.sh:6). Writes
-// <out_prefix>{census,ad,mccnn}_{single,lr,levels}.f32 (levels: every level's
-// disparity from HBP_ISP::run_ms_vis, top level first).
+// <out_prefix>{census,ad,mccnn}_{single,lr,lr_gpu,levels}.f32 (lr_gpu: the LR
+// flow with median_filter_gpu; levels: every level's disparity from
+// HBP_ISP::run_ms_vis, top level first).
 // usage: compat_pipeline left.bgr right.bgr W H D out_prefix [vol.acrt]
 #include <cstdio>
 #include <cstdlib>
@@ -76,6 +77,11 @@ static void flows(const Mat &L, const Mat &R, int D, const std::string &cost, co
     PostProcess *post = new PostProcess(L, R);
     post->left_right_check(results_left, results_right);
     post->plane_label_to_disp(results_left, results_right);
+    // the reference's GPU variant of the weighted median, on a copy
+    std::pair<Mat, Mat> gpu_left(results_left.first.clone(), results_left.second.clone());
+    post->median_filter_gpu(gpu_left, results_right);
+    post->plane_label_to_disp(gpu_left, results_right);
+    write_f32((out + "_lr_gpu.f32").c_str(), gpu_left.first);
     post->median_filter(results_left, results_right);
     post->plane_label_to_disp(results_left, results_right);
     write_f32((out + "_lr.f32").c_str(), results_left.first);

@@ -104,10 +104,28 @@ def test_driver_flows_match_the_engine(tmp_path):
         lv = torch.zeros((L - 2) * W * H, device="cuda")
         n = ctx.infer_levels_d(vol, None, wta, D, 25.0, E.default_params(), L - 2, lv)
         levels = lv.cpu().numpy().reshape(n, H, W)
+        # the Census LR flow with the GPU variant of the weighted median
+        n2 = W * H
+        f = lambda k=1: torch.zeros(k * n2, dtype=torch.float32, device="cuda")
+        dL, pL, dR, pR = f(), f(3), f(), f(3)
+        volR = torch.zeros(E.volume_bytes(W, H, D), dtype=torch.uint8, device="cuda")
+        wtaR = torch.zeros(W * H, device="cuda")
+        ctx.cost_census_d(cuda(s.left), cuda(s.right), W, H, D, cL, cR, vol, wta, volR, wtaR)
+        ctx.segment_d(cuda(s.left), W, H)
+        ctx.infer_d(vol, wta, D, E.default_params(), dL, pL)
+        ctx.segment_d(cuda(s.right), W, H)
+        ctx.infer_d(volR, wtaR, D, E.default_params(), dR, pR)
+        fail = torch.zeros(n2, dtype=torch.uint8, device="cuda")
+        dout = f()
+        ctx.lr_check_d(dL, dR, pL, fail, dout, W, H)
+        ctx.weighted_median_gpu_d(cuda(s.left), fail, pL, dout, W, H)
+        torch.cuda.synchronize()
+        lr_gpu = dout.cpu().numpy().reshape(H, W)
     finally:
         ctx.close()
     assert _same(out("census_single"), want1) and _same(out("census_lr"), want2)
     assert _same(out("census_levels"), levels)
+    assert _same(out("census_lr_gpu"), lr_gpu)
     assert _same(out("ad_single"), ad1) and _same(out("ad_lr"), ad2)
 
 
