@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(WM_T)
 }
 
 // PostProcess::median_filter_gpu (post_process.cu:188-371), the reference's
-// GPU variant of the weighted median: one block per failed pixel. Window
+// GPU variant of the weighted median: one warp per failed pixel. Window
 // samples in row-major order get the device patch weight wtab[sum|dBGR|]
 // (expf(-k / 10), launch_patch_weights) and z = fma(a, x, b * y) + c, the
 // reference device code's evaluation of a * x + b * y + c; the total weight
@@ -229,13 +229,16 @@ __global__ void __launch_bounds__(WM_T)
 // later sample smaller than the current one there. Its effect is a rotation
 // along the chain of strict running minima of [i, n): position i takes the
 // last of the chain, each chain member the previous one's sample, the first
-// member the old sample at i; position i is then final. Each step finds the
-// chain in parallel (per-thread chunk minima, an ordered scan of them, a walk
-// of each chunk) and applies the rotation; the running weight in float stops
-// the sort at the first sample past half the total, whose plane is taken.
-// NaN disparities never enter a chain, as NaN compares false there.
-constexpr int WG_T = 256, WG_MAXN = (2 * WM_R + 1) * (2 * WM_R + 1);
-constexpr int WG_MAXC = (WG_MAXN - 1 + WG_T - 1) / WG_T; // chunk length bound (7)
+// member the old sample at i; position i is then final. Each step cuts
+// [i+1, n) into 32 contiguous chunks (an odd chunk length keeps the lanes in
+// distinct shared-memory banks), finds the running minimum before each chunk
+// by an ordered scan of the chunk minima, reads the samples the chain hands
+// on across chunk borders, then lets each lane walk its chunk carrying the
+// previous chain member's sample. The running weight in float stops the sort
+// at the first sample past half the total, whose plane is taken. NaN
+// disparities never enter a chain, as NaN compares false there.
+constexpr int WG_MAXN = (2 * WM_R + 1) * (2 * WM_R + 1); // window samples (1681)
+constexpr int WG_W = 2;                                    // pixels (warps) per block
 
 // the earlier of two (z, pos) candidates unless the later is strictly smaller;
 // pos < 0: none
@@ -248,26 +251,27 @@ __device__ __forceinline__ void first_min(float &z, int &p, float z2, int p2)
     }
 }
 
-__global__ void __launch_bounds__(WG_T)
-    weighted_median_gpu_kernel(const uint8_t *__restrict__ bgr, const int *__restrict__ list, int W, int H,
-                               const float *__restrict__ plane_in, float *__restrict__ plane_out,
+__global__ void __launch_bounds__(32 * WG_W)
+    weighted_median_gpu_kernel(const uint8_t *__restrict__ bgr, const int *__restrict__ list, int nf, int W,
+                               int H, const float *__restrict__ plane_in, float *__restrict__ plane_out,
                                const float *__restrict__ wtab)
 {
-    __shared__ float zs[WG_MAXN], ws[WG_MAXN];
-    __shared__ int ids[WG_MAXN];
-    __shared__ float warp_z[WG_T / 32];
-    __shared__ int warp_p[WG_T / 32];
-    __shared__ float s_center;
-    __shared__ int s_pick;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int p = list[blockIdx.x];
+    __shared__ float zs_all[WG_W][WG_MAXN], ws_all[WG_W][WG_MAXN];
+    __shared__ int ids_all[WG_W][WG_MAXN];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * WG_W + wid;
+    if (item >= nf) // warp-uniform
+        return;
+    float *zs = zs_all[wid], *ws = ws_all[wid];
+    int *ids = ids_all[wid];
+    const int p = list[item];
     const int y = p / W, x = p - y * W;
     const int y0 = max(y - WM_R, 0), y1 = min(y + WM_R, H - 1);
     const int x0 = max(x - WM_R, 0), x1 = min(x + WM_R, W - 1);
     const int ww = x1 - x0 + 1, n = ww * (y1 - y0 + 1);
     const uint8_t *s = bgr + 3 * (size_t)p;
     const float fx = (float)x, fy = (float)y;
-    for (int j = tid; j < n; j += WG_T)
+    for (int j = lane; j < n; j += 32)
     {
         const int q = (y0 + j / ww) * W + x0 + j % ww;
         const uint8_t *t = bgr + 3 * (size_t)q;
@@ -277,24 +281,24 @@ __global__ void __launch_bounds__(WG_T)
         zs[j] = __fadd_rn(__fmaf_rn(pl[0], fx, __fmul_rn(pl[1], fy)), pl[2]);
         ids[j] = j;
     }
-    __syncthreads();
-    if (tid == 0)
+    __syncwarp();
+    float center = 0.f;
+    if (lane == 0)
     {
         float sum = 0.f;
         for (int j = 0; j < n; ++j)
             sum = __fadd_rn(sum, ws[j]);
-        s_center = __fdiv_rn(sum, 2.0f);
-        s_pick = -1;
+        center = __fdiv_rn(sum, 2.0f);
     }
-    float run = 0.f; // thread 0's running weight in sorted order
-    __syncthreads();
+    float run = 0.f; // lane 0's running weight in sorted order
+    int pick = -1;
     for (int i = 0; i < n; ++i)
     {
         const float zi = zs[i];
         const bool chain = zi == zi; // a NaN at i is never displaced
         const int m = n - i - 1;
-        const int c = (m + WG_T - 1) / WG_T;
-        const int lo = i + 1 + tid * c, hi = min(lo + c, n);
+        const int c = ((m + 31) >> 5) | 1;
+        const int lo = min(i + 1 + lane * c, n), hi = min(lo + c, n);
         // the chunk's first minimum (NaN samples never qualify)
         float cz = 0.f;
         int cp = -1;
@@ -304,8 +308,7 @@ __global__ void __launch_bounds__(WG_T)
             if (zj == zj)
                 first_min(cz, cp, zj, j);
         }
-        // ordered inclusive scan of the chunk minima: within the warp, then
-        // across warps through shared memory
+        // ordered inclusive scan of the chunk minima over the lanes
         float sz = cz;
         int sp = cp;
 #pragma unroll
@@ -322,91 +325,67 @@ __global__ void __launch_bounds__(WG_T)
                 sp = np;
             }
         }
-        if (lane == 31)
-        {
-            warp_z[wid] = sz;
-            warp_p[wid] = sp;
-        }
-        // exclusive prefix within the warp
-        float ez = __shfl_up_sync(0xffffffffu, sz, 1);
-        int ep = __shfl_up_sync(0xffffffffu, sp, 1);
-        if (lane == 0)
-            ep = -1;
-        __syncthreads();
-        // the sample at i, then the earlier warps, then the earlier lanes
-        float pz = zi;
+        float pz = zi; // the running minimum before this lane's chunk
         int pp = i;
-        for (int k = 0; k < wid; ++k)
-            first_min(pz, pp, warp_z[k], warp_p[k]);
-        first_min(pz, pp, ez, ep);
+        {
+            const float ez = __shfl_up_sync(0xffffffffu, sz, 1);
+            const int ep = __shfl_up_sync(0xffffffffu, sp, 1);
+            if (lane > 0)
+                first_min(pz, pp, ez, ep);
+        }
         float tz = zi; // the chain's end over the whole range
-        int tp = i;
-        for (int k = 0; k < WG_T / 32; ++k)
-            first_min(tz, tp, warp_z[k], warp_p[k]);
-        // walk the chunk: records j (z[j] below the running minimum) take the
-        // previous record's sample
-        int rj[WG_MAXC], rp[WG_MAXC];
-        int nr = 0;
+        int tpos = i;
+        first_min(tz, tpos, __shfl_sync(0xffffffffu, sz, 31), __shfl_sync(0xffffffffu, sp, 31));
+        // the samples handed on: the running minimum before the chunk, the
+        // chain's end (to position i) and the sample at i
+        float hz = zs[pp], hw = ws[pp];
+        int hi_ = ids[pp];
+        const float end_z = zs[tpos], end_w = ws[tpos];
+        const int end_i = ids[tpos];
+        const float wi = ws[i];
+        const int ii = ids[i];
+        __syncwarp();
         if (chain)
         {
+            float curz = pz;
             for (int j = lo; j < hi; ++j)
             {
                 const float zj = zs[j];
-                if (zj < pz)
+                if (zj < curz)
                 {
-                    rj[nr] = j;
-                    rp[nr] = pp;
-                    ++nr;
-                    pz = zj;
-                    pp = j;
+                    const float wj = ws[j];
+                    const int ij = ids[j];
+                    zs[j] = hz;
+                    ws[j] = hw;
+                    ids[j] = hi_;
+                    hz = zj;
+                    hw = wj;
+                    hi_ = ij;
+                    curz = zj;
                 }
             }
         }
-        float vz[WG_MAXC], vw[WG_MAXC];
-        int vi[WG_MAXC];
-#pragma unroll
-        for (int k = 0; k < WG_MAXC; ++k)
-            if (k < nr)
-            {
-                vz[k] = zs[rp[k]];
-                vw[k] = ws[rp[k]];
-                vi[k] = ids[rp[k]];
-            }
-        float nz = 0.f, nw = 0.f;
-        int ni = 0;
-        const bool moved = chain && tp != i;
-        if (tid == 0)
+        const bool moved = chain && tpos != i;
+        if (lane == 0)
         {
-            const int src = moved ? tp : i; // the sample that ends at position i
-            nz = zs[src];
-            nw = ws[src];
-            ni = ids[src];
-            run = __fadd_rn(run, nw);
-            if (run > s_center)
-                s_pick = ni;
+            if (moved)
+            {
+                zs[i] = end_z;
+                ws[i] = end_w;
+                ids[i] = end_i;
+            }
+            run = __fadd_rn(run, moved ? end_w : wi);
+            if (run > center)
+                pick = moved ? end_i : ii;
         }
-        __syncthreads();
-        if (s_pick >= 0)
+        pick = __shfl_sync(0xffffffffu, pick, 0);
+        __syncwarp();
+        if (pick >= 0)
             break;
-#pragma unroll
-        for (int k = 0; k < WG_MAXC; ++k)
-            if (k < nr)
-            {
-                zs[rj[k]] = vz[k];
-                ws[rj[k]] = vw[k];
-                ids[rj[k]] = vi[k];
-            }
-        if (tid == 0 && moved)
-        {
-            zs[i] = nz;
-            ws[i] = nw;
-            ids[i] = ni;
-        }
-        __syncthreads();
     }
-    if (tid == 0 && s_pick >= 0)
+    if (lane == 0 && pick >= 0)
     {
-        const int q = (y0 + s_pick / ww) * W + x0 + s_pick % ww;
+        const int q = (y0 + pick / ww) * W + x0 + pick % ww;
         plane_out[3 * (size_t)p] = plane_in[3 * (size_t)q];
         plane_out[3 * (size_t)p + 1] = plane_in[3 * (size_t)q + 1];
         plane_out[3 * (size_t)p + 2] = plane_in[3 * (size_t)q + 2];
@@ -505,7 +484,8 @@ void launch_weighted_median_gpu(const uint8_t *bgr, const uint8_t *fail, const f
     HBP_CUDA(cudaStreamSynchronize(st));
     if (nf > 0)
     {
-        weighted_median_gpu_kernel<<<nf, WG_T, 0, st>>>(bgr, list, W, H, plane_in, plane_out, wtab766);
+        weighted_median_gpu_kernel<<<ceil_div(nf, WG_W), 32 * WG_W, 0, st>>>(bgr, list, nf, W, H, plane_in,
+                                                                               plane_out, wtab766);
         note_launch();
         HBP_LAUNCH_CHECK();
     }
