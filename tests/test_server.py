@@ -47,6 +47,35 @@ def test_results_alone_and_in_a_mix_equal_run_pair(gpu, fp16):
 
 
 @pytest.mark.gpu
+def test_segmentation_variant_through_the_server(gpu):
+    """A server created with another SegHAC configuration (Ward linkage, 8
+    neighbours, pre-blur) returns hbp_run_pair's result with the same
+    parameters, bit for bit."""
+    E = gpu
+    from scenes import make_scene
+    prm = E.default_params(post=1, msg_fp16=1, linkage=3, num_nb=8, sigma=0.7)
+    s = make_scene(160, 120, 48, 31)
+    ctx = E.Context(0)
+    try:
+        want = ctx.run_pair(s.left, s.right, 48, prm)
+    finally:
+        ctx.close()
+    srv = E.Server(0, budget_bytes=8 << 30, prep_lanes=2, params=prm)
+    try:
+        got, _ = srv.wait(srv.submit(s.left, s.right, 48))
+    finally:
+        srv.close()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_server_rejects_a_bad_segmentation_configuration():
+    """The configuration is checked when the server is created (no GPU needed)."""
+    import hbp_b200 as E
+    with pytest.raises(E.HbpError):
+        E.Server(0, budget_bytes=1 << 30, prep_lanes=1, params=E.default_params(post=1, num_nb=6))
+
+
+@pytest.mark.gpu
 def test_admission_by_footprint(gpu):
     E = gpu
     from scenes import make_scene
