@@ -765,6 +765,27 @@ hbp_status hbp_weighted_median_gpu_d(hbp_ctx *c, const uint8_t *bgrL, const uint
     });
 }
 
+hbp_status hbp_check_bounded_wait(hbp_ctx *c, int *timed_out)
+{
+    if (!c || !timed_out)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        ensure_capacity(c, std::max<long>(c->cap_pixels, 1024), std::max(c->cap_disp, 16));
+        cudaStream_t st = c->st;
+        c->tmp.reset();
+        unsigned int *count2 = c->tmp.alloc<unsigned int>(2);
+        int *err = c->tmp.alloc<int>(1);
+        HBP_CUDA(cudaMemsetAsync(count2, 0, 2 * sizeof(unsigned int), st));
+        HBP_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+        launch_barrier_probe(count2, err, 200000, st); // ~50 ms of polls
+        int h = 0;
+        HBP_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        HBP_CUDA(cudaStreamSynchronize(st));
+        *timed_out = h == DERR_BARRIER_TIMEOUT ? 1 : 0;
+    });
+}
+
 hbp_status hbp_patch_weights_d(hbp_ctx *c, float *wtab766, void *stream)
 {
     if (!c || !wtab766)

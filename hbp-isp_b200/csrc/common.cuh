@@ -72,7 +72,9 @@ struct GridBarrier
     int *err;
 };
 
-__device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned int nblocks)
+constexpr long GRID_SPIN_LIMIT = 20000000; // ~ seconds with back-off
+
+__device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned int nblocks, long spin_limit = GRID_SPIN_LIMIT)
 {
     __syncthreads();
     __shared__ int ok;
@@ -92,7 +94,6 @@ __device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned int nblocks)
         else
         {
             long spins = 0;
-            const long spin_limit = 20000000; // ~ seconds with back-off
             while (*gen == g)
             {
                 if (++spins > spin_limit || *(volatile int *)b.err == DERR_BARRIER_TIMEOUT)

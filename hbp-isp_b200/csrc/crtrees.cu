@@ -280,4 +280,18 @@ void crtrees_labels(const int *nn, int N, int *clus, int *num_dev, int *err_dev,
     tmp.rewind(m);
 }
 
+// A bounded wait that nothing ends: one block waits at a grid barrier for a
+// second block that is never launched; after spin_limit polls the barrier
+// records DERR_BARRIER_TIMEOUT and the kernel returns (the check that a
+// device wait ends with a status instead of hanging).
+__global__ void barrier_probe_kernel(GridBarrier bar, long spin_limit) { grid_sync(bar, 2u, spin_limit); }
+
+void launch_barrier_probe(unsigned int *count2, int *err, long spin_limit, cudaStream_t st)
+{
+    GridBarrier b{count2, err};
+    barrier_probe_kernel<<<1, 32, 0, st>>>(b, spin_limit);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+}
+
 } // namespace hbp

@@ -103,6 +103,9 @@ void radix_sort_keys_u64(uint64_t *keys, uint64_t *keys_alt, long n, int bits, A
 // through num_dev (device int). err_dev receives DeviceErr codes.
 void crtrees_labels(const int *nn, int N, int *clus, int *num_dev, int *err_dev, Arena &tmp,
                     cudaStream_t st);
+// one block waiting at a grid barrier for a block that never comes, with the
+// given poll limit (the bounded-wait check)
+void launch_barrier_probe(unsigned int *count2, int *err, long spin_limit, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // Segmentation pyramid in the reference's ISP layout (segment.cu:884-905),

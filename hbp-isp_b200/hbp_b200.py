@@ -246,6 +246,11 @@ class Context:
     def weighted_median_gpu_d(self, bgrL, fail, plane, disp_out, W, H):
         _check(lib().hbp_weighted_median_gpu_d(self.h, _p(bgrL), _p(fail), _p(plane), _p(disp_out), W, H, None))
 
+    def check_bounded_wait(self) -> bool:
+        t = C.c_int(0)
+        _check(lib().hbp_check_bounded_wait(self.h, C.byref(t)))
+        return bool(t.value)
+
     def patch_weights_d(self, wtab766):
         _check(lib().hbp_patch_weights_d(self.h, _p(wtab766), None))
 

@@ -192,6 +192,12 @@ hbp_status hbp_weighted_median_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_
  * differ from the CPU variant's. */
 hbp_status hbp_weighted_median_gpu_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *fail,
                                      float *plane, float *disp_out, int W, int H, void *stream);
+/* A self-test with no counterpart in the reference: one block waits at the
+ * engine's grid barrier for a block that is never launched. Every device wait
+ * of the engine is bounded; this one runs out after ~50 ms, records a
+ * time-out in the device error word and returns, and *timed_out is set to 1.
+ * The context stays usable afterwards. */
+hbp_status hbp_check_bounded_wait(hbp_ctx *ctx, int *timed_out);
 /* The GPU variant's 766 patch weights expf(-k / 10), k = 0..765 (device
  * memory), as compute_patch_weight evaluates them (post_process.cu:199-213). */
 hbp_status hbp_patch_weights_d(hbp_ctx *ctx, float *wtab766, void *stream);
