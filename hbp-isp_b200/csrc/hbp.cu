@@ -974,7 +974,9 @@ __global__ void __launch_bounds__(128) k_init_nodes(const ViewDev *__restrict__ 
 
 // passing_msg_k + smooth_msg_k + normalize_msg_k (hbp_isp.cu:273-355), one
 // thread per edge
-__global__ void __launch_bounds__(128) k_edges(const ViewDev *__restrict__ V, StepDesc d)
+// 7 blocks per SM (72 registers): more warps to hide the issue stalls; measured
+// 4% faster than unconstrained (79 registers, 6 blocks), 1% than 8 blocks
+__global__ void __launch_bounds__(128, 7) k_edges(const ViewDev *__restrict__ V, StepDesc d)
 {
     int item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= d.pre[d.nt])
