@@ -278,3 +278,19 @@ def test_lab_every_colour(eng, golden_dir):
     g = out.cpu().numpy().reshape(img.shape[0], img.shape[1], 4)
     assert np.array_equal(g.view(np.uint32), O.lab(img).view(np.uint32))
     assert sha(g) == str(load(golden_dir, "lab_overrides")["sha_lab_all"])
+
+
+@pytest.mark.parametrize("W,H,D", [(16, 16, 2), (17, 19, 16), (33, 16, 8), (16, 47, 15), (64, 48, 24)])
+def test_tiny_pairs_bit_exact(eng, W, H, D):
+    """Edge sizes: the minimum image (16 x 16, D 2), D = W - 1, odd and ragged
+    tiles; the whole pair (both post modes) equals the oracle's pipeline."""
+    import pyoracle as O
+    from scenes import make_scene
+    E, ctx, torch = eng
+    s = make_scene(W, H, max(D, 16), 900 + W + H + D)  # the generator's smallest range is 16
+    got1 = ctx.run_pair(s.left, s.right, D, E.default_params(post=1))
+    want1 = O.driver_median(O.pipeline(s.left, s.right, D)["disp"])
+    assert np.array_equal(got1.view(np.uint32), want1.view(np.uint32))
+    got0 = ctx.run_pair(s.left, s.right, D, E.default_params(post=0))
+    want0 = O.pipeline(s.left, s.right, D)["disp"]
+    assert np.array_equal(got0.view(np.uint32), want0.view(np.uint32))
