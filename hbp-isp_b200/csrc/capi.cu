@@ -771,7 +771,7 @@ hbp_status hbp_check_bounded_wait(hbp_ctx *c, int *timed_out)
         return fail(HBP_ERR_INVALID_ARG, "null pointer");
     return guarded([&] {
         HBP_CUDA(cudaSetDevice(c->device));
-        ensure_capacity(c, std::max<long>(c->cap_pixels, 1024), std::max(c->cap_disp, 16));
+        ensure_capacity(c, std::max<long>(c->cap_pixels, 1), std::max(c->cap_disp, 16)); // keeps a pyramid
         cudaStream_t st = c->st;
         c->tmp.reset();
         unsigned int *count2 = c->tmp.alloc<unsigned int>(2);
