@@ -346,6 +346,8 @@ Lane *lane_at(hbp_ctx *c, int i)
 
 extern "C" {
 
+size_t hbp_params_size(void) { return sizeof(hbp_params); }
+
 void hbp_default_params(hbp_params *p)
 {
     if (!p)

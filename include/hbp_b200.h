@@ -62,6 +62,9 @@ typedef struct hbp_params
 } hbp_params;
 
 void hbp_default_params(hbp_params *p);
+/* sizeof(hbp_params) in this build, for bindings that declare the struct
+ * themselves (ctypes, cgo) to check their layout (no reference counterpart). */
+size_t hbp_params_size(void);
 const char *hbp_status_string(hbp_status s);
 const char *hbp_last_error(void);
 

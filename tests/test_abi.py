@@ -68,3 +68,13 @@ def test_new_entry_points_reject_bad_arguments_on_the_host(lib):
     assert L.hbp_patch_weights_d(None, p16, None) == INVALID
     ptrs = (P * 4)()
     assert L.hbp_pyramid_device(None, ptrs, None, None, None) == INVALID
+
+
+def test_params_layout_matches_the_binding(lib):
+    """The Python binding's hbp_params (the layout INTEGRATION.md's ctypes stub
+    shows) has the C struct's size, and the defaults are the reference's."""
+    E, L = lib
+    L.hbp_params_size.restype = C.c_size_t
+    assert C.sizeof(E.Params) == L.hbp_params_size()
+    p = E.default_params()
+    assert (p.linkage, p.num_nb, p.sigma, p.msg_fp16, p.post) == (2, 4, 0.0, 0, 1)
