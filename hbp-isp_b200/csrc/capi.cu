@@ -375,6 +375,7 @@ const char *hbp_status_string(hbp_status s)
     case HBP_ERR_TIMEOUT: return "timeout";
     case HBP_ERR_NOT_READY: return "not ready";
     case HBP_ERR_INTERNAL: return "internal error";
+    case HBP_ERR_CANCELLED: return "cancelled";
     }
     return "unknown status";
 }
@@ -1168,6 +1169,7 @@ struct hbp_server
     std::vector<std::unique_ptr<Lane>> lanes;
     std::vector<std::thread> threads;
     long long next_id = 1;
+    int preparing = 0; // requests a preparation lane has taken from to_prep
     bool stop = false;
     hbp_status fatal = HBP_OK;
     std::string fatal_msg;
@@ -1253,6 +1255,7 @@ struct hbp_server
                     return;
                 r = to_prep.front();
                 to_prep.pop_front();
+                ++preparing;
             }
             std::string msg;
             hbp_status st = guarded([&] {
@@ -1300,10 +1303,31 @@ struct hbp_server
             {
                 r->state = RQ_BP;
                 ready.push_back(r);
-                cv_sched.notify_one();
             }
+            --preparing;
+            // the scheduler waits for prepared requests, and at shutdown for
+            // the last preparation to end
+            cv_sched.notify_one();
         }
     }
+
+    // Fails every request that reached the scheduler (prepared, in BP or
+    // finishing) after a fatal error; requests still being prepared fail
+    // when their lane sees `fatal`. Caller holds mu.
+    void fail_scheduled_locked(hbp_status st, const std::string &msg)
+    {
+        ready.clear();
+        for (auto &kv : reqs)
+        {
+            const int q = kv.second->state;
+            if (q == RQ_BP || q == RQ_FINISHING)
+                finish_locked(kv.second.get(), st, msg);
+        }
+    }
+
+    // Nothing left for the scheduler: no prepared request waiting and none
+    // queued for or inside a preparation lane. Caller holds mu.
+    bool drained_locked() const { return ready.empty() && to_prep.empty() && preparing == 0; }
 
     void sched_loop()
     {
@@ -1318,6 +1342,7 @@ struct hbp_server
             std::lock_guard<std::mutex> lk(mu);
             fatal = pst;
             fatal_msg = g_err;
+            fail_scheduled_locked(fatal, fatal_msg);
             return;
         }
         auto active = [&] { return pool->active(); };
@@ -1328,9 +1353,11 @@ struct hbp_server
             std::vector<ServerReq *> join;
             {
                 std::unique_lock<std::mutex> lk(mu);
+                // at shutdown the scheduler stays until every admitted request
+                // has been prepared and run
                 if (!active() && finishing.empty())
-                    cv_sched.wait(lk, [&] { return stop || !ready.empty(); });
-                if (stop && !active() && finishing.empty() && ready.empty())
+                    cv_sched.wait(lk, [&] { return !ready.empty() || (stop && drained_locked()); });
+                if (stop && !active() && finishing.empty() && drained_locked())
                     return;
                 join.assign(ready.begin(), ready.end());
                 ready.clear();
@@ -1386,10 +1413,7 @@ struct hbp_server
                 std::lock_guard<std::mutex> lk(mu);
                 fatal = st;
                 fatal_msg = g_err;
-                for (auto &kv : reqs)
-                    if (kv.second->state != RQ_DONE && kv.second->state != RQ_QUEUED &&
-                        kv.second->state != RQ_PREPARING)
-                        finish_locked(kv.second.get(), st, fatal_msg);
+                fail_scheduled_locked(st, fatal_msg);
                 return;
             }
         }
@@ -1447,10 +1471,11 @@ void hbp_server_destroy(hbp_server *s)
         return;
     {
         std::unique_lock<std::mutex> lk(s->mu);
-        // finish what was admitted; drop what is still queued
+        // finish what was admitted; drop what is still queued (nobody can
+        // read their status: the server is freed below)
         for (ServerReq *r : s->queued)
         {
-            r->st = HBP_ERR_TIMEOUT;
+            r->st = HBP_ERR_CANCELLED;
             r->state = RQ_DONE;
         }
         s->queued.clear();

@@ -1,8 +1,9 @@
 // CRTrees: connected components of a directed 1-NN (functional) graph.
 //
-// Reference: CRTrees::get_clus (CRTrees.cu:395-434) with compute_in_degree,
+// Reference: CRTrees::get_clus (CRTrees.cu:315-354) with compute_in_degree,
 // check_larger_than_one, de_link_and_compute_mask, one_step_jump, re_link,
-// re_link_all, one_step_jump_max (:108-268) and compact_clus_label (:467-483).
+// re_link_all, one_step_jump_max (:28-187, driven by :207-312) and
+// compact_clus_label (:357-403).
 // The reference drives every pointer-jumping step from the host and reads a
 // flag back after each; here the whole procedure is one cooperative kernel
 // whose phases are separated by bounded grid barriers, so a call costs one
@@ -11,6 +12,8 @@
 // labels it produces are those of the reference (checked against the
 // reference build on random graphs and on every pyramid level).
 #include <cooperative_groups.h>
+
+#include <mutex>
 
 #include "engine.h"
 
@@ -222,23 +225,35 @@ __global__ void remap_labels(const int *label, const int *pos, int N, int *clus)
     }
 }
 
+// Grid size of the cooperative CRTrees launch on the current device: one
+// block per SM at most, which leaves room for concurrent lanes (each lane may
+// run its own cooperative CRTrees launch). Computed once per device; lanes on
+// several host threads may ask at the same time.
 int coop_blocks(int N)
 {
-    static int max_blocks = 0;
-    if (!max_blocks)
+    static std::mutex mu;
+    static int max_blocks[64] = {};
+    int dev;
+    HBP_CUDA(cudaGetDevice(&dev));
+    int mb;
     {
-        int dev, sms, per_sm = 0;
-        HBP_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu);
+        mb = dev >= 0 && dev < 64 ? max_blocks[dev] : 0;
+    }
+    if (!mb)
+    {
+        int sms, per_sm = 0;
         HBP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         HBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crtrees_kernel, CR_T, 0));
-        // one block per SM: leaves room for concurrent lanes (each lane may
-        // run its own cooperative CRTrees launch)
-        max_blocks = sms * (per_sm > 1 ? 1 : per_sm);
-        if (max_blocks < 1)
-            max_blocks = 1;
+        mb = sms * (per_sm > 1 ? 1 : per_sm);
+        if (mb < 1)
+            mb = 1;
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 64)
+            max_blocks[dev] = mb;
     }
     int want = ceil_div(N, CR_T * 4);
-    return want < 1 ? 1 : (want > max_blocks ? max_blocks : want);
+    return want < 1 ? 1 : (want > mb ? mb : want);
 }
 } // namespace
 

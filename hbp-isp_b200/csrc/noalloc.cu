@@ -99,6 +99,8 @@ float *static_scratch()
 
 void launch_driver_median_noalloc(float *disp, int W, int H, cudaStream_t st)
 {
+    if (W <= 0 || H <= 0)
+        throw StatusError{HBP_ERR_INVALID_ARG, "W and H must be positive"};
     const long n = (long)W * H;
     if (n > HBP_NOALLOC_MAX_PIXELS)
         throw StatusError{HBP_ERR_INVALID_ARG,

@@ -18,7 +18,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "hbp_b200.h")
 
 P = C.c_void_p
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "admission rejected", 4: "no convergence",
-          5: "CUDA error", 6: "timeout", 7: "not ready", 8: "internal error"}
+          5: "CUDA error", 6: "timeout", 7: "not ready", 8: "internal error", 9: "cancelled"}
 
 
 class EngineUnavailable(RuntimeError):

@@ -37,7 +37,8 @@ typedef enum hbp_status
     HBP_ERR_CUDA = 5,               /* CUDA runtime error */
     HBP_ERR_TIMEOUT = 6,            /* wait ended before the request finished */
     HBP_ERR_NOT_READY = 7,          /* poll: request still running */
-    HBP_ERR_INTERNAL = 8            /* invariant violated (capacity, ...) */
+    HBP_ERR_INTERNAL = 8,           /* invariant violated (capacity, ...) */
+    HBP_ERR_CANCELLED = 9           /* request dropped by hbp_server_destroy */
 } hbp_status;
 
 typedef struct hbp_ctx hbp_ctx;
@@ -119,7 +120,7 @@ hbp_status hbp_cost_ad_d(hbp_ctx *ctx, const uint8_t *bgrL, const uint8_t *bgrR,
 /* BGR -> CIELAB float4 (L, a, b, 1) (imutil.cu:4-40, segment.cu:795-809). */
 hbp_status hbp_lab_d(hbp_ctx *ctx, const uint8_t *bgr, long n, float *lab4, void *stream);
 
-/* CRTrees::get_clus + compact_clus_label (CRTrees.cu:395-434, :467-483):
+/* CRTrees::get_clus + compact_clus_label (CRTrees.cu:315-354, :387-403):
  * connected components of the successor array nn (every entry in [0, N)),
  * labelled 0..n-1; *num_clusters receives n. Synchronous. */
 hbp_status hbp_crtrees_d(hbp_ctx *ctx, const int *nn, int N, int *clus, int *num_clusters,
@@ -284,7 +285,11 @@ typedef struct hbp_server hbp_server;
 size_t hbp_request_bytes(int W, int H, int D);
 hbp_status hbp_server_create(int device, size_t budget_bytes, int prep_lanes, const hbp_params *prm,
                              hbp_server **out);
-/* Finishes the admitted requests, drops the queued ones, frees everything. */
+/* Finishes the admitted requests (writes their outputs), drops the ones
+ * still queued for memory, joins the server's threads and frees everything.
+ * The server and its request ids are invalid afterwards: hbp_poll and
+ * hbp_wait must not be called on it, so a caller that needs every result
+ * waits for its requests before destroying the server. */
 void hbp_server_destroy(hbp_server *srv);
 /* HBP_ERR_ADMISSION_REJECTED when the pair can never fit in the budget. */
 hbp_status hbp_submit(hbp_server *srv, const uint8_t *bgrL, const uint8_t *bgrR, int W, int H, int D,

@@ -20,7 +20,7 @@ int find(std::vector<int> &p, int x)
     return x;
 }
 
-// Canonical form of CRTrees::get_clus (CRTrees.cu:395-434). In a functional
+// Canonical form of CRTrees::get_clus (CRTrees.cu:315-354). In a functional
 // graph every weakly connected component holds exactly one cycle. The
 // reference de-links every node whose in-degree (counted from the still
 // active nodes) exceeds one, pointer-jumps the others onto those roots and
@@ -30,7 +30,7 @@ int find(std::vector<int> &p, int x)
 // component stops once its active set forms a cycle (no in-degree > 1 left);
 // a component that never had such a node is a plain cycle. Every node then
 // points straight at a node of that final cycle, and the max-pointer-jumping
-// of CRTrees.cu:249-268/354-378 labels the whole component with the largest
+// of CRTrees.cu:170-187/274-297 labels the whole component with the largest
 // node index on the final cycle.
 void crtrees_labels(const int *nn, int N, std::vector<int> &label)
 {
@@ -142,7 +142,7 @@ int compact_labels(std::vector<int> &label, int N)
 
 extern "C" {
 
-// CRTrees::get_clus + compact_clus_label (CRTrees.cu:395-434, :467-483):
+// CRTrees::get_clus + compact_clus_label (CRTrees.cu:315-354, :387-403):
 // component labels in 0..n-1, ordered by each component's label value.
 int orc_crtrees(const int *nn, int N, int *clus)
 {
@@ -153,9 +153,9 @@ int orc_crtrees(const int *nn, int N, int *clus)
     return k;
 }
 
-// Kernel-by-kernel simulation of CRTrees::get_clus (CRTrees.cu:28-434) with
+// Kernel-by-kernel simulation of CRTrees::get_clus (CRTrees.cu:28-354) with
 // the reference's ping-pong buffers, each kernel reading the state before it
-// (re_link's in-place reads, CRTrees.cu:97-120, take the pre-kernel value).
+// (re_link's in-place reads, CRTrees.cu:98-120, take the pre-kernel value).
 // Used only to cross-check orc_crtrees.
 int orc_crtrees_literal(const int *nn_in, int N, int *clus_out)
 {
@@ -225,7 +225,7 @@ int orc_crtrees_literal(const int *nn_in, int N, int *clus_out)
         C = nn;
     }
     nn = save;
-    // pointer_jumping_max (CRTrees.cu:354-378)
+    // pointer_jumping_max (CRTrees.cu:274-297)
     std::vector<int> M(C), K(N, 0);
     std::vector<int> *cn = &C, *on = &Nb, *cm = &M, *om = &K;
     bool flag = true;

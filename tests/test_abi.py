@@ -26,6 +26,8 @@ def test_host_only_entry_points(lib):
     p = E.default_params()
     assert abs(p.alpha - 1000.1) < 1e-3 and abs(p.tau_smooth - 0.6) < 1e-6 and p.min_level == 2
     assert L.hbp_status_string(0) == b"ok" and L.hbp_status_string(5) == b"CUDA error"
+    for code, name in E.STATUS.items():  # the binding's table is the library's
+        assert L.hbp_status_string(code) == name.encode(), code
     assert E.volume_bytes(720, 496, 128) == 720 * 496 * 128
     assert E.volume_bytes(17, 5, 3) == 3 * 2 * 3 * 32  # overhanging tiles are stored whole
     h = C.c_void_p()
@@ -71,8 +73,8 @@ def test_new_entry_points_reject_bad_arguments_on_the_host(lib):
 
 
 def test_params_layout_matches_the_binding(lib):
-    """The Python binding's hbp_params (the layout INTEGRATION.md's ctypes stub
-    shows) has the C struct's size, and the defaults are the reference's."""
+    """The Python binding's hbp_params (the layout a ctypes binding declares)
+    has the C struct's size, and the defaults are the reference's."""
     E, L = lib
     L.hbp_params_size.restype = C.c_size_t
     assert C.sizeof(E.Params) == L.hbp_params_size()

@@ -143,3 +143,27 @@ def test_device_memory_returns_after_contexts_and_servers(gpu):
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
     assert free0 - free1 < (64 << 20), (free0, free1)
+
+
+@pytest.mark.gpu
+def test_destroy_finishes_requests_still_in_preparation(gpu):
+    """hbp_server_destroy right after submitting: every admitted request,
+    including those a preparation lane has not yet finished (or started),
+    still runs to the end and writes its disparity, equal to hbp_run_pair's."""
+    E = gpu
+    from scenes import make_scene
+    prm = E.default_params(post=1)
+    scenes = [make_scene(160, 120, 48, 50 + i) for i in range(6)]
+    ctx = E.Context(0)
+    try:
+        want = [ctx.run_pair(s.left, s.right, 48, prm) for s in scenes]
+    finally:
+        ctx.close()
+    srv = E.Server(0, budget_bytes=8 << 30, prep_lanes=1, params=prm)  # all fit: none is dropped
+    ids = [srv.submit(s.left, s.right, 48) for s in scenes]
+    outs = [srv._live[i][2] for i in ids]
+    keep = dict(srv._live)  # the buffers must outlive the destroy
+    srv.close()
+    for o, w in zip(outs, want):
+        assert np.array_equal(o.view(np.uint32), w.view(np.uint32))
+    del keep
