@@ -28,6 +28,8 @@ int orc_crtrees(const int *nn, int N, int *clus);
 int orc_crtrees_literal(const int *nn, int N, int *clus);
 int orc_segment(const float *lab4, int W, int H, int max_levels, int *level_sizes, int *clus,
                 float *mean, int *bd, int *bdl);
+int orc_segment_target(const float *lab4, int W, int H, int link, int num_nb, int target, int max_levels,
+                       int *level_sizes, int *clus, float *mean, int *bd, int *bdl);
 int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int max_levels, int *level_sizes,
                     int *clus, float *mean, int *bd, int *bdl);
 
@@ -37,6 +39,9 @@ int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, c
             const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D,
             float alpha, float tau_smooth, int min_level, int mode, long max_steps, float *disp,
             float *plane, float *state_belief, float *state_plane);
+int orc_hbp_lockstep(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+                     const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
+                     float tau_smooth, int min_level, int mode, int shadow_fp64, float *disp, double *stats);
 int orc_hbp_levels(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
                    const int *bdl, const uint8_t *vol, const float *volf, const float *wta, int W, int H, int D,
                    float data_tau, float alpha, float tau_smooth, int min_level, int mode, float *disp_levels,

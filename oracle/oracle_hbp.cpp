@@ -26,8 +26,11 @@
 // Fused multiply-adds (the reference's nvcc build contracts these expressions,
 // in an order its output does not pin down; HBP agreement with it is the same
 // for every order tried): data cost d = fma(a, x, fma(b, y, c)) and
-// cost = fma(d + 1 - d_f, V[d], (d_f - d) * V[d+1]); smoothness point term
-// |fma(dx, X, fma(dy, Y, dz))| and message fma(c0, phi, msg).
+// cost = fma(d + 1 - d_f, V[d], (d_f - d) * V[d+1]); each plane's value at a
+// smoothness point fma(a, X, fma(b, Y, c)) and message fma(c0, phi, msg).
+// The smoothness term of two planes is sum_i |v_s,i - v_t,i| over the six
+// points (the reference evaluates the difference plane at each point,
+// hbp_isp.cu:339-344: the same quantity with other roundings).
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
@@ -68,7 +71,14 @@ struct Level
     std::vector<int> pid;     // 3 x N
 };
 
-template <typename R>
+// Lock-step shadow (shadow = true): a second copy of the continuous BP state
+// (costs, beliefs, messages) in type S, advanced with the main run's discrete
+// decisions: the same candidate planes (RANSAC points, spatial picks, random
+// adjustments) and the same kept slots (ranks of the main run's beliefs). The
+// shadow's messages are compared with the main run's at every BP step; with
+// S = double that is the main run's message error against FP64, with S = R
+// the shadow repeats the main run exactly (the replay's own check).
+template <typename R, typename S = double>
 struct Engine
 {
     int W, H, D, L;
@@ -84,42 +94,54 @@ struct Engine
     long steps = 0, max_steps = -1;
     bool stopped = false;
     bool fp16_msg = false; // messages stored as FP16 (float mode only)
+    bool shadow = false;
+    std::vector<std::vector<S>> sh_cost, sh_belief; // per level, K x N
+    std::vector<S> sh_msg, sh_msg_t;
+    // message error: shift-invariant (each message minus its own minimum, in
+    // both runs: a per-message constant moves every belief of a node alike and
+    // changes no decision) and raw (as stored, each run normalised by the mode)
+    double err_max = 0, err_sum = 0, ref_abs_sum = 0, ref_abs_max = 0, raw_max = 0, raw_sum = 0;
+    long err_n = 0;
 
-    R pixel_cost(int px, const P4<R> &pl) const
+    // read_plane_cost (hbp_isp.cu:205-227) of one pixel, evaluated in T
+    template <typename T>
+    T pixel_cost(int px, const P4<R> &pl) const
     {
-        R x = (R)(px % W), y = (R)(px / W);
-        R d_f = std::fma(pl.x, x, std::fma(pl.y, y, pl.z));
+        T x = (T)(px % W), y = (T)(px / W);
+        T d_f = std::fma((T)pl.x, x, std::fma((T)pl.y, y, (T)pl.z));
         int d = f2i_rd((float)d_f);
-        if (sizeof(R) == 8)
+        if (sizeof(T) == 8)
         {
             // FP64 mode: floor in double with the same NaN/saturation rules
             double v = (double)d_f;
             d = v != v ? 0 : (v >= 2147483648.0 ? 2147483647 : (v < -2147483648.0 ? (-2147483647 - 1) : (int)std::floor(v)));
         }
-        R cost;
+        T cost;
         if (d < 0 || d >= D - 1)
-            cost = tau;
+            cost = (T)tau;
         else
         {
             const size_t n = (size_t)W * H;
-            R v0, v1;
+            T v0, v1;
             if (volf)
             {
-                v0 = (R)volf[(size_t)d * n + px];
-                v1 = (R)volf[(size_t)(d + 1) * n + px];
+                v0 = (T)volf[(size_t)d * n + px];
+                v1 = (T)volf[(size_t)(d + 1) * n + px];
             }
             else
             {
-                v0 = (R)vol[(size_t)d * n + px];
-                v1 = (R)vol[(size_t)(d + 1) * n + px];
+                v0 = (T)vol[(size_t)d * n + px];
+                v1 = (T)vol[(size_t)(d + 1) * n + px];
             }
-            cost = std::fma((R)(d + 1) - d_f, v0, (d_f - (R)d) * v1);
+            cost = std::fma((T)(d + 1) - d_f, v0, (d_f - (T)d) * v1);
         }
-        return lambda * cost;
+        return (T)lambda * cost;
     }
 
-    // compute_plane_cost (hbp_isp.cu:1159-1174) for slots s_c .. s_c+3.
-    void plane_cost(Level<R> &l, int s_c)
+    // compute_plane_cost (hbp_isp.cu:1159-1174) for slots s_c .. s_c+3, in T,
+    // into out (K x N).
+    template <typename T>
+    void plane_cost_t(const Level<R> &l, int s_c, T *out) const
     {
 #pragma omp parallel for schedule(dynamic, 64)
         for (int n = 0; n < l.N; ++n)
@@ -129,21 +151,21 @@ struct Engine
             {
                 const P4<R> pl = l.plane[(size_t)(s_c + p) * l.N + n];
                 const int e = b + m;
-                R total = 0;
+                T total = 0;
                 for (int w256 = b / CHUNK; w256 <= (e - 1) / CHUNK; ++w256)
                 {
                     const int lo = std::max(b, w256 * CHUNK), hi = std::min(e, (w256 + 1) * CHUNK);
-                    R acc = 0;
+                    T acc = 0;
                     if (lo == w256 * CHUNK && hi == (w256 + 1) * CHUNK)
                     {
                         // the node fills the chunk: slot j sums positions
                         // j, j+32, ..., j+224 in order; xor butterfly
-                        R slots[32];
+                        T slots[32];
                         for (int j = 0; j < 32; ++j)
                         {
-                            R a = pixel_cost(l.pix[lo + j], pl);
+                            T a = pixel_cost<T>(l.pix[lo + j], pl);
                             for (int k = 1; k < CHUNK / 32; ++k)
-                                a = a + pixel_cost(l.pix[lo + j + 32 * k], pl);
+                                a = a + pixel_cost<T>(l.pix[lo + j + 32 * k], pl);
                             slots[j] = a;
                         }
                         acc = butterfly32(slots);
@@ -153,17 +175,25 @@ struct Engine
                     for (int w32 = lo / 32; w32 <= (hi - 1) / 32; ++w32)
                     {
                         const int l2 = std::max(lo, w32 * 32), h2 = std::min(hi, (w32 + 1) * 32);
-                        R x[32];
+                        T x[32];
                         for (int q = l2; q < h2; ++q)
-                            x[q - l2] = pixel_cost(l.pix[q], pl);
-                        const R piece = scan_last(x, h2 - l2);
+                            x[q - l2] = pixel_cost<T>(l.pix[q], pl);
+                        const T piece = scan_last(x, h2 - l2);
                         acc = w32 == lo / 32 ? piece : acc + piece;
                     }
                     total = w256 == b / CHUNK ? acc : total + acc;
                 }
-                l.cost[(size_t)(s_c + p) * l.N + n] = total;
+                out[(size_t)(s_c + p) * l.N + n] = total;
             }
         }
+    }
+    int level_of(const Level<R> &l) const { return (int)(&l - lv.data()); }
+    // the main run's costs of slots s_c .. s_c+3, and the shadow's
+    void plane_cost(Level<R> &l, int s_c)
+    {
+        plane_cost_t<R>(l, s_c, l.cost.data());
+        if (shadow)
+            plane_cost_t<S>(l, s_c, sh_cost[(size_t)level_of(l)].data());
     }
 
     // ransac_candidate_plane + make_three_diff_id + fit_plane_from_points
@@ -297,99 +327,209 @@ struct Engine
         }
     }
 
-    // belief_propagation (hbp_isp.cu:1206-1214, kernels :273-493).
-    void bp(Level<R> &l)
+    // passing_msg_k (hbp_isp.cu:292-304): msg = belief of the target - msg,
+    // for the 2P best and prior slots.
+    template <typename T>
+    void passing_t(const Level<R> &l, const T *belief, T *m) const
     {
         const int N = l.N, E = l.E;
-        // passing_msg_k
         for (int e = 0; e < E; ++e)
         {
             int t = l.bd[2 * (size_t)e + 1];
             for (int p = 0; p < 2 * P; ++p)
-                msg[(size_t)p * E + e] = l.belief[(size_t)p * N + t] - msg[(size_t)p * E + e];
+                m[(size_t)p * E + e] = belief[(size_t)p * N + t] - m[(size_t)p * E + e];
         }
-        // smooth_msg_k + normalize_msg_k
+    }
+
+    // smooth_msg_k + normalize_msg_k (hbp_isp.cu:273-290, :306-355) in T:
+    // msg_t[y][e] = sum over the two groups of min_p msg[p][e] + c0 * phi,
+    // normalised by the mean (min_norm = false) or by the minimum, then
+    // rounded to FP16 when fp16_store.
+    template <typename T>
+    void smooth_t(const Level<R> &l, const T *m_in, T *m_out, bool min_norm, bool fp16_store) const
+    {
+        const int N = l.N, E = l.E;
 #pragma omp parallel for schedule(static)
         for (int e = 0; e < E; ++e)
         {
             int s = l.bd[2 * (size_t)e], t = l.bd[2 * (size_t)e + 1];
             // the six points in a fixed order for both directions of an edge:
-            // the lower-index node's three, then the other's (the message of
-            // an edge and of its reverse then share each plane distance)
+            // the lower-index node's three, then the other's
             const int lo = std::min(s, t), hi = std::max(s, t);
-            R X[6], Y[6];
+            T X[6], Y[6];
             for (int i = 0; i < 3; ++i)
             {
                 int a = l.pid[3 * (size_t)lo + i], b = l.pid[3 * (size_t)hi + i];
-                X[i] = (R)(a % W);
-                Y[i] = (R)(a / W);
-                X[3 + i] = (R)(b % W);
-                Y[3 + i] = (R)(b / W);
+                X[i] = (T)(a % W);
+                Y[i] = (T)(a / W);
+                X[3 + i] = (T)(b % W);
+                Y[3 + i] = (T)(b / W);
             }
-            R dist_color = std::fmax(l.dc[e], (R)0.01f);
-            R dist_pos = std::fmax(l.dc[(size_t)E + e], (R)1.0f);
-            R c0 = dist_color * (R)l.bdl[e];
-            R out[K];
+            T dist_color = std::fmax((T)l.dc[e], (T)0.01f);
+            T dist_pos = std::fmax((T)l.dc[(size_t)E + e], (T)1.0f);
+            T c0 = dist_color * (T)l.bdl[e];
+            // each plane's value at the six points, v = fma(a, X, fma(b, Y, c));
+            // phi = sum_i |vs_i - vt_i| in point order
+            T vt[2 * P][6];
+            for (int p = 0; p < 2 * P; ++p)
+            {
+                const P4<R> pt = l.plane[(size_t)p * N + t];
+                for (int i = 0; i < 6; ++i)
+                    vt[p][i] = std::fma((T)pt.x, X[i], std::fma((T)pt.y, Y[i], (T)pt.z));
+            }
+            T out[K];
             for (int y = 0; y < K; ++y)
             {
-                P4<R> ps = l.plane[(size_t)y * N + s];
-                R acc = 0, mn = (R)FLT_MAX;
+                const P4<R> ps = l.plane[(size_t)y * N + s];
+                T vs[6];
+                for (int i = 0; i < 6; ++i)
+                    vs[i] = std::fma((T)ps.x, X[i], std::fma((T)ps.y, Y[i], (T)ps.z));
+                T acc = 0, mn = (T)FLT_MAX;
                 for (int p = 0; p < 2 * P; ++p)
                 {
                     if (p == P)
                     {
                         acc += mn;
-                        mn = (R)FLT_MAX;
+                        mn = (T)FLT_MAX;
                     }
-                    P4<R> pt = l.plane[(size_t)p * N + t];
-                    R dx = ps.x - pt.x, dy = ps.y - pt.y, dz = ps.z - pt.z;
-                    R phi = 0;
+                    T phi = 0;
                     for (int i = 0; i < 6; ++i)
                     {
-                        R term = std::fabs(std::fma(dx, X[i], std::fma(dy, Y[i], dz)));
+                        T term = std::fabs(vs[i] - vt[p][i]);
                         phi = i == 0 ? term : phi + term;
                     }
-                    phi = std::fmin(phi / (R)3 / dist_pos, tau_smooth);
-                    R m = std::fma(c0, phi, msg[(size_t)p * E + e]);
-                    if (m < mn)
-                        mn = m;
+                    phi = std::fmin(phi / (T)3 / dist_pos, (T)tau_smooth);
+                    T mm = std::fma(c0, phi, m_in[(size_t)p * E + e]);
+                    if (mm < mn)
+                        mn = mm;
                 }
                 acc += mn;
                 out[y] = acc;
             }
-            if (fp16_msg)
+            if (min_norm)
             {
-                // FP16 storage: minus the message's minimum, rounded to FP16
-                R mn = out[0];
+                // FP16 storage: minus the message's minimum (rounded to FP16)
+                T mn = out[0];
                 for (int k = 1; k < K; ++k)
                     if (out[k] < mn)
                         mn = out[k];
                 for (int k = 0; k < K; ++k)
-                    msg_t[(size_t)k * E + e] = (R)(float)(_Float16)(float)(out[k] - mn);
+                    m_out[(size_t)k * E + e] =
+                        fp16_store ? (T)(float)(_Float16)(float)(out[k] - mn) : out[k] - mn;
             }
             else
             {
-                R mean = 0;
+                T mean = 0;
                 for (int k = 0; k < K; ++k)
                     mean += out[k];
-                mean /= (R)K;
+                mean /= (T)K;
                 for (int k = 0; k < K; ++k)
-                    msg_t[(size_t)k * E + e] = out[k] - mean;
+                    m_out[(size_t)k * E + e] = out[k] - mean;
             }
         }
-        // aggregate_belief: belief = cost + out-edge messages in edge order
+    }
+
+    // aggregate_belief (hbp_isp.cu:1048-1058): belief = cost + out-edge
+    // messages in edge order.
+    template <typename T>
+    void aggregate_t(const Level<R> &l, const T *cost, const T *m_t, T *belief) const
+    {
+        const int N = l.N, E = l.E;
         for (int n = 0; n < N; ++n)
             for (int k = 0; k < K; ++k)
             {
-                R b = l.cost[(size_t)k * N + n];
+                T b = cost[(size_t)k * N + n];
                 for (int e = l.nb_off[n]; e < l.nb_off[n + 1]; ++e)
-                    b += msg_t[(size_t)k * E + e];
-                l.belief[(size_t)k * N + n] = b;
+                    b += m_t[(size_t)k * E + e];
+                belief[(size_t)k * N + n] = b;
             }
-        // ping_pang_msg_k
+    }
+
+    // ping_pang_msg_k (hbp_isp.cu:419-429): msg[rev e] = msg_t[e].
+    template <typename T>
+    void ping_pong_t(const Level<R> &l, const T *m_t, T *m) const
+    {
+        const int E = l.E;
         for (int e = 0; e < E; ++e)
             for (int k = 0; k < K; ++k)
-                msg[(size_t)k * E + l.rev[e]] = msg_t[(size_t)k * E + e];
+                m[(size_t)k * E + l.rev[e]] = m_t[(size_t)k * E + e];
+    }
+
+    // select_belief's compaction (hbp_isp.cu:452-472) of a K x N array by the
+    // ranks in `order`: slots ranked < P move to the front in slot order.
+    template <typename A>
+    void compact_nodes(const Level<R> &l, A *v) const
+    {
+        const int N = l.N;
+        for (int n = 0; n < N; ++n)
+        {
+            int nb = 0;
+            for (int k = 0; k < K; ++k)
+                if (order[(size_t)k * N + n] < P)
+                {
+                    v[(size_t)nb * N + n] = v[(size_t)k * N + n];
+                    nb++;
+                }
+        }
+    }
+
+    // select_msg (hbp_isp.cu:474-493): each edge's messages compacted by the
+    // kept slots of its target.
+    template <typename T>
+    void compact_msgs(const Level<R> &l, T *m) const
+    {
+        const int N = l.N, E = l.E;
+        for (int e = 0; e < E; ++e)
+        {
+            int t = l.bd[2 * (size_t)e + 1];
+            int nb = 0;
+            for (int k = 0; k < K; ++k)
+                if (order[(size_t)k * N + t] < P)
+                {
+                    m[(size_t)nb * E + e] = m[(size_t)k * E + e];
+                    nb++;
+                }
+        }
+    }
+
+    // belief_propagation (hbp_isp.cu:1206-1214, kernels :273-493), and the
+    // same step of the shadow with the main run's slot choices.
+    void bp(Level<R> &l)
+    {
+        const int N = l.N, E = l.E;
+        const size_t li = (size_t)level_of(l);
+        passing_t<R>(l, l.belief.data(), msg.data());
+        smooth_t<R>(l, msg.data(), msg_t.data(), fp16_msg, fp16_msg);
+        aggregate_t<R>(l, l.cost.data(), msg_t.data(), l.belief.data());
+        ping_pong_t<R>(l, msg_t.data(), msg.data());
+        if (shadow)
+        {
+            passing_t<S>(l, sh_belief[li].data(), sh_msg.data());
+            smooth_t<S>(l, sh_msg.data(), sh_msg_t.data(), fp16_msg, false);
+            for (int e = 0; e < E; ++e)
+            {
+                double mm = (double)msg_t[e], ms = (double)sh_msg_t[e];
+                for (int k = 1; k < K; ++k)
+                {
+                    mm = std::min(mm, (double)msg_t[(size_t)k * E + e]);
+                    ms = std::min(ms, (double)sh_msg_t[(size_t)k * E + e]);
+                }
+                for (int k = 0; k < K; ++k)
+                {
+                    const double a = (double)msg_t[(size_t)k * E + e], b = (double)sh_msg_t[(size_t)k * E + e];
+                    const double d = std::fabs((a - mm) - (b - ms)), r = std::fabs(a - b);
+                    err_max = d > err_max ? d : err_max;
+                    err_sum += d;
+                    raw_max = r > raw_max ? r : raw_max;
+                    raw_sum += r;
+                    ref_abs_sum += b - ms;
+                    ref_abs_max = b - ms > ref_abs_max ? b - ms : ref_abs_max;
+                }
+            }
+            err_n += (long)K * E;
+            aggregate_t<S>(l, sh_cost[li].data(), sh_msg_t.data(), sh_belief[li].data());
+            ping_pong_t<S>(l, sh_msg_t.data(), sh_msg.data());
+        }
         // get_belief_order + select_belief + select_msg
         for (int n = 0; n < N; ++n)
         {
@@ -402,29 +542,18 @@ struct Engine
                     else
                         ord[j]++;
                 }
-            int nb = 0;
             for (int k = 0; k < K; ++k)
-            {
                 order[(size_t)k * N + n] = ord[k];
-                if (ord[k] < P)
-                {
-                    l.plane[(size_t)nb * N + n] = l.plane[(size_t)k * N + n];
-                    l.cost[(size_t)nb * N + n] = l.cost[(size_t)k * N + n];
-                    l.belief[(size_t)nb * N + n] = l.belief[(size_t)k * N + n];
-                    nb++;
-                }
-            }
         }
-        for (int e = 0; e < E; ++e)
+        compact_nodes(l, l.plane.data());
+        compact_nodes(l, l.cost.data());
+        compact_nodes(l, l.belief.data());
+        compact_msgs<R>(l, msg.data());
+        if (shadow)
         {
-            int t = l.bd[2 * (size_t)e + 1];
-            int nb = 0;
-            for (int k = 0; k < K; ++k)
-                if (order[(size_t)k * N + t] < P)
-                {
-                    msg[(size_t)nb * E + e] = msg[(size_t)k * E + e];
-                    nb++;
-                }
+            compact_nodes(l, sh_cost[li].data());
+            compact_nodes(l, sh_belief[li].data());
+            compact_msgs<S>(l, sh_msg.data());
         }
     }
 
@@ -522,6 +651,18 @@ struct Engine
         s_ransac.assign(lv[0].N, 0);
         order.assign((size_t)K * lv[0].N, 0);
         plane_buf.assign((size_t)P * lv[0].N, P4<R>{0, 0, 0, 0});
+        if (shadow)
+        {
+            sh_cost.resize(L);
+            sh_belief.resize(L);
+            for (int li = 0; li < L; ++li)
+            {
+                sh_cost[li].assign((size_t)K * lv[li].N, 0);
+                sh_belief[li].assign((size_t)K * lv[li].N, 0);
+            }
+            sh_msg.assign((size_t)K * lv[0].E, 0);
+            sh_msg_t.assign((size_t)K * lv[0].E, 0);
+        }
     }
 
     bool step_done()
@@ -548,6 +689,11 @@ struct Engine
         plane_cost(l, 0);
         plane_cost(l, P);
         l.belief = l.cost;
+        if (shadow)
+        {
+            std::fill(sh_msg.begin(), sh_msg.begin() + (size_t)K * l.E, (S)0);
+            sh_belief[(size_t)li] = sh_cost[(size_t)li];
+        }
         for (int n = 0; n < l.N; ++n)
         {
             s_nb[n] = (uint32_t)l.nb_off[n];
@@ -585,16 +731,18 @@ struct Engine
     }
 };
 
-template <typename R>
+template <typename R, typename S = double>
 int run(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
         const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
         float tau_smooth, int min_level, long max_steps, float *disp, float *plane_out,
         float *state_belief, float *state_plane, bool fp16_msg = false, const float *volf = nullptr,
-        float data_tau = 25.0f, float *disp_levels = nullptr, float *plane_levels = nullptr)
+        float data_tau = 25.0f, float *disp_levels = nullptr, float *plane_levels = nullptr,
+        double *shadow_stats = nullptr)
 {
     if (L < 1 || min_level < 0 || min_level > L - 1)
         return -1;
-    Engine<R> eng;
+    Engine<R, S> eng;
+    eng.shadow = shadow_stats != nullptr;
     eng.W = W;
     eng.H = H;
     eng.D = D;
@@ -611,7 +759,7 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
     // map_msg (hbp_isp.cu:1081-1105) of level li: first slot among 0..3
     // holding the minimum belief; per pixel d = clamp(a*x + b*y + c, 0, D-1).
     auto map_level = [&](int li, float *d_out, float *p_out) {
-        const Level<R> &l = eng.lv[li];
+        const auto &l = eng.lv[li];
         std::vector<P4<R>> best(l.N);
         for (int n = 0; n < l.N; ++n)
         {
@@ -666,7 +814,7 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
         }
         keep_level(li);
     }
-    Level<R> &l = eng.lv[lm];
+    const auto &l = eng.lv[lm];
     if (state_belief)
         for (size_t i = 0; i < (size_t)K * l.N; ++i)
             state_belief[i] = (float)l.belief[i];
@@ -679,6 +827,17 @@ int run(const int *level_sizes, int L, const int *clus, const float *mean, const
             state_plane[4 * i + 3] = (float)l.plane[i].w;
         }
     map_level(lm, disp, plane_out);
+    if (shadow_stats)
+    {
+        const double n = eng.err_n ? (double)eng.err_n : 1.0;
+        shadow_stats[0] = eng.err_max;
+        shadow_stats[1] = eng.err_sum / n;
+        shadow_stats[2] = eng.ref_abs_sum / n;
+        shadow_stats[3] = (double)eng.err_n;
+        shadow_stats[4] = eng.raw_max;
+        shadow_stats[5] = eng.raw_sum / n;
+        shadow_stats[6] = eng.ref_abs_max;
+    }
     return (int)eng.steps;
 }
 } // namespace
@@ -716,6 +875,33 @@ int orc_hbp(const int *level_sizes, int L, const int *clus, const float *mean, c
                            state_plane);
     return run<float>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth,
                       min_level, max_steps, disp, plane, state_belief, state_plane);
+}
+
+// Lock-step message error of the float run (mode 0: FP32 messages; 2: FP16
+// storage), the engine's arithmetic, against a shadow run that takes the
+// same discrete decisions (candidate planes, kept slots) and carries its own
+// costs, beliefs and messages in double (shadow_fp64 = 1) or in float
+// (shadow_fp64 = 0: the shadow repeats the float run, so every error is 0).
+// The shadow normalises like the mode (mean for FP32, minimum for FP16) and
+// stores unrounded. Over every message value of every BP step, with each
+// message taken minus its own minimum in both runs: stats[0] the max and
+// stats[1] the mean of |msg - msg_shadow|, stats[2] the mean and stats[6]
+// the max of the shadow's values; stats[3] the count; stats[4] / [5] the max
+// and mean of the raw difference (each run's stored normalisation). disp as
+// orc_hbp. Returns the BP steps.
+int orc_hbp_lockstep(const int *level_sizes, int L, const int *clus, const float *mean, const int *bd,
+                     const int *bdl, const uint8_t *vol, const float *wta, int W, int H, int D, float alpha,
+                     float tau_smooth, int min_level, int mode, int shadow_fp64, float *disp, double *stats)
+{
+    if (!stats || (mode != 0 && mode != 2))
+        return -1;
+    if (shadow_fp64)
+        return run<float, double>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth,
+                                  min_level, -1, disp, nullptr, nullptr, nullptr, mode == 2, nullptr, 25.0f,
+                                  nullptr, nullptr, stats);
+    return run<float, float>(level_sizes, L, clus, mean, bd, bdl, vol, wta, W, H, D, alpha, tau_smooth,
+                             min_level, -1, disp, nullptr, nullptr, nullptr, mode == 2, nullptr, 25.0f, nullptr,
+                             nullptr, stats);
 }
 
 // The same on a float cost volume [D][H*W] (the MC-CNN path,

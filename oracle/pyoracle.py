@@ -39,10 +39,14 @@ def lib():
         _lib.orc_crtrees_literal.restype = C.c_int
         _lib.orc_segment.restype = C.c_int
         _lib.orc_segment_cfg.restype = C.c_int
+        _lib.orc_segment_target.restype = C.c_int
         _lib.orc_lab_sigma.argtypes = [P, C.c_int, C.c_int, C.c_double, P]
         _lib.orc_hbp.restype = C.c_int
         _lib.orc_hbp.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
                                  C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
+        _lib.orc_hbp_lockstep.restype = C.c_int
+        _lib.orc_hbp_lockstep.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
+                                          C.c_float, C.c_int, C.c_int, C.c_int, P, P]
         _lib.orc_hbp_f32.restype = C.c_int
         _lib.orc_hbp_f32.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
                                      C.c_float, C.c_float, C.c_int, C.c_int, C.c_long, P, P, P, P]
@@ -162,6 +166,33 @@ def segment(lab4: np.ndarray, link: int = 2, num_nb: int = 4) -> dict:
     return dict(level_sizes=sizes, clus=clus[:tc], mean=mean[: 6 * tc], bd=bd[: 2 * tb].reshape(tb, 2), bdl=bdl[:tb])
 
 
+def segment_target(lab4: np.ndarray, target: int, link: int = 2, num_nb: int = 4) -> dict:
+    """SegHAC with target_clus (the superpixel mode): the pyramid up to the
+    level whose clus maps onto exactly `target` superpixels, and the label
+    image (each pixel's superpixel)."""
+    H, W = lab4.shape[:2]
+    N0 = W * H
+    sizes = np.zeros((64, 2), np.int32)
+    clus = np.zeros(2 * N0, np.int32)
+    mean = np.zeros(12 * N0, np.float32)
+    bd = np.zeros((4 * num_nb * N0,), np.int32)
+    bdl = np.zeros(2 * num_nb * N0, np.int32)
+    L = lib().orc_segment_target(_p(np.ascontiguousarray(lab4, np.float32)), W, H, link, num_nb, target, 64,
+                                 _p(sizes), _p(clus), _p(mean), _p(bd), _p(bdl))
+    if L < 1:
+        raise ValueError("oracle segmentation rejected its input")
+    sizes = sizes[:L].copy()
+    tn, te = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
+    labels = np.arange(N0, dtype=np.int64)
+    off = 0
+    for l in range(L):
+        labels = clus[off + labels]
+        off += int(sizes[l, 0])
+    return dict(level_sizes=sizes, clus=clus[:tn].copy(), mean=mean[:6 * tn].copy(),
+                bd=bd[:2 * te].reshape(te, 2).copy(), bdl=bdl[:te].copy(),
+                labels=labels.astype(np.int32).reshape(H, W))
+
+
 def round_fp16(x: np.ndarray) -> np.ndarray:
     """The oracle's FP16 store: nearest FP16 value, back to float32."""
     x = np.ascontiguousarray(x, np.float32)
@@ -192,6 +223,43 @@ def hbp(seg: dict, vol, wta, W, H, D, alpha=1000.1, tau_smooth=0.6, min_level=2,
     if steps < 0:
         raise ValueError("oracle hbp rejected its input")
     return disp, plane, steps, sb, sp
+
+
+def hbp_lockstep(seg: dict, vol, wta, W, H, D, fp16_msg=False, shadow_fp64=True, alpha=1000.1,
+                 tau_smooth=0.6, min_level=2):
+    """The float run (the engine's arithmetic; FP16 message storage with
+    fp16_msg) with a lock-step shadow that takes the same candidate planes
+    and kept slots but carries costs, beliefs and messages in FP64
+    (shadow_fp64=False: in float, which must repeat the run exactly).
+    Returns (disparity, stats): over every message value of every BP step,
+    each message minus its own minimum in both runs (a per-message constant
+    changes no decision), msg_err_max / msg_err_mean of the difference and
+    msg_ref_mean / msg_ref_max of the FP64 values; msg_raw_err_max / _mean of
+    the stored values (each run normalised by its mode); values compared."""
+    sizes = np.ascontiguousarray(seg["level_sizes"], np.int32)
+    L = sizes.shape[0]
+    disp = np.zeros((H, W), np.float32)
+    st = np.zeros(7, np.float64)
+    mean = np.ascontiguousarray(seg["mean"], np.float32).copy()
+    steps = lib().orc_hbp_lockstep(_p(sizes), L, _p(np.ascontiguousarray(seg["clus"], np.int32)), _p(mean),
+                                   _p(np.ascontiguousarray(seg["bd"], np.int32)),
+                                   _p(np.ascontiguousarray(seg["bdl"], np.int32)),
+                                   _p(np.ascontiguousarray(vol, np.uint8)),
+                                   _p(np.ascontiguousarray(wta, np.float32)), W, H, D, alpha, tau_smooth,
+                                   min_level, 2 if fp16_msg else 0, int(shadow_fp64), _p(disp), _p(st))
+    if steps < 0:
+        raise ValueError("oracle lock-step rejected its input")
+    return disp, {"msg_err_max": float(st[0]), "msg_err_mean": float(st[1]), "msg_ref_mean": float(st[2]),
+                  "msg_ref_max": float(st[6]), "msg_raw_err_max": float(st[4]),
+                  "msg_raw_err_mean": float(st[5]), "values": int(st[3]), "steps": int(steps)}
+
+
+def pipeline_lockstep(L, R, D, fp16_msg=False, shadow_fp64=True):
+    """pipeline() with the lock-step FP64 shadow of hbp_lockstep."""
+    H, W = L.shape[:2]
+    cs = cost_stage(L, R, D)
+    seg = segment(lab(L))
+    return hbp_lockstep(seg, cs["vol"], cs["wta"], W, H, D, fp16_msg, shadow_fp64)
 
 
 def lr_check(dispL, dispR, planeL):
