@@ -59,6 +59,10 @@ struct LevelDev
     unsigned long long *keep; // N: kept slots (count | 4-bit indices)
 };
 
+#ifndef PAIR_VOLUME
+#define PAIR_VOLUME 1
+#endif
+
 struct Common
 {
     int W, H, D, TX; // TX: volume tiles per row
@@ -66,6 +70,10 @@ struct Common
     const uint8_t *vol; // tiled, vol_offset() (Census: uint8 costs)
     const float *volf;  // or the same layout in floats (MC-CNN); null for uint8
     const float *wta;   // HW
+    // Census: the data cost's copy of vol in which entry (x, y, d) holds the
+    // two costs one interpolation reads, V[d] | V[d+1] << 8 (same tiling,
+    // 16-bit entries), so that a pixel and plane take one load
+    const uint16_t *vol2;
 };
 
 __device__ __forceinline__ int px_x(uint32_t xy) { return (int)(xy & 0xffffu); }
@@ -103,9 +111,15 @@ __device__ __forceinline__ float pixel_cost(const Common &c, float xf, float yf,
         }
         else
         {
+#if PAIR_VOLUME
+            const uint32_t w = c.vol2[base + (size_t)d * VT_BYTES];
+            v0 = byte_to_float(w & 0xffu);
+            v1 = byte_to_float(w >> 8);
+#else
             const uint8_t *pv = c.vol + base + (size_t)d * VT_BYTES;
             v0 = byte_to_float(pv[0]);
             v1 = byte_to_float(pv[VT_BYTES]);
+#endif
         }
         const float fd = (float)d;
         cost = __fmaf_rn((fd + 1.0f) - d_f, v0, (d_f - fd) * v1);
@@ -130,6 +144,20 @@ __global__ void compose_im_clus(const int *im, const int *clus, int n, int *out)
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         out[i] = clus[im[i]];
+}
+
+// The pair volume of Common::vol2: entry i holds vol[i] | vol[i + 32] << 8
+// (the next disparity of the same pixel); the last disparity's entry holds
+// vol[i] alone (never read: the data cost takes tau for d >= D - 1).
+__global__ void pair_volume(const uint8_t *__restrict__ vol, long n, int D, uint16_t *__restrict__ vol2)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int d = (int)((i / VT_BYTES) % D);
+    const uint32_t lo = vol[i];
+    const uint32_t hi = d + 1 < D ? vol[i + VT_BYTES] : 0u;
+    vol2[i] = (uint16_t)(lo | hi << 8);
 }
 
 __global__ void iota_int(int *v, int n)
@@ -933,7 +961,10 @@ __device__ __forceinline__ void cost_window(const StepDesc &d, int mode, int ite
         emit_chunk(l, pc, carry_n, win, carry);
 }
 
-__global__ void __launch_bounds__(256, 4) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
+#ifndef COST_MIN_BLOCKS
+#define COST_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, COST_MIN_BLOCKS) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
 {
     const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -973,10 +1004,12 @@ __global__ void __launch_bounds__(128) k_init_nodes(const ViewDev *__restrict__ 
 }
 
 // passing_msg_k + smooth_msg_k + normalize_msg_k (hbp_isp.cu:273-355), one
-// thread per edge
-// 7 blocks per SM (72 registers): more warps to hide the issue stalls; measured
-// 4% faster than unconstrained (79 registers, 6 blocks), 1% than 8 blocks
-__global__ void __launch_bounds__(128, 7) k_edges(const ViewDev *__restrict__ V, StepDesc d)
+// thread per edge. Blocks per SM: the target labels' point values take 48
+// registers; EDGES_MIN_BLOCKS bounds the register count.
+#ifndef EDGES_MIN_BLOCKS
+#define EDGES_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(128, EDGES_MIN_BLOCKS) k_edges(const ViewDev *__restrict__ V, StepDesc d)
 {
     int item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= d.pre[d.nt])
@@ -1067,6 +1100,16 @@ __global__ void __launch_bounds__(128, 7) k_edges(const ViewDev *__restrict__ V,
         cswap(1, 3);
         cswap(1, 2);
     }
+    // Each target label's plane evaluated at the six points once per edge:
+    // phi(y, q) = sum_i |vs_y,i - vt_q,i| with v = fma(a, X_i, fma(b, Y_i, c)),
+    // two subtractions per point instead of the difference plane's two
+    // multiply-adds (the oracle restates this form).
+    float vt[2 * P][6];
+#pragma unroll
+    for (int p = 0; p < 2 * P; ++p)
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+            vt[p][i] = __fmaf_rn(pt[p].x, X[i], __fmaf_rn(pt[p].y, Y[i], pt[p].z));
     // Lower bound of q = (phi / 3) / dist_pos from one multiply: scale =
     // (1/3)(1/dist_pos)(1 - 2^-20) in rounded steps, so phi * scale is within
     // (1 - 2^-20)(1 + 2^-24)^5 of phi / (3 dist_pos), below q, which is within
@@ -1087,6 +1130,10 @@ __global__ void __launch_bounds__(128, 7) k_edges(const ViewDev *__restrict__ V,
     for (int y = 0; y < K; ++y)
     {
         const float4 ps = l.plane[(size_t)st.x * K + y];
+        float vs[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+            vs[i] = __fmaf_rn(ps.x, X[i], __fmaf_rn(ps.y, Y[i], ps.z));
         float acc = 0.f;
 #pragma unroll
         for (int g = 0; g < 2; ++g)
@@ -1096,12 +1143,10 @@ __global__ void __launch_bounds__(128, 7) k_edges(const ViewDev *__restrict__ V,
             for (int k = 0; k < P; ++k)
             {
                 const int q = g * P + k;
-                const float4 tp = pt[q];
-                float dx = ps.x - tp.x, dy = ps.y - tp.y, dz = ps.z - tp.z;
-                float phi = fabsf(__fmaf_rn(dx, X[0], __fmaf_rn(dy, Y[0], dz)));
+                float phi = fabsf(vs[0] - vt[q][0]);
 #pragma unroll
                 for (int i = 1; i < 6; ++i)
-                    phi = phi + fabsf(__fmaf_rn(dx, X[i], __fmaf_rn(dy, Y[i], dz)));
+                    phi = phi + fabsf(vs[i] - vt[q][i]);
                 const float qs = phi * scale;
                 const float qlb = qs >= 1e-30f ? qs : 0.0f;
                 float m;
@@ -1236,7 +1281,18 @@ void hbp_prepare(const Pyramid &pyr, const CostVolume &cv, const float *wta, int
     if ((int)pyr.N.size() != L || (int)pyr.E.size() != L || (int)pyr.node_off.size() != L ||
         (int)pyr.edge_off.size() != L || (int)pyr.child_base.size() != L || (int)pyr.nb_base.size() != L)
         throw StatusError{HBP_ERR_INTERNAL, "pyramid bookkeeping inconsistent"};
-    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, cv.tau, prm.tau_smooth, cv.u8, cv.f32, wta};
+    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, cv.tau, prm.tau_smooth, cv.u8, cv.f32, wta, nullptr};
+#if PAIR_VOLUME
+    if (cv.u8)
+    {
+        const long nv = (long)volume_bytes(W, H, D);
+        uint16_t *vol2 = persist.alloc<uint16_t>((size_t)nv);
+        pair_volume<<<blocks(nv, 256), 256, 0, st>>>(cv.u8, nv, D, vol2);
+        note_launch();
+        HBP_LAUNCH_CHECK();
+        c.vol2 = vol2;
+    }
+#endif
     std::vector<LevelDev> &lv = vp.impl->lv;
     lv.assign(L, LevelDev{});
     vp.L = L;
@@ -1666,9 +1722,30 @@ void BpScheduler::tick(std::vector<void *> &finished)
         prof->launches += (long)((tc.size() + MAXV - 1) / MAXV);
     }
     I.launch(vc, tc, CNT_EDGES, [&](const StepDesc &d) {
-        run(5, lvl_c, [&] { k_edges<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d); });
+        run(5, lvl_c, [&] {
+            if (tp)
+                prof->edges.mark(st);
+            k_edges<<<blocks(d.pre[d.nt], 128), 128, 0, st>>>(nullptr, d);
+            if (tp)
+                prof->edges.mark(st);
+        });
         note_launch();
     });
+    if (tp)
+    {
+        // compulsory bytes of the timed edge-message launches: per directed
+        // edge its metadata (bd 8 B, bdl 4, dc 8, rev 4) and the 12 stored
+        // message values read (the reverse edge's) and written; per node of
+        // the level its 12 planes, 8 beliefs, RANSAC points and kept slots
+        for (const View *v : vc)
+        {
+            const double E = v->vp->levelE[v->li], N = v->vp->levelN[v->li];
+            const double bm = I.prm.msg_fp16 ? 2.0 : 4.0;
+            prof->edges.bytes += E * (24.0 + 2.0 * K * bm) + N * (K * 16.0 + 2 * P * 4.0 + 16.0 + 8.0);
+            prof->edges.units += E;
+        }
+        prof->edges.launches += (long)((tc.size() + MAXV - 1) / MAXV);
+    }
     // MAP at min_level
     if (!vm.empty())
     {
