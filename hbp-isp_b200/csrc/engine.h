@@ -141,11 +141,17 @@ struct SegConfig
     int link = LINK_CENTROID;
     int num_nb = 4;
     double sigma = 0.0;
+    int target = 1; // target_clus: 1 = the whole pyramid; > 1 stops at that many superpixels
 };
 // Rejects configurations the reference cannot run (HBP_ERR_INVALID_ARG).
 void check_seg_config(const SegConfig &cfg);
+struct Pyramid;
+// Each pixel's cluster at the pyramid's last level (LabelIntFormat), and the
+// number of those clusters.
+void launch_top_labels(const Pyramid &pyr, int *labels, Arena &tmp, cudaStream_t st);
+int top_cluster_count(const Pyramid &pyr, Arena &tmp, cudaStream_t st);
 
-// segment.cu: SegHAC::run_ms with LabelISPFormat and target 1. Uses `a` for
+// segment.cu: SegHAC::run_ms with LabelISPFormat and cfg.target. Uses `a` for
 // the pyramid and `tmp` for temporaries; the host learns each level's size
 // (one small device-to-host read per level).
 void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
@@ -153,10 +159,58 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
 
 // ---------------------------------------------------------------------------
 // hbp.cu
-// Event timing of the data-cost kernel (the dominant kernel) for the
-// roofline report: every launch is bracketed by events while enabled.
+// Event timing for the roofline report: while enabled, the data-cost and the
+// edge-message launches of every 16th BP tick of the first BP stream are
+// bracketed by events.
+struct EventTimer
+{
+    std::vector<cudaEvent_t> ev; // start/stop pairs, reused
+    size_t used = 0;
+    double bytes = 0; // algorithmic bytes of the timed launches
+    double units = 0; // edges (or list positions) the timed launches covered
+    long launches = 0;
+    void reset()
+    {
+        used = 0;
+        bytes = 0;
+        units = 0;
+        launches = 0;
+    }
+    void mark(cudaStream_t st)
+    {
+        if (used == ev.size())
+        {
+            cudaEvent_t e;
+            HBP_CUDA(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+        HBP_CUDA(cudaEventRecord(ev[used++], st));
+    }
+    double total_ms()
+    {
+        double t = 0;
+        for (size_t i = 0; i + 1 < used; i += 2)
+        {
+            float ms = 0;
+            HBP_CUDA(cudaEventSynchronize(ev[i + 1]));
+            HBP_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+            t += ms;
+        }
+        return t;
+    }
+    EventTimer() = default;
+    EventTimer(const EventTimer &) = delete;
+    EventTimer &operator=(const EventTimer &) = delete;
+    ~EventTimer()
+    {
+        for (cudaEvent_t e : ev)
+            cudaEventDestroy(e);
+    }
+};
+
 struct KernelProf
 {
+    EventTimer edges; // k_edges launches (units: directed edges)
     bool on = false;
     std::vector<cudaEvent_t> ev; // start/stop pairs, reused
     size_t used = 0;
@@ -176,6 +230,7 @@ struct KernelProf
         bytes = 0;
         pixels = 0;
         launches = 0;
+        edges.reset();
         usedb = 0;
         tagb.clear();
         for (long &x : count)

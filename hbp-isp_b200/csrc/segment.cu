@@ -275,6 +275,68 @@ __global__ void node_1nn(const int2 *__restrict__ bd, const int *__restrict__ of
     dist_min[s] = best;
 }
 
+// ---------------------------------------------------------------------------
+// SegHAC::get_target_clus (segment.cu:1016-1041) with compute_dist_pos,
+// compute_scaned_pos, set_pre_clus_label and reset_clus_label (:635-755,
+// :954-1014): the Nn clusters CRTrees just formed from N nodes (Nn <= target
+// < N) become exactly `target`. Clusters are ranked by the sum of their
+// children's 1-NN distances, largest first (a stable descending sort, ties to
+// the lower label); ranks 0..b, b the first rank where breaking ranks 0..b
+// yields at least target clusters, are broken into their children, which take
+// the labels cum(i)-1, cum(i)-2, ... (cum: inclusive sum of the ranked child
+// counts) in increasing child index, capped at exact = target - Nn + b (the
+// children past the cap stay merged); unbroken rank i takes i + target - Nn.
+// Fixed orders where the reference has none: the distance sums add children
+// in increasing index (float atomics there) and the children of a broken
+// cluster take their labels in increasing index (atomicSub order there).
+
+// Per cluster c (children val[off[c] ..] in increasing index): the distance
+// sum as a descending sort key (the sums are >= 0, so the complemented bits
+// order them largest first) and c as its value.
+__global__ void target_sums(const uint32_t *val, const int *off, const float *dmin, int Nn, uint32_t *key,
+                            uint32_t *lab)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Nn)
+        return;
+    float s = 0.0f;
+    for (int j = off[c]; j < off[c + 1]; ++j)
+        s = s + dmin[val[j]];
+    key[c] = ~__float_as_uint(s);
+    lab[c] = (uint32_t)c;
+}
+
+// child count of the cluster ranked i (cnt[Nn] = 0 for the scan's total)
+__global__ void target_counts(const uint32_t *lab, const int *off, int Nn, int *cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Nn)
+        cnt[i] = off[lab[i] + 1] - off[lab[i]];
+    else if (i == Nn)
+        cnt[Nn] = 0;
+}
+
+// is_break_cluster: the first rank b with cum(b) + Nn - b - 1 >= target
+// (cum(i) = ex[i + 1]; the count is non-decreasing in i)
+__global__ void target_break(const int *ex, int Nn, int target, int *b)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Nn && ex[i + 1] + Nn - i - 1 >= target)
+        atomicMin(b, i);
+}
+
+__global__ void target_assign(const uint32_t *lab, const int *off, const uint32_t *val, const int *ex,
+                              const int *bptr, int Nn, int target, int *clus)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Nn)
+        return;
+    const int b = *bptr, exact = target - Nn + b, c = (int)lab[i];
+    const int j0 = off[c], j1 = off[c + 1];
+    for (int j = j0; j < j1; ++j)
+        clus[val[j]] = i <= b ? min(ex[i + 1] - 1 - (j - j0), exact) : i + target - Nn;
+}
+
 int bits_for(long n)
 {
     int b = 1;
@@ -290,7 +352,98 @@ int read_int(const int *dev, cudaStream_t st)
     HBP_CUDA(cudaStreamSynchronize(st));
     return h;
 }
+
+// get_target_clus on the labels clus (N nodes -> Nn clusters, Nn < target < N)
+// with the nodes' 1-NN distances dmin: clus then holds labels 0..target-1.
+void target_relabel(int *clus, const float *dmin, int N, int Nn, int target, Arena &tmp, cudaStream_t st)
+{
+    size_t m = tmp.mark();
+    uint32_t *ck = tmp.alloc<uint32_t>(N), *ck_alt = tmp.alloc<uint32_t>(N);
+    uint32_t *val = tmp.alloc<uint32_t>(N), *val_alt = tmp.alloc<uint32_t>(N);
+    int *count = tmp.alloc<int>(Nn + 1), *off = tmp.alloc<int>(Nn + 1);
+    uint32_t *key = tmp.alloc<uint32_t>(Nn), *key_alt = tmp.alloc<uint32_t>(Nn);
+    uint32_t *lab = tmp.alloc<uint32_t>(Nn), *lab_alt = tmp.alloc<uint32_t>(Nn);
+    int *ex = tmp.alloc<int>(Nn + 1), *b = tmp.alloc<int>(1);
+    // the children of every cluster in increasing index
+    HBP_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (Nn + 1), st));
+    copy_keys<<<ceil_div(N, 256), 256, 0, st>>>(clus, N, ck, count);
+    note_launch();
+    iota_u32<<<ceil_div(N, 256), 256, 0, st>>>(val, N);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    radix_sort_pairs_u32(ck, val, ck_alt, val_alt, N, bits_for(Nn), tmp, st);
+    exclusive_scan(count, off, Nn + 1, nullptr, tmp, st);
+    // rank by distance sum, then the cumulative child counts in rank order
+    target_sums<<<ceil_div(Nn, 128), 128, 0, st>>>(val, off, dmin, Nn, key, lab);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    radix_sort_pairs_u32(key, lab, key_alt, lab_alt, Nn, 32, tmp, st);
+    target_counts<<<ceil_div(Nn + 1, 128), 128, 0, st>>>(lab, off, Nn, count);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    exclusive_scan(count, ex, Nn + 1, nullptr, tmp, st);
+    HBP_CUDA(cudaMemsetAsync(b, 0x7f, sizeof(int), st)); // 0x7f7f7f7f: above every rank
+    target_break<<<ceil_div(Nn, 128), 128, 0, st>>>(ex, Nn, target, b);
+    note_launch();
+    target_assign<<<ceil_div(Nn, 128), 128, 0, st>>>(lab, off, val, ex, b, Nn, target, clus);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    tmp.rewind(m);
+}
 } // namespace
+
+namespace
+{
+// update_image_label through every level (segment.cu:871-883): a pixel's
+// label is its node's parent at the last level, clus_{L-1}(...clus_0(px)).
+__global__ void top_labels(const int *clus, const long *node_off, int L, int n, int *labels)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int v = i;
+    for (int l = 0; l < L; ++l)
+        v = clus[node_off[l] + v];
+    labels[i] = v;
+}
+
+__global__ void max_label(const int *clus, int n, int *mx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        atomicMax(mx, clus[i]);
+}
+} // namespace
+
+void launch_top_labels(const Pyramid &pyr, int *labels, Arena &tmp, cudaStream_t st)
+{
+    // the level offsets as a small device array (the pageable copy is staged
+    // before cudaMemcpyAsync returns)
+    std::vector<long> off(pyr.node_off.begin(), pyr.node_off.end());
+    size_t m = tmp.mark();
+    long *doff = tmp.alloc<long>(off.size());
+    HBP_CUDA(cudaMemcpyAsync(doff, off.data(), sizeof(long) * off.size(), cudaMemcpyHostToDevice, st));
+    const int n = pyr.W * pyr.H;
+    top_labels<<<ceil_div(n, 256), 256, 0, st>>>(pyr.clus, doff, pyr.L, n, labels);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    HBP_CUDA(cudaStreamSynchronize(st));
+    tmp.rewind(m);
+}
+
+int top_cluster_count(const Pyramid &pyr, Arena &tmp, cudaStream_t st)
+{
+    size_t m = tmp.mark();
+    int *mx = tmp.alloc<int>(1);
+    HBP_CUDA(cudaMemsetAsync(mx, 0, sizeof(int), st));
+    const int top = pyr.L - 1;
+    max_label<<<ceil_div(pyr.N[top], 256), 256, 0, st>>>(pyr.clus + pyr.node_off[top], pyr.N[top], mx);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    const int h = read_int(mx, st);
+    tmp.rewind(m);
+    return h + 1;
+}
 
 void check_seg_config(const SegConfig &cfg)
 {
@@ -300,6 +453,8 @@ void check_seg_config(const SegConfig &cfg)
         throw StatusError{HBP_ERR_INVALID_ARG, "num_nb must be 4 or 8"};
     if (!(cfg.sigma >= 0.0) || blur_radius(cfg.sigma) > BLUR_MAX_S)
         throw StatusError{HBP_ERR_INVALID_ARG, "sigma must lie in [0, 2.5): the blur radius round(3 sigma) <= 7"};
+    if (cfg.target < 1)
+        throw StatusError{HBP_ERR_INVALID_ARG, "target_clus must be >= 1"};
 }
 
 void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Arena &tmp,
@@ -307,6 +462,8 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
 {
     check_seg_config(cfg);
     const int N0 = W * H, NB = cfg.num_nb;
+    if (cfg.target >= N0)
+        throw StatusError{HBP_ERR_INVALID_ARG, "target_clus must be below the pixel count"};
     const bool use_mean = cfg.link == LINK_CENTROID || cfg.link == LINK_WARD;
     pyr.W = W;
     pyr.H = H;
@@ -368,6 +525,11 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         int Nn = read_int(num_dev, st);
         if (Nn < 1 || Nn > N)
             throw StatusError{HBP_ERR_NO_CONVERGENCE, "crtrees produced an invalid cluster count"};
+        if (Nn < cfg.target) // N > target: the previous level stopped above it
+        {
+            target_relabel(clus, dmin, N, Nn, cfg.target, tmp, st);
+            Nn = cfg.target;
+        }
         pyr.N.push_back(N);
         pyr.E.push_back((int)E);
         pyr.node_off.push_back(oc);
@@ -397,7 +559,7 @@ void segment_image(const uint8_t *bgr, int W, int H, Pyramid &pyr, Arena &a, Are
         HBP_LAUNCH_CHECK();
         exclusive_scan(count, nb_off, N + 1, nullptr, tmp, st);
         onb += N + 1;
-        if (Nn == 1)
+        if (Nn == cfg.target) // 1: the pyramid up to one node
             break;
 
         // next level's nodes and edges live right after this level's

@@ -210,6 +210,19 @@ class Context:
                                        None))
         return L.value
 
+    def segment_target_d(self, bgr, W, H, linkage, num_nb, sigma, target_clus) -> int:
+        L = C.c_int(0)
+        _check(lib().hbp_segment_target_d(self.h, _p(bgr), W, H, linkage, num_nb, C.c_double(sigma), target_clus,
+                                          C.byref(L), None))
+        return L.value
+
+    def segment_labels_d(self, labels) -> int:
+        """Every pixel's cluster at the pyramid's last level (device ints);
+        returns the number of clusters."""
+        k = C.c_int(0)
+        _check(lib().hbp_segment_labels_d(self.h, _p(labels), C.byref(k), None))
+        return k.value
+
     def lab_sigma_d(self, bgr, W, H, sigma, lab4):
         _check(lib().hbp_lab_sigma_d(self.h, _p(bgr), W, H, C.c_double(sigma), _p(lab4), None))
 

@@ -250,7 +250,63 @@ int orc_crtrees_literal(const int *nn_in, int N, int *clus_out)
     return k;
 }
 
-// SegHAC::run_ms with LabelISPFormat and target 1 (segment.cu:1279-1321), for
+// SegHAC::get_target_clus (segment.cu:1016-1041) with compute_dist_pos,
+// compute_scaned_pos, set_pre_clus_label and reset_clus_label (:635-755,
+// :954-1014): the num clusters that CRTrees just formed from num_p nodes
+// (num <= target < num_p) are ranked by the sum of their children's 1-NN
+// distances, largest first (ties: lower label first; the reference's sort is
+// a stable descending radix sort). The first b+1 ranked clusters are broken
+// into their children, b the first rank where breaking ranks 0..b gives at
+// least target clusters; the children of broken rank i take the labels
+// cum(i)-1, cum(i)-2, ... (cum: inclusive sum of the ranked child counts) in
+// increasing child index, every label above exact = target - num + b becomes
+// exact (those children stay merged), and unbroken rank i takes
+// i + target - num. The labels are then 0 .. target-1. Fixed orders where the
+// reference has none: the distance sums add children in increasing index
+// (float atomics there), and the children of a broken cluster take their
+// labels in increasing index (atomicSub order there).
+static int target_clusters(std::vector<int> &clus, const std::vector<float> &dist_min, int num_p, int num, int target)
+{
+    if (num == target)
+        return num;
+    std::vector<float> dist(num, 0.0f);
+    std::vector<int> cnt(num, 0);
+    for (int i = 0; i < num_p; ++i)
+    {
+        dist[clus[i]] += dist_min[i];
+        cnt[clus[i]]++;
+    }
+    std::vector<int> order(num);
+    for (int c = 0; c < num; ++c)
+        order[c] = c;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dist[a] > dist[b]; });
+    std::vector<int> cum(num), rank(num);
+    for (int i = 0; i < num; ++i)
+    {
+        cum[i] = (i ? cum[i - 1] : 0) + cnt[order[i]];
+        rank[order[i]] = i;
+    }
+    int b = num - 1;
+    for (int i = 0; i < num; ++i)
+        if (cum[i] + num - i - 1 >= target)
+        {
+            b = i;
+            break;
+        }
+    const int exact = target - num + b;
+    std::vector<int> used(num, 0);
+    for (int k = 0; k < num_p; ++k)
+    {
+        const int i = rank[clus[k]];
+        if (i <= b)
+            clus[k] = std::min(cum[i] - 1 - used[clus[k]]++, exact);
+        else
+            clus[k] = i + target - num;
+    }
+    return target;
+}
+
+// SegHAC::run_ms with LabelISPFormat (segment.cu:1279-1321), for
 // the linkages of segment.hpp:8-16 (0 Min, 1 Max, 2 Centroid, 3 Ward) and a
 // 4- or 8-neighbour pixel grid. Input: LAB float4 image (its fourth channel is
 // the pixel weight). Output: the image segmentation pyramid in the reference's
@@ -259,15 +315,18 @@ int orc_crtrees_literal(const int *nn_in, int N, int *clus_out)
 // floats, channel-major: sums of L, a, b, x, y and the weight), bd (E_l int
 // pairs), bdl (E_l ints), concatenated over levels. Capacities: clus 2*HW,
 // mean 12*HW, bd 4*num_nb*HW ints, bdl 2*num_nb*HW. Returns the number of
-// levels.
+// levels. target: SegHAC's target_clus; 1 builds the pyramid up to one
+// node, target > 1 (below W*H) stops at the first level whose CRTrees pass
+// leaves at most target clusters, after get_target_clus made them exactly
+// target: that level's clus maps its nodes to the target superpixels.
 //
 // Child sums are added in increasing child index starting from 0.0f (the
 // reference adds them with float atomics in an unspecified order,
 // segment.cu:472-486).
-int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int max_levels, int *level_sizes,
-                    int *clus_out, float *mean_out, int *bd_out, int *bdl_out)
+int orc_segment_target(const float *lab4, int W, int H, int link, int num_nb, int target, int max_levels,
+                       int *level_sizes, int *clus_out, float *mean_out, int *bd_out, int *bdl_out)
 {
-    if (link < 0 || link > 3 || (num_nb != 4 && num_nb != 8))
+    if (link < 0 || link > 3 || (num_nb != 4 && num_nb != 8) || target < 1 || target >= W * H)
         return -1;
     const bool use_mean = link == 2 || link == 3; // segment.hpp:248
     const int N0 = W * H;
@@ -290,6 +349,8 @@ int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int m
     {
         clus.resize(num);
         int num_new = orc_crtrees(nn.data(), num, clus.data());
+        if (num_new <= target)
+            num_new = target_clusters(clus, dist_min, num, num_new, target);
         // push the level (segment.cu:884-905)
         if (levels < max_levels)
         {
@@ -303,7 +364,7 @@ int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int m
         oc += num;
         ob += E;
         levels++;
-        if (num_new == 1)
+        if (num_new == target)
             break;
 
         // reduce_boundary_dist (segment.cu:1050-1091): map edges to parents,
@@ -411,6 +472,13 @@ int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int m
         edist.swap(edist2);
     }
     return levels;
+}
+
+int orc_segment_cfg(const float *lab4, int W, int H, int link, int num_nb, int max_levels, int *level_sizes,
+                    int *clus_out, float *mean_out, int *bd_out, int *bdl_out)
+{
+    return orc_segment_target(lab4, W, H, link, num_nb, 1, max_levels, level_sizes, clus_out, mean_out, bd_out,
+                              bdl_out);
 }
 
 // SegHAC::run_ms with CentroidLink and the 4-neighbour grid (the path's

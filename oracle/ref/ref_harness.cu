@@ -152,16 +152,17 @@ int ref_lab_sigma(const uint8_t *bgr, int W, int H, double sigma, float *lab4)
     return rc;
 }
 
-// SegHAC(link, num_nb, sigma, LabelISPFormat, 1).run_ms() (segment.cu:
-// 1279-1321), outputs as ref_segment (bd capacity 2 * num_nb * HW pairs,
-// bdl num_nb * 2 * HW). Returns the number of levels.
-int ref_segment_cfg(const uint8_t *bgr, int W, int H, int link, int num_nb, double sigma, int max_levels,
-                    int *level_sizes, int *clus, float *mean, int *bd, int *bdl)
+// SegHAC(link, num_nb, sigma, LabelISPFormat, target).run_ms() (segment.cu:
+// 1279-1321; target > 1: the superpixel mode, get_target_clus :1016-1041),
+// outputs as ref_segment (bd capacity 2 * num_nb * HW pairs, bdl
+// num_nb * 2 * HW). Returns the number of levels.
+int ref_segment_target(const uint8_t *bgr, int W, int H, int link, int num_nb, double sigma, int target,
+                       int max_levels, int *level_sizes, int *clus, float *mean, int *bd, int *bdl)
 {
     int levels = 0;
     int rc;
     {
-        SegHAC seg(wrap_bgr(bgr, W, H), (Linkage)link, num_nb, sigma, LabelISPFormat, 1, false);
+        SegHAC seg(wrap_bgr(bgr, W, H), (Linkage)link, num_nb, sigma, LabelISPFormat, target, false);
         seg.run_ms();
         rc = last_error();
         std::vector<int> nc = seg.g_num_clus_isp(), nb = seg.g_num_bd_isp();
@@ -186,6 +187,13 @@ int ref_segment_cfg(const uint8_t *bgr, int W, int H, int link, int num_nb, doub
     if (rc || rc2)
         return rc ? rc : rc2;
     return levels;
+}
+
+// The same with target 1 (the pyramid up to one node).
+int ref_segment_cfg(const uint8_t *bgr, int W, int H, int link, int num_nb, double sigma, int max_levels,
+                    int *level_sizes, int *clus, float *mean, int *bd, int *bdl)
+{
+    return ref_segment_target(bgr, W, H, link, num_nb, sigma, 1, max_levels, level_sizes, clus, mean, bd, bdl);
 }
 
 // Pixel 1-NN on the 4-grid (segment.cu:57-195): nn, dist_min and the four

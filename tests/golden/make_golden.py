@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|post_gpu|lab_sweep]
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|target|post_gpu|lab_sweep]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -39,13 +39,15 @@ class RefLib:
         self.lib = C.CDLL(path)
         for name in ("ref_grey", "ref_lab", "ref_1nn_grid", "ref_crtrees", "ref_cost",
                      "ref_segment", "ref_hbp_pair", "ref_post", "ref_hbp_f32", "ref_hbp_ad", "ref_lab_sigma",
-                     "ref_segment_cfg"):
+                     "ref_segment_cfg", "ref_segment_target"):
             getattr(self.lib, name).restype = C.c_int
         self.lib.ref_hbp_pair.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_int, C.c_int, P, P]
         self.lib.ref_lab_sigma.argtypes = [P, C.c_int, C.c_int, C.c_double, P]
         self.lib.ref_segment_cfg.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, P, P, P,
                                              P, P]
+        self.lib.ref_segment_target.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                                P, P, P, P, P]
         self.lib.ref_hbp_ad.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int,
                                         P, P, P, P, P, P]
         self.lib.ref_hbp_f32.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
@@ -150,7 +152,7 @@ class RefLib:
         assert rc == 0, rc
         return out
 
-    def segment_cfg(self, bgr, link, num_nb, sigma):
+    def segment_cfg(self, bgr, link, num_nb, sigma, target=1):
         H, W, _ = bgr.shape
         n = H * W
         sizes = np.zeros(2 * 64, np.int32)
@@ -158,8 +160,8 @@ class RefLib:
         mean = np.zeros(12 * n, np.float32)
         bd = np.zeros(4 * num_nb * n, np.int32)
         bdl = np.zeros(2 * num_nb * n, np.int32)
-        L = self.lib.ref_segment_cfg(ptr(bgr), W, H, link, num_nb, sigma, 64, ptr(sizes), ptr(clus), ptr(mean),
-                                     ptr(bd), ptr(bdl))
+        L = self.lib.ref_segment_target(ptr(bgr), W, H, link, num_nb, sigma, target, 64, ptr(sizes), ptr(clus),
+                                        ptr(mean), ptr(bd), ptr(bdl))
         assert L > 0, L
         sizes = sizes[: 2 * L].reshape(L, 2)
         tc, tb = int(sizes[:, 0].sum()), int(sizes[:, 1].sum())
@@ -313,6 +315,29 @@ def seg_record(ref: RefLib, W, H, seed):
     return rec
 
 
+# SegHAC's superpixel mode: (linkage, num_nb, target_clus) on the seg scenes
+TARGET_CFGS = [(2, 4, 7), (2, 4, 50), (2, 4, 300), (2, 4, 2000), (3, 8, 120), (0, 4, 40)]
+
+
+def target_record(ref: RefLib, W, H, seed):
+    """target_clus > 1: the pyramid (level sizes, the last level's clus) and
+    the label image of each configuration."""
+    s = make_scene(W, H, 32, seed)
+    rec = dict(W=W, H=H, seed=seed, left=s.left, cfgs=np.array(TARGET_CFGS, np.int32))
+    for i, (link, nb, target) in enumerate(TARGET_CFGS):
+        seg = ref.segment_cfg(s.left, link, nb, 0.0, target)
+        sizes = seg["level_sizes"]
+        labels = np.arange(W * H)
+        off = 0
+        for l in range(sizes.shape[0]):
+            labels = seg["clus"][off + labels]
+            off += int(sizes[l, 0])
+        rec[f"t{i}_level_sizes"] = sizes
+        rec[f"t{i}_clus"] = seg["clus"]
+        rec[f"t{i}_labels"] = labels.astype(np.int32).reshape(H, W)
+    return rec
+
+
 def post_gpu_record(ref: RefLib, golden_dir: str):
     """median_filter_gpu on the reference's own HBP results stored in the small
     fixtures (both views' disparities and planes), and the device patch weights."""
@@ -352,7 +377,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
-    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "post_gpu", "lab_sweep"], default=None)
+    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "target", "post_gpu", "lab_sweep"],
+                    default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     ref = RefLib(args.lib)
@@ -373,6 +399,11 @@ def main():
             rec = seg_record(ref, W, H, seed)
             np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
             print(name, [int(rec[f"c{i}_level_sizes"].shape[0]) for i in range(len(SEG_CFGS))])
+    if args.only in (None, "target"):
+        for (W, H, seed, name) in [(96, 64, 7, "target_96x64_s7"), (160, 112, 11, "target_160x112_s11")]:
+            rec = target_record(ref, W, H, seed)
+            np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
+            print(name, [int(rec[f"t{i}_level_sizes"].shape[0]) for i in range(len(TARGET_CFGS))])
     if args.only in (None, "post_gpu"):
         # inputs: the reference's HBP results in the committed census fixtures
         src = os.path.dirname(os.path.abspath(__file__))
@@ -382,7 +413,7 @@ def main():
         rec = lab_sweep_record(ref)
         np.savez_compressed(os.path.join(args.out, "lab_overrides.npz"), **rec)
         print("lab_sweep: colours where the host pow differs:", len(rec["keys"]))
-    if args.only in ("mccnn", "ad", "seg", "post_gpu", "lab_sweep"):
+    if args.only in ("mccnn", "ad", "seg", "target", "post_gpu", "lab_sweep"):
         return
 
     for (W, H, D, seed, full, name) in [

@@ -40,3 +40,4 @@ def test_fp64_shadow_message_error(case):
         assert e["msg_err_max"] <= e["msg_ref_max"]
     # FP16 storage adds little to the float arithmetic's own error
     assert e16["msg_err_mean"] < 1.25 * e32["msg_err_mean"]
+
