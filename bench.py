@@ -149,24 +149,94 @@ def make_pairs(n, W, H, D, seed0):
     return [make_scene(W, H, D, seed0 + i) for i in range(n)]
 
 
-def cpu_baseline(scene, W, H, D):
-    """Oracle (CPU port of the reference path) on one pair, all host cores."""
+def cpu_baseline(scenes, W, H, D):
+    """The CPU oracle (a port of the reference path) in its FP64 mode on the
+    first two pairs, all host cores; the FP32 mode (the engine's arithmetic)
+    on the first pair beside it."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as O
     cores = os.cpu_count() or 1
+    t64 = []
+    for s in scenes[:2]:
+        t0 = time.perf_counter()
+        O.driver_median(O.pipeline(s.left, s.right, D, fp64=True)["disp"])
+        t64.append(time.perf_counter() - t0)
     t0 = time.perf_counter()
-    res = O.pipeline(scene.left, scene.right, D)
-    O.driver_median(res["disp"])
-    dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": "pairs/s", "cores": cores, "kind": "port",
-            "sample": f"1 pair {W}x{H} D{D} (seed {scene.seed}) through the CPU oracle, "
-                      f"OpenMP on {cores} threads, {dt:.1f} s"}
+    O.driver_median(O.pipeline(scenes[0].left, scenes[0].right, D)["disp"])
+    t32 = time.perf_counter() - t0
+    seeds = ", ".join(str(s.seed) for s in scenes[:2])
+    return {"value": len(t64) / sum(t64), "unit": "pairs/s", "cores": cores, "kind": "port",
+            "mode": "fp64", "fp32_value": 1.0 / t32,
+            "sample": f"{len(t64)} pairs {W}x{H} D{D} (seeds {seeds}) through the CPU oracle's FP64 mode, "
+                      f"OpenMP on {cores} threads, {sum(t64):.1f} s; fp32_value: its FP32 mode on the "
+                      f"first pair, {t32:.1f} s"}
 
 
-# DRAM bytes (read + write) per list position of one k_cost launch, from the
-# committed ncu capture of a 4-view 720x496 D128 launch: 21,599,232 B over
-# 4 x 357,120 positions.
+def message_error(scene, D):
+    """Lock-step message error of FP32 and FP16 message storage against FP64
+    on one pair: the oracle's float run (bit-exact with the engine) with an
+    FP64 shadow that takes the same candidate planes and kept slots. Each
+    message is compared minus its own minimum (a per-message constant changes
+    no decision); raw errors of the stored values beside."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    out = {"pair_seed": scene.seed}
+    for name, fp16 in (("fp32", False), ("fp16", True)):
+        _, st = O.pipeline_lockstep(scene.left, scene.right, D, fp16_msg=fp16)
+        out[name] = {k: st[k] for k in ("msg_err_max", "msg_err_mean", "msg_ref_mean", "msg_ref_max",
+                                        "msg_raw_err_max", "msg_raw_err_mean", "values")}
+    return out
+
+
+# DRAM bytes (read + write) per unit of one launch, from the committed ncu
+# captures of 4-view 720x496 D128 launches (profiles/): k_cost per list
+# position, k_edges per directed edge.
 KCOST_DRAM_BYTES_PER_PIXEL = 21599232 / (4 * 357120)
+KEDGES_DRAM_BYTES_PER_EDGE = (31593216 + 1229312) / 482432
+
+
+KERNEL_NAMES = {"k_edges": "k_edges (message passing, smoothing and normalisation, one thread per "
+                           "directed edge)",
+                "k_cost": "k_cost (data cost of 4 candidate planes per pixel)"}
+
+
+def read_kernel_profiles(E, ctx):
+    """Summed device ms, launches, algorithmic bytes and units of the event-
+    timed k_cost and k_edges launches (every 16th BP tick of the first BP
+    stream) since profiling was enabled."""
+    import ctypes as C
+    out = {}
+    for kid, name in ((0, "k_cost"), (1, "k_edges")):
+        ms, n, b, u = C.c_double(), C.c_long(), C.c_double(), C.c_double()
+        E._check(E.lib().hbp_profile_read_kernel(ctx.h, kid, C.byref(ms), C.byref(n), C.byref(b), C.byref(u)))
+        out[name] = (ms.value, n.value, b.value, u.value)
+    return out
+
+
+def roofline_entry(name, prof, peak, peak_kind, hw, where):
+    """achieved = the timed launches' algorithmic bytes / their device time;
+    traffic = the committed ncu capture's DRAM bytes per unit, times the units
+    of an average timed launch."""
+    ms, n, b, u = prof
+    if ms <= 0 or n <= 0:
+        return None
+    achieved = b / (ms / 1e3) / 1e9
+    per_unit = KCOST_DRAM_BYTES_PER_PIXEL if name == "k_cost" else KEDGES_DRAM_BYTES_PER_EDGE
+    e = {"kernel": KERNEL_NAMES[name] + (", timed region: the first of the concurrent BP streams" if where == "live"
+                                         else ", BP on one stream (the kernel alone on the device)"),
+         "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+         "frac": achieved / peak, "traffic": per_unit * u / n,
+         "traffic_source": f"ncu dram__bytes_read+write per {'list position' if name == 'k_cost' else 'edge'} "
+                           f"of a 4-view 720x496 D128 capture (profiles/), times the units of an average "
+                           f"timed launch",
+         "algorithmic_bytes_per_launch": b / n, "launches_timed": n, "avg_launch_us": 1e3 * ms / n}
+    if name == "k_cost":
+        e["views_per_launch"] = u / n / hw
+    else:
+        e["edges_per_launch"] = u / n
+        e["note"] = ("instruction-issue bound (ncu: issue slots busy, DRAM a few %), so its HBM fraction "
+                     "is low by construction; the issue figures are in profiles/")
+    return e
 
 
 def max_over_ranks(x: float, dist, device) -> float:
@@ -245,10 +315,15 @@ def run_reference(args, rank):
         if i >= args.warmup:
             times.append(dt)
     tot = sum(times)
-    val = len(times) / tot
     lat = sorted(t * 1e3 for t in times)
+    # the reference's step times have a long tail (its host syncs and
+    # allocations per pair): the value is the median step's rate, the mean's
+    # beside it
+    p50 = lat[len(lat) // 2] if len(lat) % 2 else 0.5 * (lat[len(lat) // 2 - 1] + lat[len(lat) // 2])
+    val = 1e3 / p50
     out = {
         "metric": METRIC, "value": val, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+        "value_kind": "1 / median step time", "mean_value": len(times) / tot,
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
         "config": {"workload": f"1 synthetic pair {W}x{H} D{D} per step (sample of the 16-pair batch), "
@@ -256,8 +331,9 @@ def run_reference(args, rank):
                                "+ driver median", "W": W, "H": H, "D": D},
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
         "cpu_baseline": {"value": val, "unit": "pairs/s", "cores": 1, "kind": "reference",
-                         "sample": "one pair per step through the reference's own build, driven by one "
-                                   "host thread; the reference runs this path as CUDA kernels on the GPU"},
+                         "sample": f"one pair per step through the reference's own build, driven by one "
+                                   f"host thread, {len(times)} steps, median step; the reference runs this "
+                                   f"path as CUDA kernels on the GPU"},
         "e2e": {"value": val, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -541,8 +617,7 @@ def main():
     E._check(E.lib().hbp_last_phase_ms(ctx.h, ph))
     phases = {"prepare": ph[0], "bp": ph[1], "post": ph[2], "total": ph[3]}
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    pms, plaunch, pbytes, ppix = C.c_double(), C.c_long(), C.c_double(), C.c_double()
-    E._check(E.lib().hbp_profile_read(ctx.h, C.byref(pms), C.byref(plaunch), C.byref(pbytes), C.byref(ppix)))
+    live = read_kernel_profiles(E, ctx)
     E._check(E.lib().hbp_profile_enable(ctx.h, 0))
 
     # the same kernel alone on the device: one more batch (untimed) with the
@@ -554,11 +629,9 @@ def main():
         with torch.cuda.stream(stream):
             flush.random_(0, 255)
         step()
-        ims, ilaunch, ibytes, ipix = C.c_double(), C.c_long(), C.c_double(), C.c_double()
-        E._check(E.lib().hbp_profile_read(ctx.h, C.byref(ims), C.byref(ilaunch), C.byref(ibytes), C.byref(ipix)))
+        iso = read_kernel_profiles(E, ctx)
         E._check(E.lib().hbp_profile_enable(ctx.h, 0))
         E._check(E.lib().hbp_set_bp_streams(ctx.h, args.bp_streams))
-        iso = (ims.value, ilaunch.value, ibytes.value, ipix.value)
     t_max = max_over_ranks(ms, dist, "cuda")
     value = whole_job_rate(NP, args.steps, world, t_max / 1e3)
 
@@ -578,6 +651,8 @@ def main():
                     "bad2_fp32_pct": float(np.mean([bad2(d, s) for d, s in zip(d32, scenes)])),
                     "bad2_fp16_pct": float(np.mean([bad2(d, s) for d, s in zip(d16, scenes)])),
                     "pairs": NP}
+        if not args.no_cpu_baseline:
+            accuracy["message_error_vs_fp64"] = message_error(scenes[0], D)
 
     if args.breakdown and rank == 0:
         print(json.dumps(breakdown(E, ctx, step)), file=sys.stderr)
@@ -646,20 +721,15 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(scenes[0], W, H, D)
+        cpu = cpu_baseline(scenes, W, H, D)
 
     if rank == 0:
         peak, peak_kind = peaks()
-        achieved = (pbytes.value / (pms.value / 1e3)) / 1e9 if pms.value > 0 else None
-        per_launch = lambda pix, n: KCOST_DRAM_BYTES_PER_PIXEL * pix / max(1, n)
-        roof_iso = None
-        if iso and iso[0] > 0:
-            a_iso = (iso[2] / (iso[0] / 1e3)) / 1e9
-            roof_iso = {"kernel": "k_cost, BP on one stream (the kernel alone on the device)", "bound": "hbm",
-                        "achieved": a_iso, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                        "frac": a_iso / peak, "traffic": per_launch(iso[3], iso[1]),
-                        "views_per_launch": iso[3] / max(1, iso[1]) / (W * H),
-                        "launches_timed": iso[1], "avg_launch_us": 1e3 * iso[0] / max(1, iso[1])}
+        live_roof = {k: roofline_entry(k, v, peak, peak_kind, W * H, "live") for k, v in live.items()}
+        iso_roof = {k: roofline_entry(k, v, peak, peak_kind, W * H, "isolated") for k, v in iso.items()} \
+            if iso else None
+        # the dominant kernel: the larger share of the timed launches' device time
+        dom = max(live_roof, key=lambda k: live[k][0])
         lat.sort()
         line = {
             "metric": METRIC,
@@ -684,18 +754,9 @@ def main():
                            "of": "served requests, submit to result in host memory"},
             "plain_fp32": plain,
             "accuracy": accuracy,
-            "roofline": {"kernel": "k_cost (data cost of 4 candidate planes per pixel), timed region: "
-                                   "the first of the concurrent BP streams",
-                         "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": per_launch(ppix.value, plaunch.value) if plaunch.value else None,
-                         "traffic_source": "ncu dram__bytes_read+write of one k_cost launch over 4 views "
-                                           "(profiles/k_cost_level5_4x720x496_d128.md) per list position, "
-                                           "times the positions of a timed launch",
-                         "views_per_launch": ppix.value / max(1, plaunch.value) / (W * H),
-                         "launches_timed": plaunch.value,
-                         "avg_launch_us": 1e3 * pms.value / max(1, plaunch.value)},
-            "roofline_isolated": roof_iso,
+            "roofline": live_roof[dom],
+            "roofline_kernels": {"live": live_roof, "isolated": iso_roof,
+                                 "device_ms_timed": {k: v[0] for k, v in live.items()}},
             "cpu_baseline": cpu,
             "clocks": clk,
             "e2e": e2e,

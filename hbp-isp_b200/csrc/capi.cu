@@ -149,7 +149,9 @@ hbp_status guarded(F &&f)
 // edges) and the BP data; temporaries of the segmentation and the BP setup
 size_t slab_bytes(long pixels, int D)
 {
-    return (size_t)pixels * (size_t)(2 * (D + 16) + 1296) + ((size_t)96 << 20);
+    // two uint8 volumes, two 16-bit pair volumes of the data cost, the
+    // pyramids and BP state
+    return (size_t)pixels * (size_t)(2 * (D + 16) + 5 * D + 1296) + ((size_t)96 << 20);
 }
 size_t tmp_bytes(long pixels) { return (size_t)pixels * 560 + ((size_t)64 << 20); }
 
@@ -517,6 +519,12 @@ hbp_status hbp_lab_sigma_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, double 
 hbp_status hbp_segment_cfg_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int linkage, int num_nb, double sigma,
                              int *levels, void *stream)
 {
+    return hbp_segment_target_d(c, bgr, W, H, linkage, num_nb, sigma, 1, levels, stream);
+}
+
+hbp_status hbp_segment_target_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int linkage, int num_nb,
+                                double sigma, int target_clus, int *levels, void *stream)
+{
     if (!c || !bgr || !levels)
         return fail(HBP_ERR_INVALID_ARG, "null pointer");
     return guarded([&] {
@@ -524,7 +532,10 @@ hbp_status hbp_segment_cfg_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int l
         cfg.link = linkage;
         cfg.num_nb = num_nb;
         cfg.sigma = sigma;
+        cfg.target = target_clus;
         check_seg_config(cfg);
+        if ((long)target_clus >= (long)W * H)
+            throw StatusError{HBP_ERR_INVALID_ARG, "target_clus must be below W * H"};
         check_dims(W, H, 16);
         HBP_CUDA(cudaSetDevice(c->device));
         ensure_capacity(c, (long)W * H, std::max(c->cap_disp, 16));
@@ -537,6 +548,21 @@ hbp_status hbp_segment_cfg_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, int l
         check_device_error(c);
         c->have_pyr = true;
         *levels = c->pyr.L;
+    });
+}
+
+hbp_status hbp_segment_labels_d(hbp_ctx *c, int *labels, int *num_clusters, void *stream)
+{
+    if (!c || !labels || !c->have_pyr)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer or no pyramid");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = pick(c, stream);
+        c->tmp.reset();
+        launch_top_labels(c->pyr, labels, c->tmp, st);
+        if (num_clusters)
+            *num_clusters = top_cluster_count(c->pyr, c->tmp, st);
+        HBP_CUDA(cudaStreamSynchronize(st));
     });
 }
 
@@ -1079,6 +1105,29 @@ hbp_status hbp_profile_read(hbp_ctx *c, double *ms, long *launches, double *byte
     });
 }
 
+hbp_status hbp_profile_read_kernel(hbp_ctx *c, int kernel, double *ms, long *launches, double *bytes,
+                                   double *units)
+{
+    if (!c || !ms || !launches || !bytes || !units || kernel < 0 || kernel > 1)
+        return fail(HBP_ERR_INVALID_ARG, "kernel 0 (data cost) or 1 (edge messages) and four outputs");
+    return guarded([&] {
+        if (kernel == 0)
+        {
+            *ms = c->prof.total_ms();
+            *launches = c->prof.launches;
+            *bytes = c->prof.bytes;
+            *units = c->prof.pixels;
+        }
+        else
+        {
+            *ms = c->prof.edges.total_ms();
+            *launches = c->prof.edges.launches;
+            *bytes = c->prof.edges.bytes;
+            *units = c->prof.edges.units;
+        }
+    });
+}
+
 hbp_status hbp_set_bp_streams(hbp_ctx *c, int streams)
 {
     if (!c || streams < 0 || streams > 64)
@@ -1169,49 +1218,70 @@ struct hbp_server
     std::vector<std::unique_ptr<Lane>> lanes;
     std::vector<std::thread> threads;
     long long next_id = 1;
+    double bypass_ms = 2000.0; // how long a request that does not fit may be passed
     int preparing = 0; // requests a preparation lane has taken from to_prep
     bool stop = false;
     hbp_status fatal = HBP_OK;
     std::string fatal_msg;
     Lane sched; // error word and stream of the scheduler thread's own work
 
-    // Admit queued requests in arrival order while memory allows: a free
-    // slot large enough, else a new one within the budget (freeing pooled
-    // slots that are too small when that makes room). Caller holds mu.
+    // A slot for r: a pooled slot large enough (the smallest), else a new
+    // one within the budget, freeing pooled slots (the most recently pooled
+    // first) only when that makes room. False when r must wait for requests
+    // in flight to finish. Caller holds mu.
+    bool take_slot_locked(ServerReq *r)
+    {
+        const long px = (long)r->W * r->H;
+        int pick = -1;
+        for (size_t i = 0; i < pool.size(); ++i)
+            if (pool[i]->slot.cap_pixels >= px && pool[i]->slot.cap_disp >= r->D &&
+                (pick < 0 || pool[i]->bytes < pool[(size_t)pick]->bytes))
+                pick = (int)i;
+        if (pick >= 0)
+        {
+            r->ss = pool[(size_t)pick].get();
+            busy.push_back(std::move(pool[(size_t)pick]));
+            pool.erase(pool.begin() + pick);
+            return true;
+        }
+        size_t pooled = 0;
+        for (auto &p : pool)
+            pooled += p->bytes;
+        if (allocated - pooled + r->need > budget)
+            return false; // even an empty pool leaves no room
+        while (allocated + r->need > budget && !pool.empty())
+        {
+            allocated -= pool.back()->bytes;
+            pool.pop_back(); // frees its device and pinned memory
+        }
+        auto ns = std::make_unique<ServerSlot>();
+        ns->bytes = r->need;
+        allocated += r->need;
+        r->ss = ns.get();
+        r->new_slot = true;
+        busy.push_back(std::move(ns));
+        return true;
+    }
+
+    // Admit queued requests while memory allows, in arrival order, letting a
+    // request that fits pass one that does not (a large pair at the head does
+    // not block the small ones behind it) until the oldest waiting request
+    // has waited bypass_ms: from then on nothing passes it, so the pairs in
+    // flight drain and it is admitted next. Caller holds mu.
     void admit_locked()
     {
-        while (!queued.empty())
+        const double now = now_ms();
+        for (auto it = queued.begin(); it != queued.end();)
         {
-            ServerReq *r = queued.front();
-            const long px = (long)r->W * r->H;
-            int pick = -1;
-            for (size_t i = 0; i < pool.size(); ++i)
-                if (pool[i]->slot.cap_pixels >= px && pool[i]->slot.cap_disp >= r->D &&
-                    (pick < 0 || pool[i]->bytes < pool[(size_t)pick]->bytes))
-                    pick = (int)i;
-            if (pick >= 0)
+            ServerReq *r = *it;
+            if (!take_slot_locked(r))
             {
-                r->ss = pool[(size_t)pick].get();
-                busy.push_back(std::move(pool[(size_t)pick]));
-                pool.erase(pool.begin() + pick);
+                if (now - r->t_submit >= bypass_ms)
+                    break; // r has waited long enough: hold the rest back
+                ++it;
+                continue;
             }
-            else
-            {
-                while (allocated + r->need > budget && !pool.empty())
-                {
-                    allocated -= pool.back()->bytes;
-                    pool.pop_back(); // frees its device and pinned memory
-                }
-                if (allocated + r->need > budget)
-                    break; // wait for a request to finish
-                auto ns = std::make_unique<ServerSlot>();
-                ns->bytes = r->need;
-                allocated += r->need;
-                r->ss = ns.get();
-                r->new_slot = true;
-                busy.push_back(std::move(ns));
-            }
-            queued.pop_front();
+            it = queued.erase(it);
             r->state = RQ_PREPARING;
             to_prep.push_back(r);
             cv_prep.notify_one();

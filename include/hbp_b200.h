@@ -142,6 +142,22 @@ hbp_status hbp_segment_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int *le
  * (2, 4, 0.0). */
 hbp_status hbp_segment_cfg_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int linkage, int num_nb,
                              double sigma, int *levels, void *stream);
+/* The same with SegHAC's target_clus (segment.cu:1016-1041, :1279-1321):
+ * 1 is hbp_segment_cfg_d; target_clus > 1 (below W * H) stops the pyramid at
+ * the first level whose CRTrees pass leaves at most target_clus clusters,
+ * after get_target_clus has broken the clusters with the largest summed
+ * 1-NN distances into their children so that exactly target_clus remain (the
+ * superpixel mode). The last level's clus then maps its nodes to the
+ * superpixels 0 .. target_clus-1. Where the reference's order is unspecified
+ * (float atomic distance sums, atomicSub label hand-out) children count in
+ * increasing index. */
+hbp_status hbp_segment_target_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int linkage, int num_nb,
+                                double sigma, int target_clus, int *levels, void *stream);
+/* SegHAC's LabelIntFormat output (update_image_label, segment.cu:871-883,
+ * draw_segmentation :912-951) for the context's pyramid: every pixel's
+ * cluster at the last level (W*H ints on the device), and the number of
+ * those clusters in *num_clusters (may be NULL). Synchronous. */
+hbp_status hbp_segment_labels_d(hbp_ctx *ctx, int *labels, int *num_clusters, void *stream);
 /* SegHAC::img_CPU_to_GPU with sigma (segment.cu:795-809): CIELAB float4 of
  * the blurred image (the fourth channel is the blurred constant 1), into
  * lab4 (W*H float4). sigma = 0 gives hbp_lab_d's result. */
@@ -279,6 +295,9 @@ hbp_status hbp_set_bp_streams(hbp_ctx *ctx, int streams);
  * whatever runs beside it. prm applies to every request (post 0 or 1).
  * The budget counts the pairs' device slabs; the preparation lanes' scratch
  * (about 480 B per pixel of the largest pair, + 64 MB, per lane) comes on top.
+ * A queued request that does not fit yet may be passed by later ones that
+ * do, until it has waited 2 s; then nothing passes it and it is admitted as
+ * soon as the pairs in flight free its memory.
  * All functions are thread safe. Input and output buffers must stay valid
  * until hbp_wait returns for the request. */
 typedef struct hbp_server hbp_server;
@@ -315,6 +334,12 @@ hbp_status hbp_last_phase_ms(hbp_ctx *ctx, double *out4);
  * timed launches (pixels may be NULL). Enabling resets the totals. */
 hbp_status hbp_profile_enable(hbp_ctx *ctx, int on);
 hbp_status hbp_profile_read(hbp_ctx *ctx, double *ms, long *launches, double *bytes, double *pixels);
+/* The same per kernel: 0 the data cost (units: list positions), 1 the edge
+ * messages, timed on the same ticks (units: directed edges; bytes per edge
+ * 24 B of metadata and 12 message values read and written, plus per node its
+ * planes, beliefs, RANSAC points and kept slots). */
+hbp_status hbp_profile_read_kernel(hbp_ctx *ctx, int kernel, double *ms, long *launches, double *bytes,
+                                   double *units);
 /* Mode 3 additionally times every BP kernel of every 8th BP step. Breakdown
  * fills three arrays of 10 x 32 entries indexed [kind][level] (kinds: 0 node
  * select, 1 child candidates, 2 neighbour candidates, 3 set candidates,

@@ -167,3 +167,38 @@ def test_destroy_finishes_requests_still_in_preparation(gpu):
     for o, w in zip(outs, want):
         assert np.array_equal(o.view(np.uint32), w.view(np.uint32))
     del keep
+
+
+@pytest.mark.gpu
+def test_small_requests_pass_a_large_one_that_does_not_fit(gpu):
+    """Admission with bypass: a large pair that must wait for memory does not
+    hold back the small pairs queued behind it; it still runs, with the result
+    of hbp_run_pair."""
+    E = gpu
+    import time
+    from scenes import make_scene
+    prm = E.default_params(post=1)
+    big = [make_scene(450, 375, 64, 60 + i) for i in range(2)]
+    small = [make_scene(96, 64, 32, 70 + i) for i in range(3)]
+    budget = E.request_bytes(450, 375, 64) + 3 * E.request_bytes(96, 64, 32) + (64 << 20)
+    srv = E.Server(0, budget_bytes=budget, prep_lanes=2, params=prm)
+    try:
+        t0 = time.perf_counter()
+        ids = [(srv.submit(b.left, b.right, 64), time.perf_counter()) for b in big]
+        ids += [(srv.submit(s.left, s.right, 32), time.perf_counter()) for s in small]
+        done = []
+        for rid, ts in ids:
+            out, lat = srv.wait(rid)
+            done.append((ts - t0) * 1e3 + lat)
+            if rid == ids[1][0]:
+                second_big = out
+    finally:
+        srv.close()
+    # every small pair finished before the second large one, which had to
+    # wait for the first large one's memory
+    assert max(done[2:]) < done[1], done
+    ctx = E.Context(0)
+    try:
+        assert np.array_equal(second_big, ctx.run_pair(big[1].left, big[1].right, 64, prm))
+    finally:
+        ctx.close()
