@@ -71,6 +71,10 @@ def parse():
                          "min_level) at a Middlebury half-resolution size")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
+    ap.add_argument("--rates", default="", help="serve: comma-separated arrival rates, one phase each "
+                                                 "(a sweep; overrides --rate)")
+    ap.add_argument("--p99-bound-ms", type=float, default=5000.0,
+                    help="serve sweep: the p99 latency a sustainable rate must stay within")
     ap.add_argument("--profile-run", action="store_true",
                     help="skip the untimed extra batches (accuracy, isolated roofline): for profiler captures")
     ap.add_argument("--bp-streams", type=int, default=0,
@@ -211,6 +215,21 @@ def read_kernel_profiles(E, ctx):
         E._check(E.lib().hbp_profile_read_kernel(ctx.h, kid, C.byref(ms), C.byref(n), C.byref(b), C.byref(u)))
         out[name] = (ms.value, n.value, b.value, u.value)
     return out
+
+
+def autotune_rows(E, ctx, explore):
+    """The BP-stream autotuner's measurements for this context (hbp_autotune_table)."""
+    import ctypes as C
+    n = E.lib().hbp_autotune_table(ctx.h, None, 0)
+    if n <= 0:
+        return None
+    buf = (C.c_double * (9 * n))()
+    E.lib().hbp_autotune_table(ctx.h, buf, n)
+    rows = [list(buf[9 * i:9 * i + 9]) for i in range(n)]
+    return {"exploration_batches": explore,
+            "tried": [{"streams": int(r[6]), "bp_ms_per_view": round(r[7], 3), "chosen": bool(r[8])} for r in rows],
+            "class": {"W": int(rows[0][0]), "H": int(rows[0][1]), "D": int(rows[0][2]), "msg_fp16": int(rows[0][3]),
+                      "post": int(rows[0][4]), "views": int(rows[0][5])}}
 
 
 def roofline_entry(name, prof, peak, peak_kind, hw, where):
@@ -507,44 +526,58 @@ def run_config(args, E, torch):
                 "fp16_vs_fp32_identical_min": float(np.min(same))}
     if args.config == "mccnn":
         return run_mccnn(args, E, torch, local, bad)
-    # serve: Poisson arrivals of the size mix, FP16 messages, 120 GB budget
-    rng = np.random.default_rng(11)
+    # serve: Poisson arrivals of the size mix, FP16 messages, 120 GB budget;
+    # --rates runs one arrival phase per rate on the same server
     mix = [((450, 375, 64), 0.4), ((720, 496, 128), 0.3), ((1440, 992, 256), 0.2), ((2880, 1984, 384), 0.1)]
     kinds = [m for m, _ in mix]
     pool = {k: make_scene(k[0], k[1], k[2], 7000 + i) for i, k in enumerate(kinds)}
-    n_req = max(1, int(args.rate * args.duration))
-    gaps = rng.exponential(1.0 / args.rate, n_req)
-    pick = rng.choice(len(kinds), n_req, p=[p for _, p in mix])
+    rates = [float(r) for r in args.rates.split(",")] if args.rates else [args.rate]
     prm = E.default_params(msg_fp16=1, post=1)
     srv = E.Server(local, budget_bytes=120 << 30, prep_lanes=8, params=prm)
+    phases = []
     try:
         for k in kinds:  # warm-up, one of each size
             s = pool[k]
             srv.wait(srv.submit(s.left, s.right, k[2]))
-        t0 = time.perf_counter()
-        t_next = t0
-        ids = []
-        for g, j in zip(gaps, pick):
-            t_next += g
-            dt = t_next - time.perf_counter()
-            if dt > 0:
-                time.sleep(dt)
-            s = pool[kinds[j]]
-            ids.append((srv.submit(s.left, s.right, kinds[j][2]), j))
-        lat = [srv.wait(i)[1] for i, _ in ids]
-        el = time.perf_counter() - t0
+        for ri, rate in enumerate(rates):
+            rng = np.random.default_rng(11 + ri)
+            n_req = max(1, int(rate * args.duration))
+            gaps = rng.exponential(1.0 / rate, n_req)
+            pick = rng.choice(len(kinds), n_req, p=[p for _, p in mix])
+            t0 = time.perf_counter()
+            t_next = t0
+            ids = []
+            for g, j in zip(gaps, pick):
+                t_next += g
+                dt = t_next - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                s = pool[kinds[j]]
+                ids.append((srv.submit(s.left, s.right, kinds[j][2]), j))
+            t_arr = time.perf_counter() - t0
+            lat = [srv.wait(i)[1] for i, _ in ids]
+            el = time.perf_counter() - t0
+            ls = sorted(lat)
+            per = {}
+            for (i, j), l in zip(ids, lat):
+                per.setdefault(f"{kinds[j][0]}x{kinds[j][1]}xD{kinds[j][2]}", []).append(l)
+            px = sum(kinds[j][0] * kinds[j][1] for _, j in ids)
+            phases.append({"offered_rate": rate, "arrival_seconds": t_arr, "requests": n_req,
+                           "completed_per_s": n_req / el, "mpixels_per_s": px / el / 1e6,
+                           "seconds_to_drain": el,
+                           "latency_ms": {"p50": ls[len(ls) // 2], "p99": ls[min(len(ls) - 1, int(0.99 * len(ls)))]},
+                           "latency_p50_by_size_ms": {k: sorted(v)[len(v) // 2] for k, v in per.items()}})
     finally:
         srv.close()
-    ls = sorted(lat)
-    per = {}
-    for (i, j), l in zip(ids, lat):
-        per.setdefault(f"{kinds[j][0]}x{kinds[j][1]}xD{kinds[j][2]}", []).append(l)
-    return {"config": "serve", "offered_rate": args.rate, "arrival_seconds": args.duration,
-            "requests": n_req, "completed_per_s": n_req / el, "seconds_to_drain": el,
-            "latency_ms": {"p50": ls[len(ls) // 2], "p99": ls[min(len(ls) - 1, int(0.99 * len(ls)))]},
-            "latency_p50_by_size_ms": {k: sorted(v)[len(v) // 2] for k, v in per.items()},
-            "workload": "Poisson arrivals; 40% 450x375 D64, 30% 720x496 D128, 20% 1440x992 D256, "
-                        "10% 2880x1984 D384; FP16 messages; 120 GB admission budget (seed 11)"}
+    out = {"config": "serve", "phases": phases,
+           "workload": "Poisson arrivals; 40% 450x375 D64, 30% 720x496 D128, 20% 1440x992 D256, "
+                       "10% 2880x1984 D384; FP16 messages; 120 GB admission budget (seeds 11+)"}
+    if len(rates) > 1:
+        bound = args.p99_bound_ms
+        ok = [p["offered_rate"] for p in phases if p["latency_ms"]["p99"] <= bound]
+        out["p99_bound_ms"] = bound
+        out["highest_rate_within_bound"] = max(ok) if ok else None
+    return out
 
 
 def main():
@@ -588,6 +621,16 @@ def main():
     def step():
         E._check(E.lib().hbp_run_batch_d(ctx.h, NP, arrL, arrR, W, H, D, C.byref(prm), arrD, None))
 
+    # the BP stream autotuner explores its candidates on the first batches of
+    # this workload (untimed, before the warm-up); later batches use its choice
+    explore = 0
+    if args.bp_streams == 0:
+        while explore < 8:
+            rows = E.lib().hbp_autotune_table(ctx.h, None, 0)
+            step()
+            explore += 1
+            if E.lib().hbp_autotune_table(ctx.h, None, 0) == rows:
+                break  # nothing new was measured: the choice is made
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -762,6 +805,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "phase_ms_last_step": phases,
+            "autotune": autotune_rows(E, ctx, explore),
         }
         print(json.dumps(line))
     if dist:

@@ -10,6 +10,9 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <algorithm>
+#include <array>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -96,11 +99,29 @@ struct Slot
     float *dispR = nullptr, *planeR = nullptr, *plane = nullptr;
 };
 
+// Online choice of the number of BP streams of a batch, per workload class
+// (image size, disparity range, message storage, post mode, views per batch):
+// the first batches of a class try each candidate once, timing the BP phase on
+// the host clock, and later batches use the fastest. Views never read one
+// another's data, so the streams change no result, only the speed.
+struct AutoTune
+{
+    struct Entry
+    {
+        std::vector<int> cand;   // stream counts to try
+        std::vector<double> ms;  // BP ms per view of each tried candidate
+        int best = -1;           // index into cand once every candidate ran
+    };
+    bool on = true;
+    std::map<std::array<int, 6>, Entry> table;
+};
+
 struct hbp_ctx : Lane
 {
     float *wtab = nullptr; // weighted-median weight table (766 floats)
     int prof_mode = 0;     // 0 off, 1 every pair, 2 first pair of each batch call
     int bp_streams = 0;    // hbp_set_bp_streams
+    AutoTune tune;         // used while bp_streams == 0
     int max_lanes = 8;
     std::vector<std::unique_ptr<Lane>> lanes; // extra lanes (1..)
     std::vector<std::unique_ptr<Slot>> slots;
@@ -149,9 +170,7 @@ hbp_status guarded(F &&f)
 // edges) and the BP data; temporaries of the segmentation and the BP setup
 size_t slab_bytes(long pixels, int D)
 {
-    // two uint8 volumes, two 16-bit pair volumes of the data cost, the
-    // pyramids and BP state
-    return (size_t)pixels * (size_t)(2 * (D + 16) + 5 * D + 1296) + ((size_t)96 << 20);
+    return (size_t)pixels * (size_t)(2 * (D + 16) + 1296) + ((size_t)96 << 20);
 }
 size_t tmp_bytes(long pixels) { return (size_t)pixels * 560 + ((size_t)64 << 20); }
 
@@ -966,11 +985,31 @@ void run_pairs(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, const uint8_t
         }
         HbpParams q = to_params(&p, c->prof_mode ? &c->prof : nullptr);
         q.bp_streams = c->bp_streams;
+        AutoTune::Entry *tune = nullptr;
+        if (q.bp_streams == 0 && c->tune.on)
+        {
+            const std::array<int, 6> key{W, H, D, p.msg_fp16, p.post, (int)views.size()};
+            tune = &c->tune.table[key];
+            if (tune->cand.empty())
+                for (int s : {2, 4, 8, 12, 16})
+                    if (s <= (int)views.size())
+                        tune->cand.push_back(s);
+            if (tune->cand.empty())
+                tune->cand.push_back(1);
+            q.bp_streams = tune->best >= 0 ? tune->cand[(size_t)tune->best] : tune->cand[tune->ms.size()];
+        }
         c->prof.on = c->prof_mode != 0;
         c->tmp.reset();
+        const auto t_views = clk::now();
         {
             NvtxRange r("bp");
             hbp_run_views(views, q, c->tmp, c->st);
+        }
+        if (tune && tune->best < 0)
+        {
+            tune->ms.push_back(ms_since(t_views) / (double)views.size());
+            if (tune->ms.size() == tune->cand.size())
+                tune->best = (int)(std::min_element(tune->ms.begin(), tune->ms.end()) - tune->ms.begin());
         }
         c->phase_ms[1] += ms_since(t_bp);
         const auto t_post = clk::now();
@@ -1126,6 +1165,33 @@ hbp_status hbp_profile_read_kernel(hbp_ctx *c, int kernel, double *ms, long *lau
             *units = c->prof.edges.units;
         }
     });
+}
+
+hbp_status hbp_set_autotune(hbp_ctx *c, int on)
+{
+    if (!c)
+        return fail(HBP_ERR_INVALID_ARG, "null context");
+    c->tune.on = on != 0;
+    return HBP_OK;
+}
+
+int hbp_autotune_table(hbp_ctx *c, double *rows, int max_rows)
+{
+    if (!c)
+        return -1;
+    int n = 0;
+    for (const auto &kv : c->tune.table)
+        for (size_t i = 0; i < kv.second.ms.size(); ++i, ++n)
+            if (rows && n < max_rows)
+            {
+                double *r = rows + 9 * (size_t)n;
+                for (int k = 0; k < 6; ++k)
+                    r[k] = kv.first[(size_t)k];
+                r[6] = kv.second.cand[i];
+                r[7] = kv.second.ms[i];
+                r[8] = kv.second.best == (int)i ? 1.0 : 0.0;
+            }
+    return n;
 }
 
 hbp_status hbp_set_bp_streams(hbp_ctx *c, int streams)

@@ -59,10 +59,6 @@ struct LevelDev
     unsigned long long *keep; // N: kept slots (count | 4-bit indices)
 };
 
-#ifndef PAIR_VOLUME
-#define PAIR_VOLUME 1
-#endif
-
 struct Common
 {
     int W, H, D, TX; // TX: volume tiles per row
@@ -70,10 +66,6 @@ struct Common
     const uint8_t *vol; // tiled, vol_offset() (Census: uint8 costs)
     const float *volf;  // or the same layout in floats (MC-CNN); null for uint8
     const float *wta;   // HW
-    // Census: the data cost's copy of vol in which entry (x, y, d) holds the
-    // two costs one interpolation reads, V[d] | V[d+1] << 8 (same tiling,
-    // 16-bit entries), so that a pixel and plane take one load
-    const uint16_t *vol2;
 };
 
 __device__ __forceinline__ int px_x(uint32_t xy) { return (int)(xy & 0xffffu); }
@@ -111,15 +103,9 @@ __device__ __forceinline__ float pixel_cost(const Common &c, float xf, float yf,
         }
         else
         {
-#if PAIR_VOLUME
-            const uint32_t w = c.vol2[base + (size_t)d * VT_BYTES];
-            v0 = byte_to_float(w & 0xffu);
-            v1 = byte_to_float(w >> 8);
-#else
             const uint8_t *pv = c.vol + base + (size_t)d * VT_BYTES;
             v0 = byte_to_float(pv[0]);
             v1 = byte_to_float(pv[VT_BYTES]);
-#endif
         }
         const float fd = (float)d;
         cost = __fmaf_rn((fd + 1.0f) - d_f, v0, (d_f - fd) * v1);
@@ -144,20 +130,6 @@ __global__ void compose_im_clus(const int *im, const int *clus, int n, int *out)
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         out[i] = clus[im[i]];
-}
-
-// The pair volume of Common::vol2: entry i holds vol[i] | vol[i + 32] << 8
-// (the next disparity of the same pixel); the last disparity's entry holds
-// vol[i] alone (never read: the data cost takes tau for d >= D - 1).
-__global__ void pair_volume(const uint8_t *__restrict__ vol, long n, int D, uint16_t *__restrict__ vol2)
-{
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const int d = (int)((i / VT_BYTES) % D);
-    const uint32_t lo = vol[i];
-    const uint32_t hi = d + 1 < D ? vol[i + VT_BYTES] : 0u;
-    vol2[i] = (uint16_t)(lo | hi << 8);
 }
 
 __global__ void iota_int(int *v, int n)
@@ -1004,10 +976,11 @@ __global__ void __launch_bounds__(128) k_init_nodes(const ViewDev *__restrict__ 
 }
 
 // passing_msg_k + smooth_msg_k + normalize_msg_k (hbp_isp.cu:273-355), one
-// thread per edge. Blocks per SM: the target labels' point values take 48
-// registers; EDGES_MIN_BLOCKS bounds the register count.
+// thread per edge. EDGES_MIN_BLOCKS bounds the register count (blocks of
+// 128 per SM); the kernel waits on plane loads and divergent divisions, so
+// occupancy matters.
 #ifndef EDGES_MIN_BLOCKS
-#define EDGES_MIN_BLOCKS 4
+#define EDGES_MIN_BLOCKS 7
 #endif
 __global__ void __launch_bounds__(128, EDGES_MIN_BLOCKS) k_edges(const ViewDev *__restrict__ V, StepDesc d)
 {
@@ -1062,107 +1035,68 @@ __global__ void __launch_bounds__(128, EDGES_MIN_BLOCKS) k_edges(const ViewDev *
             mp[p] = bt[p] - m;
         }
     }
-    float4 pt[2 * P];
-#pragma unroll
-    for (int p = 0; p < 2 * P; ++p)
-        pt[p] = l.plane[(size_t)st.y * K + p];
-    // Each group's minimum over t's labels p of mp[p] + c0 * phi: c0 * phi is
-    // >= 0 and float addition is monotone, so a label whose mp[p] is not
-    // below the running minimum cannot lower it. The labels of each group are
-    // sorted by mp (NaN last; the planes move with them) and the scan stops
-    // at the first such label; the minimum, hence the message, is the
-    // reference's.
-    float key[2 * P];
-#pragma unroll
-    for (int p = 0; p < 2 * P; ++p)
-        key[p] = mp[p] == mp[p] ? mp[p] : INFINITY;
-#pragma unroll
-    for (int g = 0; g < 2; ++g)
-    {
-        const int b = g * P;
-        auto cswap = [&](int i, int j) {
-            if (key[b + j] < key[b + i])
-            {
-                float tk = key[b + i];
-                key[b + i] = key[b + j];
-                key[b + j] = tk;
-                float tm = mp[b + i];
-                mp[b + i] = mp[b + j];
-                mp[b + j] = tm;
-                float4 tp = pt[b + i];
-                pt[b + i] = pt[b + j];
-                pt[b + j] = tp;
-            }
-        };
-        cswap(0, 1);
-        cswap(2, 3);
-        cswap(0, 2);
-        cswap(1, 3);
-        cswap(1, 2);
-    }
-    // Each target label's plane evaluated at the six points once per edge:
-    // phi(y, q) = sum_i |vs_y,i - vt_q,i| with v = fma(a, X_i, fma(b, Y_i, c)),
-    // two subtractions per point instead of the difference plane's two
-    // multiply-adds (the oracle restates this form).
-    float vt[2 * P][6];
-#pragma unroll
-    for (int p = 0; p < 2 * P; ++p)
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-            vt[p][i] = __fmaf_rn(pt[p].x, X[i], __fmaf_rn(pt[p].y, Y[i], pt[p].z));
-    // Lower bound of q = (phi / 3) / dist_pos from one multiply: scale =
-    // (1/3)(1/dist_pos)(1 - 2^-20) in rounded steps, so phi * scale is within
-    // (1 - 2^-20)(1 + 2^-24)^5 of phi / (3 dist_pos), below q, which is within
-    // (1 - 2^-24)^2 of it, for normal values (tiny or NaN bound -> 0).
-    // Rounding is monotone, so with the bound qlb:
-    // qlb >= tau_smooth means min(q, tau_smooth) == tau_smooth exactly, and
-    // fma(c0, qlb, mp) >= the running minimum means the label cannot lower it.
-    // Only the remaining labels need the exact divisions. Every label's phi
-    // is evaluated (uniform across the warp); a label skipped this way or
-    // with mp >= the minimum leaves the minimum unchanged, as does a NaN.
+    // min(phi / 3 / dist_pos, tau_smooth) as min(phi * rq, tau_smooth), rq =
+    // (1/3) / dist_pos rounded once per edge (the oracle states the same
+    // form): every label takes the same few instructions, no division and no
+    // branch per label.
     const float tau = c.tau_smooth;
-    const float inv_dp = 1.0f / dist_pos;
-    const float inv3 = 1.0f / 3.0f;
-    const float scale = inv3 * inv_dp * 0.99999905f; // 1 - 2^-20
+    const float rq = (1.0f / 3.0f) / dist_pos;
     __shared__ float s_out[K][128];
     float sum = 0.f;
+    // Two passes, one per label group, so that only one group's point values
+    // (4 labels x 6 points) are held in registers: the first pass leaves each
+    // source label's group-0 minimum in s_out, the second adds the group-1
+    // minimum to it (msg_t = min_0 + min_1, the reference's order). phi(y, q)
+    // = sum_i |vs_y,i - vt_q,i| with v = fma(a, X_i, fma(b, Y_i, c)): each
+    // plane evaluated at the six points once per pass, two subtractions per
+    // point and label pair (the oracle states the same form).
 #pragma unroll 1
-    for (int y = 0; y < K; ++y)
+    for (int g = 0; g < 2; ++g)
     {
-        const float4 ps = l.plane[(size_t)st.x * K + y];
-        float vs[6];
+        float vt[P][6], mg[P];
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
-            vs[i] = __fmaf_rn(ps.x, X[i], __fmaf_rn(ps.y, Y[i], ps.z));
-        float acc = 0.f;
-#pragma unroll
-        for (int g = 0; g < 2; ++g)
+        for (int k = 0; k < P; ++k)
         {
+            const float4 tp = l.plane[(size_t)st.y * K + g * P + k];
+            mg[k] = mp[g * P + k];
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                vt[k][i] = __fmaf_rn(tp.x, X[i], __fmaf_rn(tp.y, Y[i], tp.z));
+        }
+#pragma unroll 1
+        for (int y = 0; y < K; ++y)
+        {
+            const float4 ps = l.plane[(size_t)st.x * K + y];
+            // point by point: the source plane's value at point i, then each
+            // label's running sum (phi_k adds points 0..5 in order)
+            float phis[P];
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+            {
+                const float vs = __fmaf_rn(ps.x, X[i], __fmaf_rn(ps.y, Y[i], ps.z));
+#pragma unroll
+                for (int k = 0; k < P; ++k)
+                    phis[k] = i == 0 ? fabsf(vs - vt[k][0]) : phis[k] + fabsf(vs - vt[k][i]);
+            }
+            // the group's minimum over its labels in slot order (a NaN never
+            // lowers it)
             float mn = FLT_MAX;
 #pragma unroll
             for (int k = 0; k < P; ++k)
             {
-                const int q = g * P + k;
-                float phi = fabsf(vs[0] - vt[q][0]);
-#pragma unroll
-                for (int i = 1; i < 6; ++i)
-                    phi = phi + fabsf(vs[i] - vt[q][i]);
-                const float qs = phi * scale;
-                const float qlb = qs >= 1e-30f ? qs : 0.0f;
-                float m;
-                if (qlb >= tau)
-                    m = __fmaf_rn(c0, tau, mp[q]);
-                else if (k == 0 || __fmaf_rn(c0, qlb, mp[q]) < mn)
-                    m = __fmaf_rn(c0, fminf(phi / 3.0f / dist_pos, tau), mp[q]);
-                else
-                    m = mn;
+                const float m = __fmaf_rn(c0, fminf(phis[k] * rq, tau), mg[k]);
                 if (m < mn)
                     mn = m;
             }
-            acc = acc + mn;
+            if (g == 0)
+                s_out[y][threadIdx.x] = 0.f + mn;
+            else
+            {
+                const float acc = s_out[y][threadIdx.x] + mn;
+                s_out[y][threadIdx.x] = acc;
+                sum = sum + acc;
+            }
         }
-        s_out[y][threadIdx.x] = acc;
-        sum = sum + acc;
     }
     float out[K];
 #pragma unroll
@@ -1281,18 +1215,7 @@ void hbp_prepare(const Pyramid &pyr, const CostVolume &cv, const float *wta, int
     if ((int)pyr.N.size() != L || (int)pyr.E.size() != L || (int)pyr.node_off.size() != L ||
         (int)pyr.edge_off.size() != L || (int)pyr.child_base.size() != L || (int)pyr.nb_base.size() != L)
         throw StatusError{HBP_ERR_INTERNAL, "pyramid bookkeeping inconsistent"};
-    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, cv.tau, prm.tau_smooth, cv.u8, cv.f32, wta, nullptr};
-#if PAIR_VOLUME
-    if (cv.u8)
-    {
-        const long nv = (long)volume_bytes(W, H, D);
-        uint16_t *vol2 = persist.alloc<uint16_t>((size_t)nv);
-        pair_volume<<<blocks(nv, 256), 256, 0, st>>>(cv.u8, nv, D, vol2);
-        note_launch();
-        HBP_LAUNCH_CHECK();
-        c.vol2 = vol2;
-    }
-#endif
+    Common c{W, H, D, ceil_div(W, VT_W), prm.alpha, cv.tau, prm.tau_smooth, cv.u8, cv.f32, wta};
     std::vector<LevelDev> &lv = vp.impl->lv;
     lv.assign(L, LevelDev{});
     vp.L = L;

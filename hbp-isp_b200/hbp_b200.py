@@ -58,6 +58,8 @@ def lib():
         L.hbp_submit.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, P, C.POINTER(C.c_longlong)]
         L.hbp_poll.argtypes = [P, C.c_longlong]
         L.hbp_wait.argtypes = [P, C.c_longlong, C.c_double, C.POINTER(C.c_double)]
+        L.hbp_autotune_table.argtypes = [P, P, C.c_int]
+        L.hbp_autotune_table.restype = C.c_int
         _lib = L
     return _lib
 

@@ -281,6 +281,17 @@ hbp_status hbp_set_lanes(hbp_ctx *ctx, int lanes);
  * kernels of different pairs share the GPU; streams > 0 fixes the number
  * (1 = every BP kernel alone on the device). 0 restores the default. */
 hbp_status hbp_set_bp_streams(hbp_ctx *ctx, int streams);
+/* While the stream count is automatic (0), batches autotune it (no reference
+ * counterpart): per class (W, H, D, msg_fp16, post, views per batch) the first
+ * batches try 2, 4, 8, 12 and 16 streams (those not above the views), one
+ * batch each, timing the BP phase, and later batches use the fastest. The
+ * streams change no result. on = 0 turns it off (the default 8 streams, two
+ * views each). */
+hbp_status hbp_set_autotune(hbp_ctx *ctx, int on);
+/* The autotuner's measurements: up to max_rows rows of 9 doubles (W, H, D,
+ * msg_fp16, post, views, streams, BP ms per view, 1 if chosen); returns the
+ * number of rows (or -1 for a null context). rows may be NULL to count. */
+int hbp_autotune_table(hbp_ctx *ctx, double *rows, int max_rows);
 
 /* ------------------------------------------------------------ serving */
 

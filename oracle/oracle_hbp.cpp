@@ -30,7 +30,10 @@
 // smoothness point fma(a, X, fma(b, Y, c)) and message fma(c0, phi, msg).
 // The smoothness term of two planes is sum_i |v_s,i - v_t,i| over the six
 // points (the reference evaluates the difference plane at each point,
-// hbp_isp.cu:339-344: the same quantity with other roundings).
+// hbp_isp.cu:339-344: the same quantity with other roundings), and
+// min(phi / 3 / dist_pos, tau_smooth) is taken as min(phi * rq, tau_smooth)
+// with rq = (1/3) / dist_pos rounded once per edge (:349, two divisions per
+// label there).
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
@@ -368,6 +371,8 @@ struct Engine
             T dist_color = std::fmax((T)l.dc[e], (T)0.01f);
             T dist_pos = std::fmax((T)l.dc[(size_t)E + e], (T)1.0f);
             T c0 = dist_color * (T)l.bdl[e];
+            // (phi / 3) / dist_pos as phi times one per-edge factor
+            const T rq = ((T)1 / (T)3) / dist_pos;
             // each plane's value at the six points, v = fma(a, X, fma(b, Y, c));
             // phi = sum_i |vs_i - vt_i| in point order
             T vt[2 * P][6];
@@ -398,7 +403,7 @@ struct Engine
                         T term = std::fabs(vs[i] - vt[p][i]);
                         phi = i == 0 ? term : phi + term;
                     }
-                    phi = std::fmin(phi / (T)3 / dist_pos, (T)tau_smooth);
+                    phi = std::fmin(phi * rq, (T)tau_smooth);
                     T mm = std::fma(c0, phi, m_in[(size_t)p * E + e]);
                     if (mm < mn)
                         mn = mm;

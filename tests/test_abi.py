@@ -2,6 +2,7 @@
 declares; host-only entry points answer without a GPU."""
 import ctypes as C
 
+import numpy as np
 import pytest
 
 
@@ -80,3 +81,19 @@ def test_params_layout_matches_the_binding(lib):
     assert C.sizeof(E.Params) == L.hbp_params_size()
     p = E.default_params()
     assert (p.linkage, p.num_nb, p.sigma, p.msg_fp16, p.post) == (2, 4, 0.0, 0, 1)
+
+
+def test_volume_layout_helper(lib):
+    """volume_to_dhw inverts the Census volume layout the header states, at a
+    ragged size (W and H not multiples of the tile size)."""
+    E, L = lib
+    W, H, D = 19, 6, 7
+    rng = np.random.default_rng(3)
+    dhw = rng.integers(0, 26, (D, H, W), dtype=np.uint8)
+    TX = (W + 7) // 8
+    buf = np.zeros(E.volume_bytes(W, H, D), np.uint8)
+    for d in range(D):
+        for y in range(H):
+            for x in range(W):
+                buf[((y // 4 * TX + x // 8) * D + d) * 32 + (y % 4) * 8 + x % 8] = dhw[d, y, x]
+    assert np.array_equal(E.volume_to_dhw(buf, W, H, D), dhw.reshape(D, H * W))

@@ -23,3 +23,26 @@ def test_superpixel_mode_restatement(target):
         full, one = O.segment(lab), O.segment_target(lab, 1)
         for k in ("level_sizes", "clus", "mean", "bd", "bdl"):
             assert np.array_equal(full[k], one[k]), k
+
+
+@pytest.mark.parametrize("name", ["target_96x64_s7", "target_160x112_s11"])
+def test_superpixel_mode_against_reference(golden_dir, name):
+    """The reference build's superpixels (make_golden.py --only target): the
+    same level sizes and the same clus below the last level; at the last level
+    the reference hands labels out with atomicSub in no fixed order, so the
+    label images are compared as partitions (each oracle superpixel's majority
+    reference superpixel) and must agree on >= 98% of the pixels."""
+    import os
+    import pyoracle as O
+    z = dict(np.load(os.path.join(golden_dir, name + ".npz")))
+    lab = O.lab(z["left"])
+    for i, (link, nb, target) in enumerate(z["cfgs"].tolist()):
+        o = O.segment_target(lab, target, link, nb)
+        sizes = z[f"t{i}_level_sizes"]
+        assert np.array_equal(o["level_sizes"], sizes), (name, i)
+        n_last = int(sizes[-1, 0])
+        assert np.array_equal(o["clus"][:-n_last], z[f"t{i}_clus"][:-n_last]), (name, i)
+        ref = z[f"t{i}_labels"]
+        pairs = o["labels"].astype(np.int64).ravel() * target + ref.astype(np.int64).ravel()
+        cnt = np.bincount(pairs, minlength=target * target).reshape(target, target)
+        assert cnt.max(axis=1).sum() / ref.size >= 0.98, (name, i)

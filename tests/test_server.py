@@ -178,13 +178,15 @@ def test_small_requests_pass_a_large_one_that_does_not_fit(gpu):
     import time
     from scenes import make_scene
     prm = E.default_params(post=1)
-    big = [make_scene(450, 375, 64, 60 + i) for i in range(2)]
+    big = [make_scene(720, 496, 128, 60 + i) for i in range(2)]
     small = [make_scene(96, 64, 32, 70 + i) for i in range(3)]
-    budget = E.request_bytes(450, 375, 64) + 3 * E.request_bytes(96, 64, 32) + (64 << 20)
+    nb, ns = E.request_bytes(720, 496, 128), E.request_bytes(96, 64, 32)
+    budget = nb + 3 * ns + ns // 2  # the second large pair waits for the first's memory
+    assert 2 * nb > budget
     srv = E.Server(0, budget_bytes=budget, prep_lanes=2, params=prm)
     try:
         t0 = time.perf_counter()
-        ids = [(srv.submit(b.left, b.right, 64), time.perf_counter()) for b in big]
+        ids = [(srv.submit(b.left, b.right, 128), time.perf_counter()) for b in big]
         ids += [(srv.submit(s.left, s.right, 32), time.perf_counter()) for s in small]
         done = []
         for rid, ts in ids:
@@ -199,6 +201,6 @@ def test_small_requests_pass_a_large_one_that_does_not_fit(gpu):
     assert max(done[2:]) < done[1], done
     ctx = E.Context(0)
     try:
-        assert np.array_equal(second_big, ctx.run_pair(big[1].left, big[1].right, 64, prm))
+        assert np.array_equal(second_big, ctx.run_pair(big[1].left, big[1].right, 128, prm))
     finally:
         ctx.close()
