@@ -226,10 +226,14 @@ def autotune_rows(E, ctx, explore):
     buf = (C.c_double * (9 * n))()
     E.lib().hbp_autotune_table(ctx.h, buf, n)
     rows = [list(buf[9 * i:9 * i + 9]) for i in range(n)]
+    classes = {}
+    for r in rows:
+        key = (int(r[0]), int(r[1]), int(r[2]), int(r[3]), int(r[4]), int(r[5]))
+        classes.setdefault(key, []).append({"streams": int(r[6]), "bp_ms_per_view": round(r[7], 3),
+                                            "chosen": bool(r[8])})
     return {"exploration_batches": explore,
-            "tried": [{"streams": int(r[6]), "bp_ms_per_view": round(r[7], 3), "chosen": bool(r[8])} for r in rows],
-            "class": {"W": int(rows[0][0]), "H": int(rows[0][1]), "D": int(rows[0][2]), "msg_fp16": int(rows[0][3]),
-                      "post": int(rows[0][4]), "views": int(rows[0][5])}}
+            "classes": [{"W": k[0], "H": k[1], "D": k[2], "msg_fp16": k[3], "post": k[4], "views": k[5],
+                         "tried": v} for k, v in classes.items()]}
 
 
 def roofline_entry(name, prof, peak, peak_kind, hw, where):
