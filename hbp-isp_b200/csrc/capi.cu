@@ -1268,6 +1268,11 @@ struct ServerReq
 };
 
 size_t request_bytes(int W, int H, int D) { return slab_bytes((long)W * H, D); }
+
+// BP streams of the server's scheduler (pairs join the least-loaded one)
+#ifndef SERVER_BP_STREAMS
+#define SERVER_BP_STREAMS 8
+#endif
 } // namespace
 
 struct hbp_server
@@ -1472,7 +1477,7 @@ struct hbp_server
         // 8 schedulers on their own streams, ticked in turn; a joining pair
         // goes to the one with the fewest pairs in flight
         std::unique_ptr<BpPool> pool;
-        hbp_status pst = guarded([&] { pool = std::make_unique<BpPool>(q, 8); });
+        hbp_status pst = guarded([&] { pool = std::make_unique<BpPool>(q, SERVER_BP_STREAMS); });
         if (pst != HBP_OK)
         {
             std::lock_guard<std::mutex> lk(mu);

@@ -139,11 +139,17 @@ __global__ void iota_int(int *v, int n)
         v[i] = i;
 }
 
-__global__ void count_keys(const int *k, int n, int *count)
+// First list position of every node from the sorted node keys (every node
+// holds at least one pixel): off[key[i]] = i where a run of equal keys
+// starts, off[N] = n. No atomics: at coarse levels a count by atomics put
+// every pixel on a handful of counters.
+__global__ void run_starts(const uint32_t *key, int n, int N, int *off)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n)
-        atomicAdd(&count[k[i]], 1);
+    if (i < n && (i == 0 || key[i] != key[i - 1]))
+        off[key[i]] = i;
+    if (i == 0)
+        off[N] = n;
 }
 
 // A node's data-cost chunks are the 256-position windows of the level's pixel
@@ -977,10 +983,9 @@ __global__ void __launch_bounds__(128) k_init_nodes(const ViewDev *__restrict__ 
 
 // passing_msg_k + smooth_msg_k + normalize_msg_k (hbp_isp.cu:273-355), one
 // thread per edge. EDGES_MIN_BLOCKS bounds the register count (blocks of
-// 128 per SM); the kernel waits on plane loads and divergent divisions, so
-// occupancy matters.
+// 128 per SM).
 #ifndef EDGES_MIN_BLOCKS
-#define EDGES_MIN_BLOCKS 7
+#define EDGES_MIN_BLOCKS 5
 #endif
 __global__ void __launch_bounds__(128, EDGES_MIN_BLOCKS) k_edges(const ViewDev *__restrict__ V, StepDesc d)
 {
@@ -1043,22 +1048,18 @@ __global__ void __launch_bounds__(128, EDGES_MIN_BLOCKS) k_edges(const ViewDev *
     const float rq = (1.0f / 3.0f) / dist_pos;
     __shared__ float s_out[K][128];
     float sum = 0.f;
-    // Two passes, one per label group, so that only one group's point values
-    // (4 labels x 6 points) are held in registers: the first pass leaves each
-    // source label's group-0 minimum in s_out, the second adds the group-1
-    // minimum to it (msg_t = min_0 + min_1, the reference's order). phi(y, q)
-    // = sum_i |vs_y,i - vt_q,i| with v = fma(a, X_i, fma(b, Y_i, c)): each
-    // plane evaluated at the six points once per pass, two subtractions per
-    // point and label pair (the oracle states the same form).
-#pragma unroll 1
-    for (int g = 0; g < 2; ++g)
+    // The eight target labels' point values are held in registers (96
+    // registers, 5 blocks of 128 per SM; splitting the two label groups into
+    // two passes fits 7 blocks but reloads every source plane and measured 4%
+    // slower); per source label the two groups' minima, msg_t =
+    // (0 + min_0) + min_1 (the reference's order). phi(y, q) = sum_i |vs_y,i - vt_q,i| with
+    // v = fma(a, X_i, fma(b, Y_i, c)) (the oracle states the same form).
     {
-        float vt[P][6], mg[P];
+        float vt[2 * P][6];
 #pragma unroll
-        for (int k = 0; k < P; ++k)
+        for (int k = 0; k < 2 * P; ++k)
         {
-            const float4 tp = l.plane[(size_t)st.y * K + g * P + k];
-            mg[k] = mp[g * P + k];
+            const float4 tp = l.plane[(size_t)st.y * K + k];
 #pragma unroll
             for (int i = 0; i < 6; ++i)
                 vt[k][i] = __fmaf_rn(tp.x, X[i], __fmaf_rn(tp.y, Y[i], tp.z));
@@ -1067,35 +1068,31 @@ __global__ void __launch_bounds__(128, EDGES_MIN_BLOCKS) k_edges(const ViewDev *
         for (int y = 0; y < K; ++y)
         {
             const float4 ps = l.plane[(size_t)st.x * K + y];
-            // point by point: the source plane's value at point i, then each
-            // label's running sum (phi_k adds points 0..5 in order)
-            float phis[P];
+            float phis[2 * P];
 #pragma unroll
             for (int i = 0; i < 6; ++i)
             {
                 const float vs = __fmaf_rn(ps.x, X[i], __fmaf_rn(ps.y, Y[i], ps.z));
 #pragma unroll
-                for (int k = 0; k < P; ++k)
+                for (int k = 0; k < 2 * P; ++k)
                     phis[k] = i == 0 ? fabsf(vs - vt[k][0]) : phis[k] + fabsf(vs - vt[k][i]);
             }
-            // the group's minimum over its labels in slot order (a NaN never
-            // lowers it)
-            float mn = FLT_MAX;
+            float acc = 0.f;
 #pragma unroll
-            for (int k = 0; k < P; ++k)
+            for (int g = 0; g < 2; ++g)
             {
-                const float m = __fmaf_rn(c0, fminf(phis[k] * rq, tau), mg[k]);
-                if (m < mn)
-                    mn = m;
+                float mn = FLT_MAX;
+#pragma unroll
+                for (int k = 0; k < P; ++k)
+                {
+                    const float m = __fmaf_rn(c0, fminf(phis[g * P + k] * rq, tau), mp[g * P + k]);
+                    if (m < mn)
+                        mn = m;
+                }
+                acc = acc + mn;
             }
-            if (g == 0)
-                s_out[y][threadIdx.x] = 0.f + mn;
-            else
-            {
-                const float acc = s_out[y][threadIdx.x] + mn;
-                s_out[y][threadIdx.x] = acc;
-                sum = sum + acc;
-            }
+            s_out[y][threadIdx.x] = acc;
+            sum = sum + acc;
         }
     }
     float out[K];
@@ -1255,15 +1252,14 @@ void hbp_prepare(const Pyramid &pyr, const CostVolume &cv, const float *wta, int
             int *pix_off = persist.alloc<int>(N + 1);
             iota_xy<<<blocks(HW, 256), 256, 0, st>>>(kt, pix, im, W, HW);
             note_launch();
-            HBP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (N + 1), st));
-            count_keys<<<blocks(HW, 256), 256, 0, st>>>(im, HW, cnt);
-            note_launch();
             HBP_LAUNCH_CHECK();
             int bits = 1;
             while ((1 << bits) < N)
                 ++bits;
             radix_sort_pairs_u32(kt, pix, ka, va, HW, bits, tmp, st);
-            exclusive_scan(cnt, pix_off, N + 1, nullptr, tmp, st);
+            run_starts<<<blocks(HW, 256), 256, 0, st>>>(kt, HW, N, pix_off);
+            note_launch();
+            HBP_LAUNCH_CHECK();
             int *chunk_off = persist.alloc<int>(N + 1);
             chunk_counts<<<blocks(N + 1, 256), 256, 0, st>>>(pix_off, N, cnt);
             note_launch();
