@@ -80,7 +80,8 @@ def parse():
     ap.add_argument("--bp-streams", type=int, default=0,
                     help="BP streams of a batch (0: the engine's default; 1 for profiler captures)")
     ap.add_argument("--window", type=int, default=0,
-                    help="served requests in flight (default: the pairs per step)")
+                    help="served requests in flight (default: twice the pairs per step, so that the "
+                         "next pairs are prepared while the BP of the others runs)")
     ap.add_argument("--breakdown", action="store_true",
                     help="after the timed region, one extra step with every BP kernel of every 8th "
                          "BP step event-timed; per-kernel/per-level estimate printed to stderr")
@@ -511,7 +512,8 @@ def run_config(args, E, torch):
         res = {}
         for name, f16 in (("fp32", 0), ("fp16", 1)):
             prm = E.default_params(msg_fp16=f16, post=1)
-            E._check(E.lib().hbp_run_batch_d(ctx.h, n, arr(dL), arr(dR), W, H, D, C.byref(prm), arr(out), None))
+            for _ in range(4):  # warm-up, and the BP-stream autotuner's candidates (2, 4, 8)
+                E._check(E.lib().hbp_run_batch_d(ctx.h, n, arr(dL), arr(dR), W, H, D, C.byref(prm), arr(out), None))
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             E._check(E.lib().hbp_run_batch_d(ctx.h, n, arr(dL), arr(dR), W, H, D, C.byref(prm), arr(out), None))
@@ -522,13 +524,17 @@ def run_config(args, E, torch):
                          "bad1_pct": float(np.mean([bad(x, s, 1.0) for x, s in zip(d, scenes)])),
                          "bad2_pct": float(np.mean([bad(x, s, 2.0) for x, s in zip(d, scenes)]))}
         same = [float(np.mean(a == b)) for a, b in zip(res["fp16"]["disp"], res["fp32"]["disp"])]
-        ctx.close()
         for r in res.values():
             r.pop("disp")
-        return {"config": "precision", "workload": f"{n} synthetic pairs {W}x{H} D{D}, 40 segments, "
-                                                   "hbp_run_batch_d", "fp32": res["fp32"], "fp16": res["fp16"],
-                "fp16_vs_fp32_identical_mean": float(np.mean(same)),
-                "fp16_vs_fp32_identical_min": float(np.min(same))}
+        out = {"config": "precision", "workload": f"{n} synthetic pairs {W}x{H} D{D}, 40 segments, "
+                                                  "hbp_run_batch_d", "fp32": res["fp32"], "fp16": res["fp16"],
+               "fp16_vs_fp32_identical_mean": float(np.mean(same)),
+               "fp16_vs_fp32_identical_min": float(np.min(same)),
+               "autotune": autotune_rows(E, ctx, 4)}
+        if not args.no_cpu_baseline:
+            out["message_error_vs_fp64"] = message_error(scenes[0], D)
+        ctx.close()
+        return out
     if args.config == "mccnn":
         return run_mccnn(args, E, torch, local, bad)
     # serve: Poisson arrivals of the size mix, FP16 messages, 120 GB budget;
@@ -726,7 +732,7 @@ def main():
             # requests that the final drain (in-flight count falling to 0) is a
             # small part of the timed region
             n_req = max(NP * args.steps, 8 * NP)
-            window = args.window or NP
+            window = args.window or 2 * NP
             t0 = time.perf_counter()
             inflight = []
             k = 0
