@@ -79,6 +79,7 @@ def parse():
                     help="skip the untimed extra batches (accuracy, isolated roofline): for profiler captures")
     ap.add_argument("--bp-streams", type=int, default=0,
                     help="BP streams of a batch (0: the engine's default; 1 for profiler captures)")
+    ap.add_argument("--prep-lanes", type=int, default=8, help="served: the server's preparation lanes")
     ap.add_argument("--window", type=int, default=0,
                     help="served requests in flight (default: twice the pairs per step, so that the "
                          "next pairs are prepared while the BP of the others runs)")
@@ -721,7 +722,7 @@ def main():
     if not args.no_e2e:
         pinL = [torch.from_numpy(s.left).pin_memory().numpy() for s in scenes]
         pinR = [torch.from_numpy(s.right).pin_memory().numpy() for s in scenes]
-        srv = E.Server(local, budget_bytes=120 << 30, prep_lanes=8, params=prm)
+        srv = E.Server(local, budget_bytes=120 << 30, prep_lanes=args.prep_lanes, params=prm)
         try:
             ids = [srv.submit(pinL[i], pinR[i], D) for i in range(NP)]  # warm-up
             for i in ids:

@@ -2,7 +2,7 @@
 CUDA build (oracle/_ref/libhbpref.so, made by ``make -C oracle/ref``) on seeded
 synthetic scenes. It needs a GPU; run it on a B200 box:
 
-    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|target|post_gpu|lab_sweep]
+    python tests/golden/make_golden.py --out <dir> [--only census|mccnn|ad|seg|target|post_gpu|post_c1|lab_sweep]
 
 and copy ``<dir>/*.npz`` into tests/golden/. The fixtures hold the reference's
 outputs for every stage of the stereo path at small sizes (full arrays) and at
@@ -338,6 +338,24 @@ def target_record(ref: RefLib, W, H, seed):
     return rec
 
 
+def post_c1_record(ref: RefLib):
+    """Post-processing at the single-pair size (450x375, D 64, seed 1000): the
+    reference's own HBP results of both views, then its LR check + fill, its
+    weighted median (CPU variant) and its GPU variant, so that the tie order of
+    the median is pinned on many failed pixels."""
+    W, H, D, seed = 450, 375, 64, 1000
+    s = make_scene(W, H, D, seed)
+    L, R = s.left, s.right
+    disp, plane, _ = ref.hbp_pair(L, R, D)
+    dispR, planeR, _ = ref.hbp_pair(L, R, D, right_view=True)
+    post_d, post_p = ref.post(L, R, disp, plane, dispR, planeR, median=True)
+    lr_d, lr_p = ref.post(L, R, disp, plane, dispR, planeR, median=False)
+    gpu_d, gpu_p = ref.post(L, R, disp, plane, dispR, planeR, median=2)
+    return dict(W=W, H=H, D=D, seed=seed, left=L, right=R, disp=disp, plane=plane.astype(np.float32),
+                disp_right=dispR, plane_right=planeR.astype(np.float32), lr_disp=lr_d, post_disp=post_d,
+                post_gpu_disp=gpu_d, post_gpu_plane=gpu_p.astype(np.float32))
+
+
 def post_gpu_record(ref: RefLib, golden_dir: str):
     """median_filter_gpu on the reference's own HBP results stored in the small
     fixtures (both views' disparities and planes), and the device patch weights."""
@@ -377,7 +395,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--lib", default=None)
-    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "target", "post_gpu", "lab_sweep"],
+    ap.add_argument("--only", choices=["census", "mccnn", "ad", "seg", "target", "post_gpu", "post_c1", "lab_sweep"],
                     default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
@@ -404,6 +422,9 @@ def main():
             rec = target_record(ref, W, H, seed)
             np.savez_compressed(os.path.join(args.out, name + ".npz"), **rec)
             print(name, [int(rec[f"t{i}_level_sizes"].shape[0]) for i in range(len(TARGET_CFGS))])
+    if args.only in (None, "post_c1"):
+        np.savez_compressed(os.path.join(args.out, "post_450x375_d64_s1000.npz"), **post_c1_record(ref))
+        print("post_c1")
     if args.only in (None, "post_gpu"):
         # inputs: the reference's HBP results in the committed census fixtures
         src = os.path.dirname(os.path.abspath(__file__))
@@ -413,7 +434,7 @@ def main():
         rec = lab_sweep_record(ref)
         np.savez_compressed(os.path.join(args.out, "lab_overrides.npz"), **rec)
         print("lab_sweep: colours where the host pow differs:", len(rec["keys"]))
-    if args.only in ("mccnn", "ad", "seg", "target", "post_gpu", "lab_sweep"):
+    if args.only in ("mccnn", "ad", "seg", "target", "post_gpu", "post_c1", "lab_sweep"):
         return
 
     for (W, H, D, seed, full, name) in [

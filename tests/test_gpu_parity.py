@@ -294,3 +294,32 @@ def test_tiny_pairs_bit_exact(eng, W, H, D):
     got0 = ctx.run_pair(s.left, s.right, D, E.default_params(post=0))
     want0 = O.pipeline(s.left, s.right, D)["disp"]
     assert np.array_equal(got0.view(np.uint32), want0.view(np.uint32))
+
+
+def test_post_process_at_single_pair_size_vs_reference(eng, golden_dir):
+    """LR check + fill, the weighted median and its GPU variant on the
+    reference's own 450x375 D64 HBP results (thousands of failed pixels)
+    equal the reference build's outputs bit for bit."""
+    E, ctx, torch = eng
+    path = os.path.join(golden_dir, "post_450x375_d64_s1000.npz")
+    if not os.path.exists(path):
+        pytest.skip("make_golden.py --only post_c1 not run")
+    z = dict(np.load(path))
+    L = z["left"]
+    H, W = L.shape[:2]
+    for variant in ("cpu", "gpu"):
+        dL, dR = dev(torch, z["disp"]), dev(torch, z["disp_right"])
+        pl = dev(torch, z["plane"].reshape(-1))
+        fail = torch.zeros(H * W, dtype=torch.uint8, device="cuda")
+        dout = torch.zeros(H * W, dtype=torch.float32, device="cuda")
+        ctx.lr_check_d(dL, dR, pl, fail, dout, W, H)
+        assert np.array_equal(dout.cpu().numpy().reshape(H, W), z["lr_disp"])
+        if variant == "cpu":
+            ctx.weighted_median_d(dev(torch, L), fail, pl, dout, W, H)
+            want = z["post_disp"]
+        else:
+            ctx.weighted_median_gpu_d(dev(torch, L), fail, pl, dout, W, H)
+            want = z["post_gpu_disp"]
+        torch.cuda.synchronize()
+        got = dout.cpu().numpy().reshape(H, W)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (variant, int((got != want).sum()))

@@ -323,3 +323,24 @@ def test_float_path_against_fp64():
         d = O.pipeline(s.left, s.right, 48, **kw)["disp"]
         assert np.mean(np.abs(d - d64) < 1.0) >= 0.99, kw
         assert abs(bad(d) - bad(d64)) <= 0.1, kw
+
+
+def test_post_process_at_single_pair_size(golden_dir):
+    """LR check + fill, the weighted median (CPU variant's order) and the GPU
+    variant's order on the reference's own HBP results at 450x375 D64, where
+    thousands of failed pixels exercise the median's tie order: the oracle
+    reproduces the reference build's disparities bit for bit."""
+    import os
+    path = os.path.join(golden_dir, "post_450x375_d64_s1000.npz")
+    if not os.path.exists(path):
+        pytest.skip("make_golden.py --only post_c1 not run")
+    z = dict(np.load(path))
+    f = load(golden_dir, "post_gpu")
+    pl, fail = O.lr_check(z["disp"], z["disp_right"], z["plane"])
+    assert np.array_equal(O.plane_to_disp(pl), z["lr_disp"])
+    assert int(fail.sum()) > 1000
+    pm = O.weighted_median(z["left"], fail, pl, stable=False)
+    assert np.array_equal(O.plane_to_disp(pm), z["post_disp"])
+    pg = O.weighted_median_gpu(z["left"], fail, pl, f["patch_weights"], z_mode=0)
+    assert np.array_equal(pg.view(np.uint32), z["post_gpu_plane"].view(np.uint32))
+    assert np.array_equal(O.plane_to_disp(pg).view(np.uint32), z["post_gpu_disp"].view(np.uint32))
