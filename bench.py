@@ -730,9 +730,10 @@ def main():
             if dist:
                 dist.barrier()
             # a closed loop that refills as soon as any request completes; enough
-            # requests that the final drain (in-flight count falling to 0) is a
-            # small part of the timed region
-            n_req = max(NP * args.steps, 8 * NP)
+            # requests (40 batches' worth) that the ramp-up and the final drain
+            # (in-flight count rising from and falling to 0) are a small part
+            # of the timed region
+            n_req = max(NP * args.steps, 40 * NP)
             window = args.window or 2 * NP
             t0 = time.perf_counter()
             inflight = []
