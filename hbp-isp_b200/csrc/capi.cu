@@ -101,16 +101,20 @@ struct Slot
 
 // Online choice of the number of BP streams of a batch, per workload class
 // (image size, disparity range, message storage, post mode, views per batch):
-// the first batches of a class try each candidate once, timing the BP phase on
-// the host clock, and later batches use the fastest. Views never read one
-// another's data, so the streams change no result, only the speed.
+// the first batches of a class try each candidate twice (two rounds), timing
+// the BP phase on the host clock and keeping each candidate's faster trial (a
+// single trial can catch a one-off stall), and later batches use the fastest.
+// Views never read one another's data, so the streams change no result, only
+// the speed.
 struct AutoTune
 {
+    static constexpr int ROUNDS = 2;
     struct Entry
     {
         std::vector<int> cand;   // stream counts to try
-        std::vector<double> ms;  // BP ms per view of each tried candidate
-        int best = -1;           // index into cand once every candidate ran
+        std::vector<double> ms;  // BP ms per view of each candidate (the faster trial)
+        int trials = 0;          // batches measured
+        int best = -1;           // index into cand once every candidate ran ROUNDS times
     };
     bool on = true;
     std::map<std::array<int, 6>, Entry> table;
@@ -996,7 +1000,8 @@ void run_pairs(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, const uint8_t
                         tune->cand.push_back(s);
             if (tune->cand.empty())
                 tune->cand.push_back(1);
-            q.bp_streams = tune->best >= 0 ? tune->cand[(size_t)tune->best] : tune->cand[tune->ms.size()];
+            q.bp_streams = tune->best >= 0 ? tune->cand[(size_t)tune->best]
+                                           : tune->cand[(size_t)tune->trials % tune->cand.size()];
         }
         c->prof.on = c->prof_mode != 0;
         c->tmp.reset();
@@ -1007,8 +1012,13 @@ void run_pairs(hbp_ctx *c, int npairs, const uint8_t *const *bgrL, const uint8_t
         }
         if (tune && tune->best < 0)
         {
-            tune->ms.push_back(ms_since(t_views) / (double)views.size());
-            if (tune->ms.size() == tune->cand.size())
+            const double ms = ms_since(t_views) / (double)views.size();
+            const size_t i = (size_t)tune->trials % tune->cand.size();
+            if (i >= tune->ms.size())
+                tune->ms.push_back(ms);
+            else
+                tune->ms[i] = std::min(tune->ms[i], ms);
+            if (++tune->trials == AutoTune::ROUNDS * (int)tune->cand.size())
                 tune->best = (int)(std::min_element(tune->ms.begin(), tune->ms.end()) - tune->ms.begin());
         }
         c->phase_ms[1] += ms_since(t_bp);

@@ -283,10 +283,11 @@ hbp_status hbp_set_lanes(hbp_ctx *ctx, int lanes);
 hbp_status hbp_set_bp_streams(hbp_ctx *ctx, int streams);
 /* While the stream count is automatic (0), batches autotune it (no reference
  * counterpart): per class (W, H, D, msg_fp16, post, views per batch) the first
- * batches try 2, 4, 8, 12 and 16 streams (those not above the views), one
- * batch each, timing the BP phase, and later batches use the fastest. The
- * streams change no result. on = 0 turns it off (the default 8 streams, two
- * views each). */
+ * batches try 2, 4, 8, 12 and 16 streams (those not above the views), two
+ * batches each in two rounds, timing the BP phase and keeping each count's
+ * faster batch, and later batches use the fastest. The streams change no
+ * result. on = 0 turns it off (the default 8 streams, two views each). The
+ * table's rows hold each count's faster batch. */
 hbp_status hbp_set_autotune(hbp_ctx *ctx, int on);
 /* The autotuner's measurements: up to max_rows rows of 9 doubles (W, H, D,
  * msg_fp16, post, views, streams, BP ms per view, 1 if chosen); returns the
