@@ -574,17 +574,38 @@ hbp_status hbp_segment_target_d(hbp_ctx *c, const uint8_t *bgr, int W, int H, in
     });
 }
 
-hbp_status hbp_segment_labels_d(hbp_ctx *c, int *labels, int *num_clusters, void *stream)
+hbp_status hbp_segment_draw_d(hbp_ctx *c, int level, int format, const uint8_t *bgr, void *out, void *stream)
 {
-    if (!c || !labels || !c->have_pyr)
+    if (!c || !out || !c->have_pyr)
         return fail(HBP_ERR_INVALID_ARG, "null pointer or no pyramid");
+    if (level < -1 || level >= c->pyr.L)
+        return fail(HBP_ERR_INVALID_ARG, "level must be -1 (the last) or 0 .. levels-1");
+    if (format < SEG_DRAW_UCHAR3 || format > SEG_DRAW_BOUNDARY)
+        return fail(HBP_ERR_INVALID_ARG, "format must be 0 (label BGR bytes), 1 (label ints) or 2 (boundaries)");
+    if (format == SEG_DRAW_BOUNDARY && !bgr)
+        return fail(HBP_ERR_INVALID_ARG, "the boundary picture needs the BGR image");
     return guarded([&] {
         HBP_CUDA(cudaSetDevice(c->device));
         cudaStream_t st = pick(c, stream);
         c->tmp.reset();
-        launch_top_labels(c->pyr, labels, c->tmp, st);
+        launch_draw_segmentation(c->pyr, level < 0 ? c->pyr.L - 1 : level, format, bgr, out, c->tmp, st);
+    });
+}
+
+hbp_status hbp_segment_labels_d(hbp_ctx *c, int level, int *labels, int *num_clusters, void *stream)
+{
+    if (!c || !labels || !c->have_pyr)
+        return fail(HBP_ERR_INVALID_ARG, "null pointer or no pyramid");
+    if (level < -1 || level >= c->pyr.L)
+        return fail(HBP_ERR_INVALID_ARG, "level must be -1 (the last) or 0 .. levels-1");
+    return guarded([&] {
+        HBP_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = pick(c, stream);
+        const int lv = level < 0 ? c->pyr.L - 1 : level;
+        c->tmp.reset();
+        launch_level_labels(c->pyr, lv, labels, c->tmp, st);
         if (num_clusters)
-            *num_clusters = top_cluster_count(c->pyr, c->tmp, st);
+            *num_clusters = level_cluster_count(c->pyr, lv, c->tmp, st);
         HBP_CUDA(cudaStreamSynchronize(st));
     });
 }

@@ -146,10 +146,21 @@ struct SegConfig
 // Rejects configurations the reference cannot run (HBP_ERR_INVALID_ARG).
 void check_seg_config(const SegConfig &cfg);
 struct Pyramid;
-// Each pixel's cluster at the pyramid's last level (LabelIntFormat), and the
-// number of those clusters.
-void launch_top_labels(const Pyramid &pyr, int *labels, Arena &tmp, cudaStream_t st);
-int top_cluster_count(const Pyramid &pyr, Arena &tmp, cudaStream_t st);
+// Each pixel's cluster after pyramid level `level` (LabelIntFormat, 0-based
+// labels), and the number of those clusters.
+void launch_level_labels(const Pyramid &pyr, int level, int *labels, Arena &tmp, cudaStream_t st);
+int level_cluster_count(const Pyramid &pyr, int level, Arena &tmp, cudaStream_t st);
+// draw_segmentation's pictures of that label image, in the reference's
+// SegFormat numbering: W*H*3 bytes (label+1 as BGR bytes, or the boundaries
+// in red over `bgr`) or W*H ints (label+1).
+enum SegDraw
+{
+    SEG_DRAW_UCHAR3 = 0,
+    SEG_DRAW_INT = 1,
+    SEG_DRAW_BOUNDARY = 2
+};
+void launch_draw_segmentation(const Pyramid &pyr, int level, int format, const uint8_t *bgr, void *out,
+                              Arena &tmp, cudaStream_t st);
 
 // segment.cu: SegHAC::run_ms with LabelISPFormat and cfg.target. Uses `a` for
 // the pyramid and `tmp` for temporaries; the host learns each level's size

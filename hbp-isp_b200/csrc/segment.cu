@@ -394,8 +394,8 @@ void target_relabel(int *clus, const float *dmin, int N, int Nn, int target, Are
 
 namespace
 {
-// update_image_label through every level (segment.cu:871-883): a pixel's
-// label is its node's parent at the last level, clus_{L-1}(...clus_0(px)).
+// update_image_label through levels 0..L-1 (segment.cu:871-883): a pixel's
+// label is clus_{L-1}(...clus_0(px)), its cluster after level L-1.
 __global__ void top_labels(const int *clus, const long *node_off, int L, int n, int *labels)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -413,9 +413,53 @@ __global__ void max_label(const int *clus, int n, int *mx)
     if (i < n)
         atomicMax(mx, clus[i]);
 }
+
+// draw_segmentation's three pictures of a label image (segment.cu:907-951,
+// kernels :213-292): label+1 as a BGR byte triple (low byte first), label+1
+// as an int, or the input image with the pixels whose left or upper
+// neighbour lies in another cluster painted red (0,0,255).
+__global__ void draw_labels(const int *labels, const uint8_t *bgr, int W, int H, int format, void *out)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W)
+        return;
+    const int i = y * W + x, c = labels[i];
+    if (format == SEG_DRAW_INT)
+    {
+        static_cast<int *>(out)[i] = c + 1;
+        return;
+    }
+    uint8_t *o = static_cast<uint8_t *>(out) + 3 * (size_t)i;
+    if (format == SEG_DRAW_UCHAR3)
+    {
+        const unsigned v = (unsigned)(c + 1);
+        o[0] = (uint8_t)v;
+        o[1] = (uint8_t)(v >> 8);
+        o[2] = (uint8_t)(v >> 16);
+        return;
+    }
+    const bool edge = (x > 0 && labels[i - 1] != c) || (y > 0 && labels[i - W] != c);
+    const uint8_t *s = bgr + 3 * (size_t)i;
+    o[0] = edge ? 0 : s[0];
+    o[1] = edge ? 0 : s[1];
+    o[2] = edge ? 255 : s[2];
+}
 } // namespace
 
-void launch_top_labels(const Pyramid &pyr, int *labels, Arena &tmp, cudaStream_t st)
+void launch_draw_segmentation(const Pyramid &pyr, int level, int format, const uint8_t *bgr, void *out,
+                              Arena &tmp, cudaStream_t st)
+{
+    size_t m = tmp.mark();
+    int *labels = tmp.alloc<int>((size_t)pyr.W * pyr.H);
+    launch_level_labels(pyr, level, labels, tmp, st);
+    draw_labels<<<dim3(ceil_div(pyr.W, 128), pyr.H), 128, 0, st>>>(labels, bgr, pyr.W, pyr.H, format, out);
+    note_launch();
+    HBP_LAUNCH_CHECK();
+    HBP_CUDA(cudaStreamSynchronize(st));
+    tmp.rewind(m);
+}
+
+void launch_level_labels(const Pyramid &pyr, int level, int *labels, Arena &tmp, cudaStream_t st)
 {
     // the level offsets as a small device array (the pageable copy is staged
     // before cudaMemcpyAsync returns)
@@ -424,15 +468,17 @@ void launch_top_labels(const Pyramid &pyr, int *labels, Arena &tmp, cudaStream_t
     long *doff = tmp.alloc<long>(off.size());
     HBP_CUDA(cudaMemcpyAsync(doff, off.data(), sizeof(long) * off.size(), cudaMemcpyHostToDevice, st));
     const int n = pyr.W * pyr.H;
-    top_labels<<<ceil_div(n, 256), 256, 0, st>>>(pyr.clus, doff, pyr.L, n, labels);
+    top_labels<<<ceil_div(n, 256), 256, 0, st>>>(pyr.clus, doff, level + 1, n, labels);
     note_launch();
     HBP_LAUNCH_CHECK();
     HBP_CUDA(cudaStreamSynchronize(st));
     tmp.rewind(m);
 }
 
-int top_cluster_count(const Pyramid &pyr, Arena &tmp, cudaStream_t st)
+int level_cluster_count(const Pyramid &pyr, int level, Arena &tmp, cudaStream_t st)
 {
+    if (level + 1 < pyr.L)
+        return pyr.N[level + 1];
     size_t m = tmp.mark();
     int *mx = tmp.alloc<int>(1);
     HBP_CUDA(cudaMemsetAsync(mx, 0, sizeof(int), st));

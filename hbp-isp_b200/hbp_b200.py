@@ -218,11 +218,16 @@ class Context:
                                           C.byref(L), None))
         return L.value
 
-    def segment_labels_d(self, labels) -> int:
-        """Every pixel's cluster at the pyramid's last level (device ints);
-        returns the number of clusters."""
+    def segment_draw_d(self, out, fmt: int, bgr=None, level: int = -1) -> None:
+        """SegHAC's picture of level `level` into device memory `out`: fmt 0
+        label+1 as BGR bytes, 1 label+1 as ints, 2 the boundaries over `bgr`."""
+        _check(lib().hbp_segment_draw_d(self.h, level, fmt, _p(bgr), _p(out), None))
+
+    def segment_labels_d(self, labels, level: int = -1) -> int:
+        """Every pixel's cluster after pyramid level `level` (-1: the last)
+        as device ints; returns the number of clusters."""
         k = C.c_int(0)
-        _check(lib().hbp_segment_labels_d(self.h, _p(labels), C.byref(k), None))
+        _check(lib().hbp_segment_labels_d(self.h, level, _p(labels), C.byref(k), None))
         return k.value
 
     def lab_sigma_d(self, bgr, W, H, sigma, lab4):

@@ -154,10 +154,22 @@ hbp_status hbp_segment_cfg_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int
 hbp_status hbp_segment_target_d(hbp_ctx *ctx, const uint8_t *bgr, int W, int H, int linkage, int num_nb,
                                 double sigma, int target_clus, int *levels, void *stream);
 /* SegHAC's LabelIntFormat output (update_image_label, segment.cu:871-883,
- * draw_segmentation :912-951) for the context's pyramid: every pixel's
- * cluster at the last level (W*H ints on the device), and the number of
- * those clusters in *num_clusters (may be NULL). Synchronous. */
-hbp_status hbp_segment_labels_d(hbp_ctx *ctx, int *labels, int *num_clusters, void *stream);
+ * draw_segmentation :907-951) for the context's pyramid: every pixel's
+ * cluster after pyramid level `level` (0 .. levels-1; -1 = the last level,
+ * the superpixels of the target mode), W*H ints on the device, numbered from
+ * 0 (the reference's image adds 1), and the number of those clusters in
+ * *num_clusters (may be NULL). The reference draws one such image per level
+ * with target_clus 1 and only the last otherwise. Synchronous. */
+hbp_status hbp_segment_labels_d(hbp_ctx *ctx, int level, int *labels, int *num_clusters, void *stream);
+
+/* SegHAC::draw_segmentation (segment.cu:907-951) for pyramid level `level`
+ * (-1 = the last), with the reference's SegFormat numbers: format 0
+ * (LabelUchar3Format) writes W*H*3 bytes, label+1 as B,G,R = bits 0-7, 8-15,
+ * 16-23; format 1 (LabelIntFormat) writes W*H ints, label+1; format 2
+ * (BoundaryFormat) writes W*H*3 bytes, the BGR image `bgr` (device, the one
+ * segmented) with every pixel whose left or upper neighbour has another label
+ * set to (0,0,255). `out` is device memory. Synchronous. */
+hbp_status hbp_segment_draw_d(hbp_ctx *ctx, int level, int format, const uint8_t *bgr, void *out, void *stream);
 /* SegHAC::img_CPU_to_GPU with sigma (segment.cu:795-809): CIELAB float4 of
  * the blurred image (the fourth channel is the blurred constant 1), into
  * lab4 (W*H float4). sigma = 0 gives hbp_lab_d's result. */

@@ -18,16 +18,18 @@
 namespace hbp_isp
 {
 
-// Element types, with OpenCV's codes (CV_8UC1, CV_8UC3, CV_32FC1, CV_32FC3).
+// Element types, with OpenCV's codes (CV_8UC1, CV_8UC3, CV_32SC1, CV_32FC1,
+// CV_32FC3).
 enum MatType
 {
     MAT_8UC1 = 0,
     MAT_8UC3 = 16,
+    MAT_32SC1 = 4,
     MAT_32FC1 = 5,
     MAT_32FC3 = 21
 };
 
-// A host image: rows x cols x channels of uint8 or float, row-major and
+// A host image: rows x cols x channels of uint8, int32 or float, row-major and
 // contiguous (cv::Mat's continuous layout). It owns its pixels, or wraps a
 // caller's buffer (a cv::Mat's .data, for instance) without copying.
 class Mat
@@ -46,7 +48,7 @@ class Mat
 
     int type() const { return type_; }
     int channels() const { return type_ == MAT_8UC3 || type_ == MAT_32FC3 ? 3 : 1; }
-    size_t elemSize1() const { return type_ == MAT_32FC1 || type_ == MAT_32FC3 ? 4 : 1; }
+    size_t elemSize1() const { return type_ == MAT_32FC1 || type_ == MAT_32FC3 || type_ == MAT_32SC1 ? 4 : 1; }
     size_t elemSize() const { return elemSize1() * (size_t)channels(); }
     size_t total() const { return (size_t)rows * (size_t)cols; }
     size_t bytes() const { return total() * elemSize(); }

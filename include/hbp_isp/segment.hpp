@@ -1,9 +1,10 @@
 // SegHAC with the reference's interface (segment.hpp:8-27, :248): the image
-// segmentation pyramid on the B200 engine (hbp_segment_cfg_d). Offered: every
-// linkage (CentoridLink is the reference's spelling), 4 or 8 neighbours,
-// sigma with round(3 sigma) <= 7, LabelISPFormat, target 1; other formats,
-// superpixel targets and cycle display are rejected. Each SegHAC owns the
-// engine context that holds its pyramid; ISPData shares it.
+// segmentation pyramid on the B200 engine (hbp_segment_target_d). Offered:
+// every linkage (CentoridLink is the reference's spelling), 4 or 8
+// neighbours, sigma with round(3 sigma) <= 7, every output format, the full
+// hierarchy (target_clus 1) or target_clus superpixels; the cycle-root
+// display (show_cycle) is rejected. Each SegHAC owns the engine context that
+// holds its pyramid; ISPData shares it.
 #pragma once
 
 #include <cmath>
@@ -38,24 +39,50 @@ class SegHAC
         : width(src.cols), height(src.rows), m_link(link), m_num_nb(num_nb), m_sigma(sigma)
     {
         detail::need_bgr(src, "SegHAC");
-        if (seg_format != LabelISPFormat || target_clus != 1 || show_cycle)
-            throw std::invalid_argument("SegHAC: offered for LabelISPFormat, target 1, no cycle display");
+        if (seg_format < LabelUchar3Format || seg_format > EmptyFormat)
+            throw std::invalid_argument("SegHAC: unknown output format");
+        if (target_clus < 1 || (long)target_clus >= (long)width * height)
+            throw std::invalid_argument("SegHAC: target_clus must lie in [1, pixels)");
+        if (show_cycle)
+            throw std::invalid_argument("SegHAC: the cycle-root display is not offered");
         if (link < MinLink || link > WardLink || (num_nb != 4 && num_nb != 8) || !(sigma >= 0.0) ||
             (int)std::round(3 * sigma) > 7)
             throw std::invalid_argument("SegHAC: linkage Min/Max/Centroid/Ward, 4 or 8 neighbours, "
                                         "round(3 sigma) <= 7");
+        m_format = seg_format;
+        m_target = target_clus;
         img = detail::upload(src);
         ctx = std::make_shared<detail::Ctx>();
     }
 
-    // run_ms (segment.cu:1279-1321). With LabelISPFormat the reference leaves
-    // segs untouched (save_output, :1099-1113), and so does this. Each run
-    // builds the pyramid from the current image anew.
+    // run_ms (segment.cu:1279-1321) with save_output's pictures (:1096-1111):
+    // LabelISPFormat and EmptyFormat leave segs untouched; the other formats
+    // append one picture per level with target_clus 1, else one of the
+    // target_clus superpixels. LabelUchar3Format and BoundaryFormat give
+    // CV_8UC3 pictures, LabelIntFormat CV_32SC1 (labels from 1), and
+    // LabelDeviceIntFormat, which the reference draws nothing for, empty
+    // Mats. Each run builds the pyramid from the current image anew.
     void run_ms(std::vector<Mat> *segs = nullptr)
     {
-        (void)segs;
-        detail::check(hbp_segment_cfg_d(ctx->h, img->as<uint8_t>(), width, height, (int)m_link, m_num_nb, m_sigma,
-                                        &levels, nullptr));
+        detail::check(hbp_segment_target_d(ctx->h, img->as<uint8_t>(), width, height, (int)m_link, m_num_nb,
+                                           m_sigma, m_target, &levels, nullptr));
+        if (m_format == LabelISPFormat || m_format == EmptyFormat)
+            return;
+        if (!segs)
+            throw std::invalid_argument("SegHAC::run_ms: this output format needs a picture list");
+        for (int l = m_target == 1 ? 0 : levels - 1; l < levels; ++l)
+        {
+            if (m_format == LabelDeviceIntFormat)
+            {
+                segs->emplace_back();
+                continue;
+            }
+            Mat pic(height, width, m_format == LabelIntFormat ? MAT_32SC1 : MAT_8UC3);
+            detail::DevBuf out(pic.bytes());
+            detail::check(hbp_segment_draw_d(ctx->h, l, (int)m_format, img->as<uint8_t>(), out.p, nullptr));
+            detail::check(hbp_copy(pic.data, out.p, pic.bytes()));
+            segs->push_back(pic);
+        }
     }
 
     // set_frame (segment.hpp:87-91): the next image of a video stream, same size
@@ -122,6 +149,8 @@ class SegHAC
     Linkage m_link;
     int m_num_nb;
     double m_sigma;
+    SegFormat m_format = LabelISPFormat;
+    int m_target = 1;
     int levels = 0;
     detail::Buf img;
 };
@@ -132,7 +161,12 @@ using hbp_isp::CentoridLink;
 using hbp_isp::MaxLink;
 using hbp_isp::MinLink;
 using hbp_isp::WardLink;
+using hbp_isp::BoundaryFormat;
+using hbp_isp::EmptyFormat;
+using hbp_isp::LabelDeviceIntFormat;
+using hbp_isp::LabelIntFormat;
 using hbp_isp::LabelISPFormat;
+using hbp_isp::LabelUchar3Format;
 using hbp_isp::Linkage;
 using hbp_isp::SegFormat;
 using hbp_isp::SegHAC;

@@ -8,7 +8,9 @@
 // volume file, the MC-CNN cost (alpha 1.3, bench_MiddV3_train.sh:6). Writes
 // <out_prefix>{census,ad,mccnn}_{single,lr,lr_gpu,levels}.f32 (lr_gpu: the LR
 // flow with median_filter_gpu; levels: every level's disparity from
-// HBP_ISP::run_ms_vis, top level first).
+// HBP_ISP::run_ms_vis, top level first), and SegHAC's pictures of the left
+// image (segment.cu:1096-1111): <out_prefix>seg_{int,u3,bd}_t{1,60}.bin, the
+// pictures of run_ms(&segs) concatenated.
 // usage: compat_pipeline left.bgr right.bgr W H D out_prefix [vol.acrt]
 #include <cstdio>
 #include <cstdlib>
@@ -125,6 +127,40 @@ static void stream_check(const Mat &L, const Mat &R)
         throw std::runtime_error("set_seq_img + run_ms differs from a fresh SegHAC");
 }
 
+// SegHAC's picture formats: the full hierarchy (target 1, one picture per
+// level) and 60 superpixels (one picture), Ward linkage with 8 neighbours.
+static void seg_pictures(const Mat &L, const std::string &out)
+{
+    const std::pair<SegFormat, const char *> fmts[] = {
+        {LabelIntFormat, "int"}, {LabelUchar3Format, "u3"}, {BoundaryFormat, "bd"}};
+    for (int target : {1, 60})
+        for (const auto &f : fmts)
+        {
+            SegHAC seg(L, WardLink, 8, 0, f.first, target, false);
+            std::vector<Mat> segs;
+            seg.run_ms(&segs);
+            if ((int)segs.size() != (target == 1 ? seg.g_levels() : 1))
+                throw std::runtime_error("SegHAC::run_ms gave the wrong number of pictures");
+            std::ofstream o(out + "seg_" + f.second + "_t" + std::to_string(target) + ".bin", std::ios::binary);
+            for (const Mat &m : segs)
+                o.write(reinterpret_cast<const char *>(m.data), (std::streamsize)m.bytes());
+        }
+    // the formats that give no picture
+    std::vector<Mat> segs;
+    SegHAC dev(L, WardLink, 8, 0, LabelDeviceIntFormat, 1, false);
+    dev.run_ms(&segs);
+    for (const Mat &m : segs)
+        if (!m.empty())
+            throw std::runtime_error("LabelDeviceIntFormat gave a picture");
+    if ((int)segs.size() != dev.g_levels())
+        throw std::runtime_error("LabelDeviceIntFormat: one empty picture per level expected");
+    SegHAC none(L, WardLink, 8, 0, EmptyFormat, 1, false);
+    segs.clear();
+    none.run_ms(&segs);
+    if (!segs.empty())
+        throw std::runtime_error("EmptyFormat gave pictures");
+}
+
 int main(int argc, char **argv)
 {
     if (argc != 7 && argc != 8)
@@ -138,6 +174,7 @@ int main(int argc, char **argv)
     {
         Mat L = read_bgr(argv[1], W, H), R = read_bgr(argv[2], W, H);
         stream_check(L, R);
+        seg_pictures(L, out);
         flows(L, R, D, "Census", "", 1000.1f, out + "census");
         flows(L, R, D, "AD", "", 1000.1f, out + "ad");
         if (argc == 8)

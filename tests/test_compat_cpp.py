@@ -123,10 +123,58 @@ def test_driver_flows_match_the_engine(tmp_path):
         lr_gpu = dout.cpu().numpy().reshape(H, W)
     finally:
         ctx.close()
+    _check_seg_pictures(tmp_path, s, W, H)
     assert _same(out("census_single"), want1) and _same(out("census_lr"), want2)
     assert _same(out("census_levels"), levels)
     assert _same(out("census_lr_gpu"), lr_gpu)
     assert _same(out("ad_single"), ad1) and _same(out("ad_lr"), ad2)
+
+
+def _draw(labels, bgr, fmt):
+    """draw_segmentation's pictures (segment.cu:213-292) of a 0-based label
+    image, restated in numpy: "int" label+1; "u3" label+1 as B,G,R bytes, low
+    byte first; "bd" the image with pixels unlike their left or upper
+    neighbour set to (0,0,255)."""
+    c = labels.astype(np.int64) + 1
+    if fmt == "int":
+        return c.astype(np.int32)
+    if fmt == "u3":
+        return np.stack([c & 255, (c >> 8) & 255, (c >> 16) & 255], -1).astype(np.uint8)
+    edge = np.zeros(labels.shape, bool)
+    edge[:, 1:] |= labels[:, 1:] != labels[:, :-1]
+    edge[1:, :] |= labels[1:, :] != labels[:-1, :]
+    out = bgr.copy()
+    out[edge] = (0, 0, 255)
+    return out
+
+
+def _check_seg_pictures(tmp_path, s, W, H):
+    """SegHAC::run_ms(&segs) in each picture format (Ward, 8 neighbours) against
+    the engine's label image of every level (target 1) or of the 60
+    superpixels, drawn by the reference's rules."""
+    import hbp_b200 as E
+    import torch
+    ctx = E.Context(0)
+    try:
+        img = torch.from_numpy(np.ascontiguousarray(s.left)).cuda()
+        for target in (1, 60):
+            L = ctx.segment_target_d(img, W, H, 3, 8, 0.0, target)
+            levels = range(L) if target == 1 else [L - 1]
+            labels = []
+            for lv in levels:
+                t = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+                k = ctx.segment_labels_d(t, lv)
+                lab = t.cpu().numpy().reshape(H, W)
+                assert np.array_equal(np.unique(lab), np.arange(k))
+                labels.append(lab)
+            assert target == 1 or len(np.unique(labels[0])) == target
+            for fmt, dt, ch in (("int", np.int32, 1), ("u3", np.uint8, 3), ("bd", np.uint8, 3)):
+                got = np.fromfile(tmp_path / f"o_seg_{fmt}_t{target}.bin", dt)
+                want = np.concatenate([_draw(lab, s.left, fmt).ravel() for lab in labels])
+                assert got.shape == want.shape, (fmt, target)
+                assert np.array_equal(got, want), (fmt, target)
+    finally:
+        ctx.close()
 
 
 @pytest.mark.gpu

@@ -65,6 +65,54 @@ def test_pyramid_variants_bit_exact(eng, golden_dir, cfg):
         assert np.array_equal(g[k], z[f"c{i}_{k}"]), k
 
 
+@pytest.mark.parametrize("cfg", [(2, 4, 0.0), (3, 8, 0.7)])
+def test_level_pictures(eng, cfg):
+    """The label image of every level (update_image_label, segment.cu:871-883)
+    is the oracle's clus maps composed through that level, and the three
+    pictures of draw_segmentation (:907-951) follow from it: label+1 as ints,
+    label+1 as B,G,R bytes (low byte first), boundaries in red over the image."""
+    import pyoracle as O
+    from scenes import make_scene
+    E, ctx, torch = eng
+    link, nb, sigma = cfg
+    s = make_scene(160, 112, 32, 13)
+    H, W = 112, 160
+    img = torch.from_numpy(np.ascontiguousarray(s.left)).cuda()
+    L = ctx.segment_cfg_d(img, W, H, link, nb, sigma)
+    o = O.segment(_lab(E, ctx, torch, s.left, sigma), link, nb)
+    sizes = o["level_sizes"][:, 0]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    comp = np.arange(H * W)
+    labels = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+    pic_i = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+    pic_b = torch.zeros(H * W * 3, dtype=torch.uint8, device="cuda")
+    assert L == len(sizes)
+    for lv in range(L):
+        comp = o["clus"][off[lv]:off[lv + 1]][comp]
+        k = ctx.segment_labels_d(labels, lv)
+        lab = labels.cpu().numpy()
+        assert np.array_equal(lab, comp), lv
+        assert k == (sizes[lv + 1] if lv + 1 < L else 1)
+        c = comp.astype(np.int64) + 1
+        ctx.segment_draw_d(pic_i, 1, level=lv)
+        assert np.array_equal(pic_i.cpu().numpy(), c)
+        ctx.segment_draw_d(pic_b, 0, level=lv)
+        u3 = np.stack([c & 255, (c >> 8) & 255, (c >> 16) & 255], -1).astype(np.uint8)
+        assert np.array_equal(pic_b.cpu().numpy().reshape(-1, 3), u3)
+        ctx.segment_draw_d(pic_b, 2, bgr=img, level=lv)
+        g = comp.reshape(H, W)
+        edge = np.zeros((H, W), bool)
+        edge[:, 1:] |= g[:, 1:] != g[:, :-1]
+        edge[1:, :] |= g[1:, :] != g[:-1, :]
+        bd = s.left.copy()
+        bd[edge] = (0, 0, 255)
+        assert np.array_equal(pic_b.cpu().numpy().reshape(H, W, 3), bd)
+    with pytest.raises(E.HbpError):
+        ctx.segment_labels_d(labels, L)
+    with pytest.raises(E.HbpError):
+        ctx.segment_draw_d(pic_b, 2, level=0)  # the boundary picture needs the image
+
+
 @pytest.mark.parametrize("cfg", [(0, 8, 0.0), (3, 4, 0.7)])
 def test_pair_with_variant_segmentation(eng, cfg):
     """hbp_run_pair with the configuration in hbp_params equals the oracle's
