@@ -2,7 +2,9 @@
 // CRTrees, SegHAC, ISPData, StereoData, HBP_ISP, PostProcess, medianFilter),
 // header-only, on top of the C ABI of libhbp_b200.so (include/hbp_b200.h).
 // This file: the image type standing in for cv::Mat, device buffers and
-// contexts, error handling.
+// contexts, error handling. Where <opencv2/core.hpp> is on the include path,
+// hbp_isp::Mat converts from and to cv::Mat, so the reference's call sites
+// can pass and receive cv::Mat.
 #pragma once
 
 #include <cstdint>
@@ -14,6 +16,11 @@
 #include <vector>
 
 #include "../hbp_b200.h"
+
+#if __has_include(<opencv2/core.hpp>)
+#include <opencv2/core.hpp>
+#define HBP_ISP_WITH_OPENCV 1
+#endif
 
 namespace hbp_isp
 {
@@ -45,6 +52,20 @@ class Mat
         data = own_->data();
     }
     Mat(int r, int c, int type, void *external) : rows(r), cols(c), data(static_cast<uint8_t *>(external)), type_(type) {}
+#ifdef HBP_ISP_WITH_OPENCV
+    // a cv::Mat's pixels, wrapped without copying (the cv::Mat keeps them):
+    // continuous and of one of the types above
+    Mat(const cv::Mat &m) : rows(m.rows), cols(m.cols), data(static_cast<uint8_t *>(m.data)), type_(m.type())
+    {
+        const bool known = type_ == MAT_8UC1 || type_ == MAT_8UC3 || type_ == MAT_32SC1 || type_ == MAT_32FC1 ||
+                           type_ == MAT_32FC3;
+        if (!m.empty() && (!known || !m.isContinuous()))
+            throw std::invalid_argument("hbp_isp::Mat: a continuous cv::Mat of type CV_8UC1, CV_8UC3, CV_32SC1, "
+                                        "CV_32FC1 or CV_32FC3 is required");
+    }
+    // a cv::Mat holding a copy of these pixels
+    operator cv::Mat() const { return empty() ? cv::Mat() : cv::Mat(rows, cols, type_, data).clone(); }
+#endif
 
     int type() const { return type_; }
     int channels() const { return type_ == MAT_8UC3 || type_ == MAT_32FC3 ? 3 : 1; }

@@ -27,6 +27,20 @@ def test_headers_compile():
     _compile(None, syntax_only=True)
 
 
+def test_cv_mat_conversions(tmp_path):
+    """With an OpenCV core header on the include path (here the project's
+    stand-in), hbp_isp::Mat wraps a cv::Mat without copying, converts back by
+    copy, and refuses unsupported or non-continuous images. Host only."""
+    exe = str(tmp_path / "cvmat_check")
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(ROOT, "tests", "compat", "cv"), os.path.join(ROOT, "tests", "compat", "cvmat_check.cpp"),
+           "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
+
+
 def _run_driver(tmp_path, s, W, H, D, src=None):
     exe = str(tmp_path / "compat_pipeline")
     _compile(exe)
