@@ -7,6 +7,8 @@ launch of every kernel at a stated size. Nothing is timed or checked here.
     python hbp-isp_b200/profile_workload.py --workload median_gpu ...  # median_filter_gpu variant
     python hbp-isp_b200/profile_workload.py --workload mccnn --W 1440 --H 992 --D 144
     python hbp-isp_b200/profile_workload.py --workload ad ...
+    python hbp-isp_b200/profile_workload.py --workload segvar ...
+    python hbp-isp_b200/profile_workload.py --workload noalloc ...
 
 pair:        hbp_run_pair (post 1): grey/census/Hamming, LAB, 1-NN grid,
              CRTrees, the pyramid levels (radix sorts, scans, sums, 1-NN),
@@ -16,6 +18,10 @@ pair_lr:     hbp_run_pair (post 2): the above for both views, then the LR
 median_gpu:  the weighted median's GPU variant on the LR result of a pair.
 mccnn:       the MC-CNN volume ingest (a synthetic float volume) and HBP on it.
 ad:          the AD cost (float grey, AD volume) and HBP on it.
+segvar:      SegHAC's other configurations on the left image: Min linkage,
+             the 8-neighbour grid, the sigma = 1 pre-blur and 300 superpixels
+             (target mode), then its label image and boundary picture.
+noalloc:     the no-allocation driver median on a disparity map.
 """
 from __future__ import annotations
 
@@ -31,7 +37,7 @@ sys.path.insert(0, HERE)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", required=True, choices=["pair", "pair_lr", "median_gpu", "mccnn", "ad"])
+    ap.add_argument("--workload", required=True, choices=["pair", "pair_lr", "median_gpu", "mccnn", "ad", "segvar", "noalloc"])
     ap.add_argument("--W", type=int, default=720)
     ap.add_argument("--H", type=int, default=496)
     ap.add_argument("--D", type=int, default=128)
@@ -73,6 +79,16 @@ def main():
             out = torch.zeros((H, W), device="cuda")
             ctx.lr_check_d(dispL, dispR, planeL, fail, out, W, H)
             ctx.weighted_median_gpu_d(dL, fail, planeL, out, W, H)
+        elif a.workload == "segvar":
+            img = dev(s.left)
+            ctx.segment_target_d(img, W, H, 0, 8, 1.0, 300)
+            labels = torch.zeros(H * W, dtype=torch.int32, device="cuda")
+            ctx.segment_labels_d(labels)
+            pic = torch.zeros(H * W * 3, dtype=torch.uint8, device="cuda")
+            ctx.segment_draw_d(pic, 2, bgr=img)
+        elif a.workload == "noalloc":
+            disp = dev((np.random.default_rng(a.seed).random((H, W)) * D).astype(np.float32))
+            E.driver_median_noalloc_d(disp, W, H)
         elif a.workload == "mccnn":
             src = dev(mccnn_like_volume(s, D, a.seed + 1).astype(np.float32))
             vol = torch.zeros(E.volume_f32_bytes(W, H, D) // 4, device="cuda")
