@@ -939,12 +939,18 @@ __device__ __forceinline__ void cost_window(const StepDesc &d, int mode, int ite
         emit_chunk(l, pc, carry_n, win, carry);
 }
 
-#ifndef COST_MIN_BLOCKS
-#define COST_MIN_BLOCKS 4
+// Blocks of COST_BLOCK threads (a warp per 256-position window), at least
+// COST_MIN_BLOCKS per SM: 128 x 8 holds the same 64-register budget and
+// warps per SM as 256 x 4 and ends a launch with a shorter tail.
+#ifndef COST_BLOCK
+#define COST_BLOCK 128
 #endif
-__global__ void __launch_bounds__(256, COST_MIN_BLOCKS) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
+#ifndef COST_MIN_BLOCKS
+#define COST_MIN_BLOCKS (1024 / COST_BLOCK)
+#endif
+__global__ void __launch_bounds__(COST_BLOCK, COST_MIN_BLOCKS) k_cost(const ViewDev *__restrict__ V, StepDesc d, int mode)
 {
-    const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int item = blockIdx.x * (COST_BLOCK / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (item >= d.pre[d.nt]) // warp-uniform
         return;
@@ -1341,7 +1347,7 @@ namespace
 {
 void launch_cost(const ViewDev *V, const StepDesc &d, int mode, cudaStream_t st)
 {
-    k_cost<<<blocks((long)d.pre[d.nt] * 32, 256), 256, 0, st>>>(V, d, mode);
+    k_cost<<<blocks((long)d.pre[d.nt] * 32, COST_BLOCK), COST_BLOCK, 0, st>>>(V, d, mode);
     note_launch();
 }
 
