@@ -197,8 +197,8 @@ def message_error(scene, D):
 # DRAM bytes (read + write) per unit of one launch, from the committed ncu
 # captures of 4-view 720x496 D128 launches (profiles/k_*_4x720x496_d128.md):
 # k_cost per list position (the mean of its level-2 and level-5 captures,
-# 55.82 and 31.22 MB), k_edges per directed edge (level 2, 47.19 MB).
-KCOST_DRAM_BYTES_PER_PIXEL = (55.81696e6 + 31.21664e6) / 2 / (4 * 357120)
+# 55.71 and 31.22 MB), k_edges per directed edge (level 2, 47.19 MB).
+KCOST_DRAM_BYTES_PER_PIXEL = (55.707648e6 + 31.2192e6) / 2 / (4 * 357120)
 KEDGES_DRAM_BYTES_PER_EDGE = 47.190272e6 / 482432
 
 
