@@ -1,6 +1,7 @@
 """The CPU oracle against the reference's own outputs (golden fixtures made by
 tests/golden/make_golden.py from the reference CUDA build on a B200)."""
 import hashlib
+import sys
 import os
 
 import numpy as np
@@ -344,3 +345,23 @@ def test_post_process_at_single_pair_size(golden_dir):
     pg = O.weighted_median_gpu(z["left"], fail, pl, f["patch_weights"], z_mode=0)
     assert np.array_equal(pg.view(np.uint32), z["post_gpu_plane"].view(np.uint32))
     assert np.array_equal(O.plane_to_disp(pg).view(np.uint32), z["post_gpu_disp"].view(np.uint32))
+
+
+def test_large_size_fixture_is_current():
+    """tests/golden/large_oracle.json holds the oracle's disparity hashes of the
+    benchmark-size pairs that tests/test_gpu_large.py compares the engine with.
+    They must come from the current oracle sources and scene generator, or the
+    GPU test falls back to running the oracle itself at 1440x992 (minutes of
+    CPU): regenerate with tests/golden/make_large_oracle.py after changing
+    either."""
+    import json
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_large_oracle as G
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "large_oracle.json")) as f:
+        fx = json.load(f)
+    assert set(fx) == set(G.CASES)
+    sha = G.oracle_source_sha()
+    for name, case in G.CASES.items():
+        assert fx[name]["oracle_sha"] == sha, name
+        s = G.scene_of(case)
+        assert fx[name]["input_sha"] == G.sha_arrays(s.left, s.right), name
